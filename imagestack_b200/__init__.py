@@ -1,0 +1,248 @@
+"""B200 permutohedral-lattice Gauss transform, behind ImageStack's operation interface.
+
+The compute path is ``libpermgpu.so`` (hand-written sm_100a kernels behind the C ABI of
+``include/permgpu.h``), called through ctypes.  This module mirrors the reference's
+static ``apply`` functions (src/GaussTransform.h:6-36) for the ``permutohedral_gpu``
+method:
+
+* ``GaussTransform.apply(slice, splat, values, sigmas)`` — un-normalised transform
+  (src/GaussTransform.cpp:115-226);
+* ``JointBilateral.apply(image, reference, fw, fh, ft, color_sigma)`` — in place
+  (src/GaussTransform.cpp:504-678);
+* ``Bilateral.apply(image, fw, fh, ft, color_sigma)`` — in place (:730-734).
+
+Images are planar float32 arrays shaped (channels, frames, height, width) or
+(channels, height, width): numpy arrays live in host memory; torch CUDA tensors are used
+in place on the device.  There is no CPU path: without the library or a B200 every call
+raises ``PgpuError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpermgpu.so")
+
+OK = 0
+ERR_ARGUMENT, ERR_UNSUPPORTED, ERR_CUDA, ERR_MEMORY, ERR_CAPACITY = 1, 2, 3, 4, 5
+ERR_NO_DEVICE, ERR_ADMISSION, ERR_TIMEOUT = 7, 8, 9
+
+PAYLOADS = {"fp32": 0, "fp16": 1, "bf16": 2, "fp64": 3}
+MEM_HOST, MEM_DEVICE = 0, 1
+
+
+class PgpuError(RuntimeError):
+    """A failed call into libpermgpu (the reference raises ImageStack::Exception)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__("permgpu error %d: %s" % (code, message))
+        self.code = code
+
+
+class Image(C.Structure):
+    """pgpu_image: mirrors ImageStack::Image (src/Image.h:26-27)."""
+    _fields_ = [("base", C.c_void_p), ("width", C.c_int), ("height", C.c_int),
+                ("frames", C.c_int), ("channels", C.c_int), ("ystride", C.c_longlong),
+                ("tstride", C.c_longlong), ("cstride", C.c_longlong)]
+
+
+class Options(C.Structure):
+    _fields_ = [("payload", C.c_int), ("memory", C.c_int), ("device", C.c_int),
+                ("stream", C.c_void_p), ("load_factor", C.c_float), ("flags", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("points", C.c_longlong), ("vertices", C.c_longlong), ("capacity", C.c_longlong),
+                ("d", C.c_int), ("vd", C.c_int), ("payload", C.c_int), ("retries", C.c_int),
+                ("ms_splat", C.c_float), ("ms_compact", C.c_float), ("ms_neighbours", C.c_float),
+                ("ms_blur", C.c_float), ("ms_slice", C.c_float), ("ms_total", C.c_float)]
+
+
+EXPORTS = ["pgpu_default_options", "pgpu_last_error", "pgpu_version", "pgpu_device_count",
+           "pgpu_gauss_transform", "pgpu_joint_bilateral", "pgpu_bilateral", "pgpu_last_stats",
+           "pgpu_lattice_dump"]
+
+_lib = None
+
+
+def lib():
+    """Load libpermgpu.so (raises PgpuError if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise PgpuError(ERR_NO_DEVICE, "libpermgpu.so is not built (python -m imagestack_b200.build)")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    L.pgpu_default_options.argtypes = [P(Options)]
+    L.pgpu_last_error.restype = C.c_char_p
+    L.pgpu_gauss_transform.argtypes = [P(Image), P(Image), P(Image), P(C.c_float), C.c_int,
+                                       P(Image), P(Options)]
+    L.pgpu_joint_bilateral.argtypes = [P(Image), P(Image), C.c_float, C.c_float, C.c_float,
+                                       C.c_float, P(Options)]
+    L.pgpu_bilateral.argtypes = [P(Image), C.c_float, C.c_float, C.c_float, C.c_float, P(Options)]
+    L.pgpu_last_stats.argtypes = [P(Stats)]
+    L.pgpu_lattice_dump.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                    P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise PgpuError(rc, lib().pgpu_last_error().decode(errors="replace"))
+
+
+def last_stats() -> dict:
+    s = Stats()
+    _check(lib().pgpu_last_stats(C.byref(s)))
+    return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _view(a, name: str) -> tuple[Image, int]:
+    """pgpu_image of a planar (c, f, h, w) / (c, h, w) float32 array; returns (view, memory)."""
+    if _is_torch(a):
+        import torch
+        if a.dtype != torch.float32:
+            raise PgpuError(ERR_ARGUMENT, "%s must be float32" % name)
+        t = a if a.dim() == 4 else a.unsqueeze(1)
+        if t.dim() != 4 or t.stride(3) != 1:
+            raise PgpuError(ERR_ARGUMENT, "%s must be (c, [f,] h, w) with unit x stride" % name)
+        c, f, h, w = t.shape
+        v = Image(t.data_ptr(), w, h, f, c, t.stride(2), t.stride(1), t.stride(0))
+        return v, (MEM_DEVICE if t.is_cuda else MEM_HOST)
+    if not isinstance(a, np.ndarray) or a.dtype != np.float32:
+        raise PgpuError(ERR_ARGUMENT, "%s must be a float32 numpy array or torch tensor" % name)
+    t = a if a.ndim == 4 else a[:, None]
+    if t.ndim != 4 or t.strides[3] != 4:
+        raise PgpuError(ERR_ARGUMENT, "%s must be (c, [f,] h, w) with unit x stride" % name)
+    c, f, h, w = t.shape
+    s = [x // 4 for x in t.strides]
+    v = Image(t.ctypes.data, w, h, f, c, s[2], s[1], s[0])
+    return v, MEM_HOST
+
+
+def _options(memory: int, payload: str, device: int = 0, stream=None, load_factor: float = 0.5):
+    o = Options()
+    lib().pgpu_default_options(C.byref(o))
+    o.payload = PAYLOADS[payload]
+    o.memory = memory
+    o.device = device
+    o.stream = stream
+    o.load_factor = load_factor
+    return o
+
+
+def _torch_stream(a):
+    import torch
+    return C.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)
+
+
+def _method_ok(method: str):
+    if method != "permutohedral_gpu":
+        raise PgpuError(ERR_UNSUPPORTED,
+                        "only the permutohedral_gpu method runs here; the reference's other "
+                        "methods stay on its CPU path")
+
+
+class GaussTransform:
+    """GaussTransform::apply with the permutohedral_gpu method."""
+
+    @staticmethod
+    def apply(slice_positions, splat_positions, values, sigmas, method: str = "permutohedral_gpu",
+              payload: str = "fp32", load_factor: float = 0.5):
+        _method_ok(method)
+        same = slice_positions is None or slice_positions is splat_positions
+        sp, mem = _view(splat_positions, "splat")
+        va, mem2 = _view(values, "values")
+        sl = sp if same else _view(slice_positions, "slice")[0]
+        if mem != mem2:
+            raise PgpuError(ERR_ARGUMENT, "images must all be on the host or all on the device")
+        src = splat_positions if same else slice_positions
+        shape = (values.shape[0],) + tuple(src.shape[1:])
+        if _is_torch(splat_positions):
+            import torch
+            out = torch.empty(shape, dtype=torch.float32, device=splat_positions.device)
+        else:
+            out = np.empty(shape, np.float32)
+        ov, _ = _view(out, "out")
+        sig = (C.c_float * len(sigmas))(*[float(s) for s in sigmas])
+        stream = _torch_stream(splat_positions) if mem == MEM_DEVICE else None
+        opt = _options(mem, payload, stream=stream, load_factor=load_factor,
+                       device=(splat_positions.device.index or 0) if mem == MEM_DEVICE else 0)
+        _check(lib().pgpu_gauss_transform(None if same else C.byref(sl), C.byref(sp), C.byref(va),
+                                          sig, len(sigmas), C.byref(ov), C.byref(opt)))
+        return out
+
+
+class JointBilateral:
+    """JointBilateral::apply with the permutohedral_gpu method (in place on `image`)."""
+
+    @staticmethod
+    def apply(image, reference, filter_width: float, filter_height: float, filter_frames: float,
+              color_sigma: float, method: str = "permutohedral_gpu", payload: str = "fp32",
+              load_factor: float = 0.5):
+        _method_ok(method)
+        im, mem = _view(image, "image")
+        ref, mem2 = _view(reference, "reference")
+        if mem != mem2:
+            raise PgpuError(ERR_ARGUMENT, "image and reference must be in the same memory")
+        stream = _torch_stream(image) if mem == MEM_DEVICE else None
+        opt = _options(mem, payload, stream=stream, load_factor=load_factor,
+                       device=(image.device.index or 0) if mem == MEM_DEVICE else 0)
+        _check(lib().pgpu_joint_bilateral(C.byref(im), C.byref(ref), filter_width, filter_height,
+                                          filter_frames, color_sigma, C.byref(opt)))
+        return image
+
+
+class Bilateral:
+    """Bilateral::apply with the permutohedral_gpu method (in place)."""
+
+    @staticmethod
+    def apply(image, filter_width: float, filter_height: float, filter_frames: float,
+              color_sigma: float, method: str = "permutohedral_gpu", payload: str = "fp32",
+              load_factor: float = 0.5):
+        _method_ok(method)
+        im, mem = _view(image, "image")
+        stream = _torch_stream(image) if mem == MEM_DEVICE else None
+        opt = _options(mem, payload, stream=stream, load_factor=load_factor,
+                       device=(image.device.index or 0) if mem == MEM_DEVICE else 0)
+        _check(lib().pgpu_bilateral(C.byref(im), filter_width, filter_height, filter_frames,
+                                    color_sigma, C.byref(opt)))
+        return image
+
+
+def lattice_dump(pos: np.ndarray, val: np.ndarray, payload: str = "fp32") -> dict:
+    """Everything one lattice computes for n interleaved points (pos scaled by 1/sigma):
+    keys (M, d) in vertex order, replay vertex index and weight (n, d+1), vertex values
+    after splat and after blur (M, vd), and the replay slice (n, vd)."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    val = np.ascontiguousarray(val, np.float32)
+    n, d = pos.shape
+    vd = val.shape[1]
+    rows = n * (d + 1)
+    m = C.c_int(0)
+    keys = np.empty((rows, d), np.int16)
+    rv = np.empty((n, d + 1), np.int32)
+    rw = np.empty((n, d + 1), np.float32)
+    sv = np.empty((rows, vd), np.float32)
+    bv = np.empty((rows, vd), np.float32)
+    out = np.empty((n, vd), np.float32)
+    _check(lib().pgpu_lattice_dump(d, vd, n, pos.ctypes.data, val.ctypes.data, PAYLOADS[payload],
+                                   C.byref(m), keys.ctypes.data, rv.ctypes.data, rw.ctypes.data,
+                                   sv.ctypes.data, bv.ctypes.data, out.ctypes.data))
+    M = m.value
+    return {"keys": keys[:M].copy(), "replay_vtx": rv, "replay_w": rw, "splat": sv[:M].copy(),
+            "blur": bv[:M].copy(), "out": out}
+
+
+def device_count() -> int:
+    return int(lib().pgpu_device_count())

@@ -1,0 +1,743 @@
+// Host side of the lattice: per-device workspace, the launch sequence of one lattice,
+// the operation logic of ImageStack's GaussTransform / JointBilateral / Bilateral for
+// the permutohedral method, and the C ABI declared in include/permgpu.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "engine.h"
+
+namespace pgpu {
+
+// ---------------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------------
+static thread_local std::string t_error;
+static thread_local pgpu_stats t_stats;
+static thread_local bool t_have_stats = false;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_error = buf;
+    return code;
+}
+
+void clear_error() { t_error.clear(); }
+const char* last_error() { return t_error.c_str(); }
+void set_stats(const pgpu_stats& s) { t_stats = s; t_have_stats = true; }
+bool get_stats(pgpu_stats* s) { if (t_have_stats) *s = t_stats; return t_have_stats; }
+
+// ---------------------------------------------------------------------------------
+// buffers and engines
+// ---------------------------------------------------------------------------------
+int DevBuf::ensure(size_t need) {
+    if (need == 0) need = 16;
+    if (need <= bytes) return PGPU_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    const size_t nb = need + need / 8;
+    if (cudaMalloc(&p, nb) != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        return fail(PGPU_ERR_MEMORY, "device allocation of %zu bytes failed", nb);
+    }
+    bytes = nb;
+    return PGPU_OK;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+DevBuf::~DevBuf() { release(); }
+
+int device_count_sm100() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int good = 0;
+    for (int i = 0; i < n; ++i) {
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, i) == cudaSuccess && p.major == 10) ++good;
+    }
+    return good;
+}
+
+int Engine::init(int dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || dev < 0 || dev >= n) {
+        cudaGetLastError();
+        return fail(PGPU_ERR_NO_DEVICE, "no CUDA device %d (this library has no CPU path)", dev);
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || prop.major != 10)
+        return fail(PGPU_ERR_NO_DEVICE, "device %d is not an sm_100 (B200) GPU", dev);
+    CUDA_TRY(cudaSetDevice(dev));
+    device = dev;
+    sms = prop.multiProcessorCount;
+    CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaHostAlloc((void**)&hstat, 64, cudaHostAllocDefault));
+    for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+    return PGPU_OK;
+}
+
+static std::mutex g_engines_mu;
+static std::map<int, std::unique_ptr<Engine>> g_engines;
+
+int get_engine(int dev, Engine** out) {
+    std::lock_guard<std::mutex> lk(g_engines_mu);
+    auto it = g_engines.find(dev);
+    if (it != g_engines.end()) {
+        *out = it->second.get();
+        return PGPU_OK;
+    }
+    std::unique_ptr<Engine> e(new Engine());
+    const int rc = e->init(dev);
+    if (rc != PGPU_OK) return rc;
+    *out = e.get();
+    g_engines[dev] = std::move(e);
+    return PGPU_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// lattice constants, computed in single precision in the order of the reference
+// constructor (src/Permutohedral.h:257-274) and of `scale` (:301).  This file is
+// compiled without fast-math and with -ffp-contract=off on the host side.
+// ---------------------------------------------------------------------------------
+LatticeConsts make_consts(int d) {
+    LatticeConsts lc;
+    memset(&lc, 0, sizeof(lc));
+    for (int i = 0; i < d; i++) {
+        volatile float s = 1.0f / (sqrtf((float)(i + 1) * (i + 2)));
+        volatile float m = (float)(d + 1) * sqrtf((float)(2.0 / 3));
+        lc.sf[i] = s * m;
+    }
+    volatile float one = 1.0f;
+    lc.inv_d1 = one / (float)(d + 1);
+    return lc;
+}
+
+int vdp_for(int vd) { return vd <= 2 ? 2 : vd <= 4 ? 4 : vd <= 8 ? 8 : 0; }
+
+// ---------------------------------------------------------------------------------
+// one lattice: splat, compact, neighbours, blur, slice
+// ---------------------------------------------------------------------------------
+int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
+    const int d = J.d, vd = J.vd;
+    const DimOps* ops = dim_ops(d);
+    if (!ops) return fail(PGPU_ERR_UNSUPPORTED, "%d position dimensions (supported: 1..%d)", d, kMaxD);
+    const int vdp = vdp_for(vd);
+    if (!vdp) return fail(PGPU_ERR_UNSUPPORTED, "%d value channels (supported: 1..8)", vd);
+    if (J.payload < 0 || J.payload > 3) return fail(PGPU_ERR_ARGUMENT, "unknown payload %d", J.payload);
+    const int kw = key_words(d);
+    const uint64_t entries = (uint64_t)J.n * (uint64_t)(d + 1);
+    if (entries >= 0xFFFFFFFFull) return fail(PGPU_ERR_UNSUPPORTED, "too many points for one lattice (%u)", J.n);
+    const uint32_t nwords = (uint32_t)((entries + 31) / 32);
+    const float load = (J.load > 0.05f && J.load <= 0.9f) ? J.load : 0.5f;
+    const LatticeConsts lc = make_consts(d);
+    const size_t accb = accum_bytes(J.payload), payb = payload_bytes(J.payload);
+
+    double ratio = 1.0;
+    {
+        auto it = E.ratio.find(d);
+        if (it != E.ratio.end()) ratio = it->second;
+    }
+    uint64_t cap = 0;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        uint64_t est = (uint64_t)std::ceil(ratio * 1.3 * (double)J.n) + 1024;
+        if (est > entries + 1024) est = entries + 1024;
+        uint64_t want = (uint64_t)std::ceil((double)est / load);
+        if (attempt > 0 && want <= cap) want = cap * 2;
+        cap = (want + 255) & ~255ull;
+        if (cap < 1024) cap = 1024;
+        if (cap > 0x7FFFFF00ull) return fail(PGPU_ERR_CAPACITY, "lattice needs more than 2^31 slots");
+
+        int rc;
+        if ((rc = E.key0.ensure(cap * 16)) || (rc = E.keyn.ensure((kw - 1) * cap * 16)) ||
+            (rc = E.tvals.ensure(cap * vdp * accb)) || (rc = E.ft.ensure(cap * 4)) ||
+            (rc = E.slot2vtx.ensure(cap * 4)) || (rc = E.bitmap.ensure((size_t)nwords * 4)) ||
+            (rc = E.offs.ensure((size_t)nwords * 4)) ||
+            (rc = E.partials.ensure((size_t)scan_parts(nwords) * 4 + 16)) ||
+            (rc = E.vkey0.ensure(cap * 16)) || (rc = E.vkeyn.ensure((kw - 1) * cap * 16)) ||
+            (rc = E.vv0.ensure(cap * vdp * payb)) || (rc = E.vv1.ensure(cap * vdp * payb)) ||
+            (rc = E.nbr.ensure((size_t)(d + 1) * cap * 8)) || (rc = E.dstat.ensure(64)))
+            return rc;
+
+        unsigned* dstatus = (unsigned*)E.dstat.p;
+        uint32_t* dM = (uint32_t*)E.dstat.p + 1;
+        CUDA_TRY(cudaMemsetAsync(E.key0.p, 0xFF, cap * 16, st));
+        CUDA_TRY(cudaMemsetAsync(E.tvals.p, 0, cap * vdp * accb, st));
+        CUDA_TRY(cudaMemsetAsync(E.ft.p, 0xFF, cap * 4, st));
+        CUDA_TRY(cudaMemsetAsync(E.bitmap.p, 0, (size_t)nwords * 4, st));
+        CUDA_TRY(cudaMemsetAsync(E.dstat.p, 0, 64, st));
+        CUDA_TRY(cudaEventRecord(E.ev[0], st));
+
+        TableView tv{(uint4*)E.key0.p, (uint4*)E.keyn.p, (uint32_t)cap};
+        SplatArgs sa;
+        sa.src = J.splat;
+        sa.n = J.n;
+        sa.lc = lc;
+        sa.table = tv;
+        sa.vals = E.tvals.p;
+        sa.ft = (uint32_t*)E.ft.p;
+        sa.status = dstatus;
+        if (!ops->splat(sa, vdp, J.payload, st)) return fail(PGPU_ERR_UNSUPPORTED, "splat variant");
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaEventRecord(E.ev[1], st));
+
+        launch_mark((const uint32_t*)E.ft.p, (uint32_t)cap, (uint32_t*)E.bitmap.p, E.sms, st);
+        launch_scan((const uint32_t*)E.bitmap.p, nwords, (uint32_t*)E.partials.p,
+                    (uint32_t*)E.offs.p, dM, st);
+        CompactArgs ca;
+        ca.table = tv;
+        ca.ft = (const uint32_t*)E.ft.p;
+        ca.bitmap = (uint32_t*)E.bitmap.p;
+        ca.nwords = nwords;
+        ca.offs = (const uint32_t*)E.offs.p;
+        ca.slot2vtx = (uint32_t*)E.slot2vtx.p;
+        ca.vkey0 = (uint4*)E.vkey0.p;
+        ca.vkeyn = (uint4*)E.vkeyn.p;
+        ca.vcap = (uint32_t)cap;
+        ca.tvals = E.tvals.p;
+        ca.vvals = E.vv0.p;
+        if (!launch_assign(ca, kw, vdp, J.payload, E.sms, st)) return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
+        CUDA_TRY(cudaGetLastError());
+        if (J.dump_splat)
+            CUDA_TRY(cudaMemcpyAsync(J.dump_splat, E.vv0.p, std::min<size_t>(cap * vdp * payb, J.dump_bytes),
+                                     cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(cudaEventRecord(E.ev[2], st));
+
+        NbrArgs na;
+        na.table = tv;
+        na.slot2vtx = (const uint32_t*)E.slot2vtx.p;
+        na.vkey0 = (const uint4*)E.vkey0.p;
+        na.vkeyn = (const uint4*)E.vkeyn.p;
+        na.vcap = (uint32_t)cap;
+        na.nverts = dM;
+        na.nbr = (int2*)E.nbr.p;
+        ops->neighbours(na, (uint32_t)cap, E.sms, st);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaEventRecord(E.ev[3], st));
+
+        void* bufs[2] = {E.vv0.p, E.vv1.p};
+        for (int j = 0; j <= d; ++j) {
+            BlurArgs ba;
+            ba.nbr = (const int2*)E.nbr.p + (size_t)j * cap;
+            ba.nverts = dM;
+            ba.src = bufs[j & 1];
+            ba.dst = bufs[(j + 1) & 1];
+            if (!launch_blur(ba, (uint32_t)cap, vdp, J.payload, E.sms, st)) return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
+        }
+        CUDA_TRY(cudaGetLastError());
+        void* final_vals = bufs[(d + 1) & 1];
+        if (J.dump_blur)
+            CUDA_TRY(cudaMemcpyAsync(J.dump_blur, final_vals, std::min<size_t>(cap * vdp * payb, J.dump_bytes),
+                                     cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(cudaEventRecord(E.ev[4], st));
+
+        SliceArgs sl;
+        sl.src = J.replay ? J.splat : J.slice;
+        sl.n = J.replay ? J.n : J.n_slice;
+        sl.lc = lc;
+        sl.table = tv;
+        sl.slot2vtx = (const uint32_t*)E.slot2vtx.p;
+        sl.vvals = final_vals;
+        sl.vd = vd;
+        sl.out = J.out;
+        sl.rec_vtx = J.rec_vtx;
+        sl.rec_w = J.rec_w;
+        sl.status = dstatus;
+        if (!ops->slice(sl, vdp, J.payload, st)) return fail(PGPU_ERR_UNSUPPORTED, "slice variant");
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaEventRecord(E.ev[5], st));
+        CUDA_TRY(cudaMemcpyAsync(E.hstat, E.dstat.p, 16, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+
+        const unsigned status = E.hstat[0];
+        const uint32_t M = E.hstat[1];
+        if (status & kStatusKeyRange)
+            return fail(PGPU_ERR_ARGUMENT,
+                        "positions leave the lattice's int16 key range (the reference's keys "
+                        "wrap there and its rank indices leave [0, d]); scale them down");
+        if (status & (kStatusProbeLimit | kStatusSpinLimit)) {
+            ratio = std::max(ratio * 2.5, (double)M / std::max<uint32_t>(J.n, 1));
+            continue;
+        }
+        if (J.n) E.ratio[d] = (double)M / (double)J.n;
+        E.last_cap = cap;
+        pgpu_stats s;
+        memset(&s, 0, sizeof(s));
+        s.points = J.n;
+        s.vertices = M;
+        s.capacity = (long long)cap;
+        s.d = d;
+        s.vd = vd;
+        s.payload = J.payload;
+        s.retries = attempt;
+        cudaEventElapsedTime(&s.ms_splat, E.ev[0], E.ev[1]);
+        cudaEventElapsedTime(&s.ms_compact, E.ev[1], E.ev[2]);
+        cudaEventElapsedTime(&s.ms_neighbours, E.ev[2], E.ev[3]);
+        cudaEventElapsedTime(&s.ms_blur, E.ev[3], E.ev[4]);
+        cudaEventElapsedTime(&s.ms_slice, E.ev[4], E.ev[5]);
+        cudaEventElapsedTime(&s.ms_total, E.ev[0], E.ev[5]);
+        set_stats(s);
+        if (J.vertices_out) *J.vertices_out = M;
+        return PGPU_OK;
+    }
+    return fail(PGPU_ERR_CAPACITY, "hash table overfull after retries (d=%d, n=%u)", d, J.n);
+}
+
+// ---------------------------------------------------------------------------------
+// views and host staging
+// ---------------------------------------------------------------------------------
+bool view_ok(const pgpu_image* v) {
+    return v && v->base && v->width > 0 && v->height > 0 && v->frames > 0 && v->channels > 0 &&
+           v->ystride >= v->width && v->tstride >= 0 && v->cstride >= 0;
+}
+
+bool same_view(const pgpu_image& a, const pgpu_image& b) {
+    return a.base == b.base && a.ystride == b.ystride && a.tstride == b.tstride &&
+           a.cstride == b.cstride && a.width == b.width && a.height == b.height &&
+           a.frames == b.frames && a.channels == b.channels;
+}
+
+bool is_dense(const pgpu_image& v) {
+    return v.ystride == v.width && v.tstride == (long long)v.width * v.height &&
+           (v.channels == 1 || v.cstride == (long long)v.width * v.height * v.frames);
+}
+
+pgpu_image dense_like(const pgpu_image& v, float* base, int channels) {
+    pgpu_image d = v;
+    d.base = base;
+    d.channels = channels;
+    d.ystride = v.width;
+    d.tstride = (long long)v.width * v.height;
+    d.cstride = (long long)v.width * v.height * v.frames;
+    return d;
+}
+
+static int copy_view(const pgpu_image& src, const pgpu_image& dst, int channels, cudaMemcpyKind kind,
+                     cudaStream_t st) {
+    if (is_dense(src) && is_dense(dst)) {
+        CUDA_TRY(cudaMemcpyAsync(dst.base, src.base,
+                                 sizeof(float) * (size_t)src.width * src.height * src.frames * channels,
+                                 kind, st));
+        return PGPU_OK;
+    }
+    for (int c = 0; c < channels; ++c)
+        for (int t = 0; t < src.frames; ++t)
+            CUDA_TRY(cudaMemcpy2DAsync(dst.base + c * dst.cstride + t * dst.tstride,
+                                       sizeof(float) * dst.ystride,
+                                       src.base + c * src.cstride + t * src.tstride,
+                                       sizeof(float) * src.ystride, sizeof(float) * src.width,
+                                       src.height, kind, st));
+    return PGPU_OK;
+}
+
+int upload(Engine& E, DevBuf& buf, const pgpu_image& host, pgpu_image* dev, cudaStream_t st) {
+    const size_t n = (size_t)host.width * host.height * host.frames * host.channels;
+    int rc = buf.ensure(n * sizeof(float));
+    if (rc) return rc;
+    (void)E;
+    *dev = dense_like(host, (float*)buf.p, host.channels);
+    return copy_view(host, *dev, host.channels, cudaMemcpyHostToDevice, st);
+}
+
+int download(const pgpu_image& dev, const pgpu_image& host, int channels, cudaStream_t st) {
+    return copy_view(dev, host, channels, cudaMemcpyDeviceToHost, st);
+}
+
+PlanarView planar(const pgpu_image& v) { return PlanarView{v.base, v.ystride, v.tstride, v.cstride}; }
+
+OutView outview(const pgpu_image& v, int channels, int normalize) {
+    OutView o;
+    o.base = v.base;
+    o.ystride = v.ystride;
+    o.tstride = v.tstride;
+    o.cstride = v.cstride;
+    o.channels = channels;
+    o.normalize = normalize;
+    return o;
+}
+
+// ---------------------------------------------------------------------------------
+// GaussTransform::apply, PERMUTOHEDRAL (src/GaussTransform.cpp:115-133, 163-226),
+// on device views.
+// ---------------------------------------------------------------------------------
+int gauss_transform_device(Engine& E, const pgpu_image* slice, const pgpu_image& splat,
+                           const pgpu_image& values, const float* sigmas, int n_sigmas,
+                           const pgpu_image& out, int payload, float load, cudaStream_t st) {
+    if (splat.width != values.width || splat.height != values.height || splat.frames != values.frames)
+        return fail(PGPU_ERR_ARGUMENT, "Weights and locations of the Gaussians must be the same size");
+    const bool replay = !slice || same_view(*slice, splat);
+    if (!replay && slice->channels != splat.channels)
+        return fail(PGPU_ERR_ARGUMENT,
+                    "The evaluation locations and the locations of the Gaussians must have the same number of channels.");
+    if (n_sigmas < splat.channels) return fail(PGPU_ERR_ARGUMENT, "need one sigma per position channel");
+    const pgpu_image& sl = replay ? splat : *slice;
+    if (out.width != sl.width || out.height != sl.height || out.frames != sl.frames ||
+        out.channels < values.channels)
+        return fail(PGPU_ERR_ARGUMENT, "output must have the slice positions' size and the values' channels");
+    if (splat.channels > kMaxD) return fail(PGPU_ERR_UNSUPPORTED, "%d position dimensions (supported: 1..%d)", splat.channels, kMaxD);
+
+    LatticeJob J;
+    J.d = splat.channels;
+    J.vd = values.channels;
+    J.payload = payload;
+    J.load = load;
+    J.n = (uint32_t)((size_t)splat.width * splat.height * splat.frames);
+    PointSource& s = J.splat;
+    memset(&s, 0, sizeof(s));
+    s.width = splat.width;
+    s.height = splat.height;
+    s.frames = splat.frames;
+    s.pos = planar(splat);
+    s.pos_channels = splat.channels;
+    for (int c = 0; c < splat.channels; ++c) {
+        volatile float one = 1.0f;
+        s.pos_scale[c] = one / sigmas[c];   // invSigma (src/GaussTransform.cpp:131)
+    }
+    s.val = planar(values);
+    s.val_channels = values.channels;
+    s.homogeneous = 0;
+    J.replay = replay;
+    if (!replay) {
+        J.slice = s;
+        J.slice.width = sl.width;
+        J.slice.height = sl.height;
+        J.slice.frames = sl.frames;
+        J.slice.pos = planar(sl);
+        J.n_slice = (uint32_t)((size_t)sl.width * sl.height * sl.frames);
+    }
+    J.out = outview(out, values.channels, 0);
+    return run_lattice(E, J, st);
+}
+
+// ---------------------------------------------------------------------------------
+// JointBilateral::apply with the permutohedral method (src/GaussTransform.cpp:504-678)
+// ---------------------------------------------------------------------------------
+static pgpu_image region(const pgpu_image& v, int x, int y, int t, int w, int h, int f) {
+    pgpu_image r = v;
+    r.base = v.base + x + (long long)y * v.ystride + (long long)t * v.tstride;
+    r.width = w;
+    r.height = h;
+    r.frames = f;
+    return r;
+}
+
+int joint_bilateral_device(Engine& E, const pgpu_image& im, const pgpu_image& ref, float fw,
+                           float fh, float ft, float cs, int payload, float load, cudaStream_t st) {
+    if (im.width != ref.width || im.height != ref.height || im.frames != ref.frames)
+        return fail(PGPU_ERR_ARGUMENT, "Image and reference must be the same size");
+    if (im.width == 1) fw = 0;
+    if (im.height == 1) fh = 0;
+    if (im.frames == 1) ft = 0;
+    if (im.width > 1 && fw == 0) {   // each column independently (:516-522)
+        for (int x = 0; x < im.width; x++) {
+            int rc = joint_bilateral_device(E, region(im, x, 0, 0, 1, im.height, im.frames),
+                                            region(ref, x, 0, 0, 1, ref.height, ref.frames), 0, fh,
+                                            ft, cs, payload, load, st);
+            if (rc) return rc;
+        }
+        return PGPU_OK;
+    }
+    if (im.height > 1 && fh == 0) {   // each row independently (:524-530)
+        for (int y = 0; y < im.height; y++) {
+            int rc = joint_bilateral_device(E, region(im, 0, y, 0, im.width, 1, im.frames),
+                                            region(ref, 0, y, 0, ref.width, 1, ref.frames), fw, 0,
+                                            ft, cs, payload, load, st);
+            if (rc) return rc;
+        }
+        return PGPU_OK;
+    }
+    if (im.frames > 1 && ft == 0) {   // each frame independently (:532-538)
+        for (int t = 0; t < im.frames; t++) {
+            int rc = joint_bilateral_device(E, region(im, 0, 0, t, im.width, im.height, 1),
+                                            region(ref, 0, 0, t, ref.width, ref.height, 1), fw, fh,
+                                            0, cs, payload, load, st);
+            if (rc) return rc;
+        }
+        return PGPU_OK;
+    }
+    const bool fx = im.width > 1 && fw < 10 * im.width;
+    const bool fy = im.height > 1 && fh < 10 * im.height;
+    const bool fz = im.frames > 1 && ft < 10 * im.frames;
+    const int d = ref.channels + (fx ? 1 : 0) + (fy ? 1 : 0) + (fz ? 1 : 0);
+    if (d > kMaxD) return fail(PGPU_ERR_UNSUPPORTED, "%d position dimensions (supported: 1..%d)", d, kMaxD);
+    if (im.channels + 1 > 8) return fail(PGPU_ERR_UNSUPPORTED, "%d image channels (supported: 1..7)", im.channels);
+
+    LatticeJob J;
+    J.d = d;
+    J.vd = im.channels + 1;
+    J.payload = payload;
+    J.load = load;
+    J.n = (uint32_t)((size_t)im.width * im.height * im.frames);
+    PointSource& s = J.splat;
+    memset(&s, 0, sizeof(s));
+    s.width = im.width;
+    s.height = im.height;
+    s.frames = im.frames;
+    s.pos = planar(ref);
+    s.pos_channels = ref.channels;
+    volatile float one = 1.0f;
+    const float inv_r = one / cs;   // ref / colorSigma == ref * (1.0f/colorSigma) (src/Expr.h:2439-2443)
+    for (int c = 0; c < ref.channels; ++c) s.pos_scale[c] = inv_r;
+    s.coord_mask = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
+    s.coord_scale[0] = fx ? one / fw : 0.0f;
+    s.coord_scale[1] = fy ? one / fh : 0.0f;
+    s.coord_scale[2] = fz ? one / ft : 0.0f;
+    s.val = planar(im);
+    s.val_channels = im.channels;
+    s.homogeneous = 1;
+    J.replay = true;
+    J.out = outview(im, im.channels, 1);
+    return run_lattice(E, J, st);
+}
+
+}  // namespace pgpu
+
+// =================================================================================
+// C ABI
+// =================================================================================
+using namespace pgpu;
+
+namespace {
+
+struct ApiScope {
+    Engine* E = nullptr;
+    std::unique_lock<std::mutex> lock;
+    cudaStream_t st = nullptr;
+    int rc = PGPU_OK;
+    ApiScope(const pgpu_options* opt) {
+        clear_error();
+        const int dev = opt ? opt->device : 0;
+        rc = get_engine(dev, &E);
+        if (rc) return;
+        lock = std::unique_lock<std::mutex>(E->mu);
+        if (cudaSetDevice(dev) != cudaSuccess) {
+            rc = fail(PGPU_ERR_CUDA, "cudaSetDevice(%d) failed", dev);
+            return;
+        }
+        st = (opt && opt->memory == PGPU_MEM_DEVICE && opt->stream) ? (cudaStream_t)opt->stream : E->stream;
+    }
+};
+
+pgpu_options opts_or_default(const pgpu_options* o) {
+    pgpu_options d;
+    pgpu_default_options(&d);
+    return o ? *o : d;
+}
+
+}  // namespace
+
+extern "C" {
+
+void pgpu_default_options(pgpu_options* opt) {
+    if (!opt) return;
+    memset(opt, 0, sizeof(*opt));
+    opt->payload = PGPU_PAYLOAD_FP32;
+    opt->memory = PGPU_MEM_HOST;
+    opt->device = 0;
+    opt->stream = nullptr;
+    opt->load_factor = 0.5f;
+}
+
+const char* pgpu_last_error(void) { return last_error(); }
+
+int pgpu_version(void) { return 100; }
+
+int pgpu_device_count(void) { return device_count_sm100(); }
+
+int pgpu_last_stats(pgpu_stats* out) {
+    if (!out) return fail(PGPU_ERR_ARGUMENT, "null stats pointer");
+    if (!get_stats(out)) return fail(PGPU_ERR_ARGUMENT, "no lattice has run on this thread");
+    return PGPU_OK;
+}
+
+int pgpu_gauss_transform(const pgpu_image* slice, const pgpu_image* splat, const pgpu_image* values,
+                         const float* sigmas, int n_sigmas, pgpu_image* out,
+                         const pgpu_options* opt_in) {
+    const pgpu_options opt = opts_or_default(opt_in);
+    if (!view_ok(splat) || !view_ok(values) || !view_ok(out) || (slice && !view_ok(slice)) || !sigmas)
+        return fail(PGPU_ERR_ARGUMENT, "invalid image view or sigmas");
+    ApiScope S(&opt);
+    if (S.rc) return S.rc;
+    Engine& E = *S.E;
+    if (opt.memory == PGPU_MEM_DEVICE) {
+        int rc = gauss_transform_device(E, slice, *splat, *values, sigmas, n_sigmas, *out,
+                                        opt.payload, opt.load_factor, S.st);
+        return rc;
+    }
+    const bool replay = !slice || same_view(*slice, *splat);
+    pgpu_image dsplat, dvals, dslice, dout;
+    int rc;
+    if ((rc = upload(E, E.img_a, *splat, &dsplat, S.st))) return rc;
+    if ((rc = upload(E, E.img_b, *values, &dvals, S.st))) return rc;
+    if (!replay && (rc = upload(E, E.img_c, *slice, &dslice, S.st))) return rc;
+    const pgpu_image& sl = replay ? *splat : *slice;
+    if ((rc = E.img_d.ensure(sizeof(float) * (size_t)sl.width * sl.height * sl.frames * values->channels)))
+        return rc;
+    dout = dense_like(sl, (float*)E.img_d.p, values->channels);
+    rc = gauss_transform_device(E, replay ? nullptr : &dslice, dsplat, dvals, sigmas, n_sigmas, dout,
+                                opt.payload, opt.load_factor, S.st);
+    if (rc) return rc;
+    if ((rc = download(dout, *out, values->channels, S.st))) return rc;
+    CUDA_TRY(cudaStreamSynchronize(S.st));
+    return PGPU_OK;
+}
+
+int pgpu_joint_bilateral(pgpu_image* im, const pgpu_image* ref, float filter_width,
+                         float filter_height, float filter_frames, float color_sigma,
+                         const pgpu_options* opt_in) {
+    const pgpu_options opt = opts_or_default(opt_in);
+    if (!view_ok(im) || !view_ok(ref)) return fail(PGPU_ERR_ARGUMENT, "invalid image view");
+    ApiScope S(&opt);
+    if (S.rc) return S.rc;
+    Engine& E = *S.E;
+    if (opt.memory == PGPU_MEM_DEVICE)
+        return joint_bilateral_device(E, *im, *ref, filter_width, filter_height, filter_frames,
+                                      color_sigma, opt.payload, opt.load_factor, S.st);
+    const bool same = same_view(*im, *ref);
+    pgpu_image dim, dref;
+    int rc;
+    if ((rc = upload(E, E.img_a, *im, &dim, S.st))) return rc;
+    if (same) dref = dim;
+    else if ((rc = upload(E, E.img_b, *ref, &dref, S.st))) return rc;
+    rc = joint_bilateral_device(E, dim, dref, filter_width, filter_height, filter_frames, color_sigma,
+                                opt.payload, opt.load_factor, S.st);
+    if (rc) return rc;
+    if ((rc = download(dim, *im, im->channels, S.st))) return rc;
+    CUDA_TRY(cudaStreamSynchronize(S.st));
+    return PGPU_OK;
+}
+
+int pgpu_bilateral(pgpu_image* im, float filter_width, float filter_height, float filter_frames,
+                   float color_sigma, const pgpu_options* opt) {
+    return pgpu_joint_bilateral(im, im, filter_width, filter_height, filter_frames, color_sigma, opt);
+}
+
+int pgpu_lattice_dump(int d, int vd, int n, const float* pos, const float* val, int payload,
+                      int* n_vertices, short* keys, int* replay_vtx, float* replay_w,
+                      float* splat_vals, float* blur_vals, float* out) {
+    if (d < 1 || d > kMaxD || vd < 1 || vd > 8 || n < 1 || !pos || !val)
+        return fail(PGPU_ERR_ARGUMENT, "invalid dump arguments");
+    pgpu_options opt;
+    pgpu_default_options(&opt);
+    opt.payload = payload;
+    ApiScope S(&opt);
+    if (S.rc) return S.rc;
+    Engine& E = *S.E;
+    cudaStream_t st = S.st;
+    // planar (channel-major) copies of the interleaved points
+    std::vector<float> hp((size_t)n * d), hv((size_t)n * vd);
+    for (int i = 0; i < n; ++i) {
+        for (int c = 0; c < d; ++c) hp[(size_t)c * n + i] = pos[(size_t)i * d + c];
+        for (int c = 0; c < vd; ++c) hv[(size_t)c * n + i] = val[(size_t)i * vd + c];
+    }
+    const int vdp = vdp_for(vd);
+    const size_t rows = (size_t)n * (d + 1);
+    const size_t payb = payload_bytes(payload);
+    DevBuf bp, bv, bo, brv, brw, bsv, bbv;
+    int rc;
+    if ((rc = bp.ensure(hp.size() * 4)) || (rc = bv.ensure(hv.size() * 4)) ||
+        (rc = bo.ensure((size_t)n * vd * 4)) || (rc = brv.ensure(rows * 4)) ||
+        (rc = brw.ensure(rows * 4)))
+        return rc;
+    // at most n*(d+1) vertices: the dumps copy that many rows of the vertex buffers
+    const size_t dump_bytes = rows * vdp * payb;
+    if ((rc = bsv.ensure(dump_bytes)) || (rc = bbv.ensure(dump_bytes))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(bp.p, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(bv.p, hv.data(), hv.size() * 4, cudaMemcpyHostToDevice, st));
+    pgpu_image vpos = {(float*)bp.p, n, 1, 1, d, n, n, n};
+    pgpu_image vval = {(float*)bv.p, n, 1, 1, vd, n, n, n};
+    pgpu_image vout = {(float*)bo.p, n, 1, 1, vd, n, n, n};
+    LatticeJob J;
+    J.d = d;
+    J.vd = vd;
+    J.payload = payload;
+    J.load = 0.5f;
+    J.n = (uint32_t)n;
+    memset(&J.splat, 0, sizeof(J.splat));
+    J.splat.width = n;
+    J.splat.height = 1;
+    J.splat.frames = 1;
+    J.splat.pos = planar(vpos);
+    J.splat.pos_channels = d;
+    for (int c = 0; c < d; ++c) J.splat.pos_scale[c] = 1.0f;
+    J.splat.val = planar(vval);
+    J.splat.val_channels = vd;
+    J.replay = true;
+    J.out = outview(vout, vd, 0);
+    J.rec_vtx = (int*)brv.p;
+    J.rec_w = (float*)brw.p;
+    J.dump_splat = bsv.p;
+    J.dump_blur = bbv.p;
+    J.dump_bytes = dump_bytes;
+    uint32_t M = 0;
+    J.vertices_out = &M;
+    rc = run_lattice(E, J, st);
+    if (rc) return rc;
+    if (n_vertices) *n_vertices = (int)M;
+    if (out) CUDA_TRY(cudaMemcpy(out, bo.p, (size_t)n * vd * 4, cudaMemcpyDeviceToHost));
+    if (replay_vtx) CUDA_TRY(cudaMemcpy(replay_vtx, brv.p, rows * 4, cudaMemcpyDeviceToHost));
+    if (replay_w) CUDA_TRY(cudaMemcpy(replay_w, brw.p, rows * 4, cudaMemcpyDeviceToHost));
+    const int kw = key_words(d);
+    if (keys) {
+        std::vector<uint4> k0(M), kn((size_t)(kw - 1) * M);
+        const size_t vcap = E.last_cap;
+        if (M) CUDA_TRY(cudaMemcpy(k0.data(), E.vkey0.p, (size_t)M * 16, cudaMemcpyDeviceToHost));
+        for (int w = 1; w < kw; ++w)
+            if (M) CUDA_TRY(cudaMemcpy(kn.data() + (size_t)(w - 1) * M, (uint4*)E.vkeyn.p + (size_t)(w - 1) * vcap,
+                                      (size_t)M * 16, cudaMemcpyDeviceToHost));
+        for (uint32_t v = 0; v < M; ++v) {
+            for (int c = 0; c < d; ++c) {
+                const int wi = lane_word(c), lp = lane_pos(c);
+                const uint4 w = wi == 0 ? k0[v] : kn[(size_t)(wi - 1) * M + v];
+                const uint32_t u = (lp >> 1) == 0 ? w.x : (lp >> 1) == 1 ? w.y : (lp >> 1) == 2 ? w.z : w.w;
+                const uint32_t lane = (lp & 1) ? (u >> 16) : (u & 0xFFFFu);
+                keys[(size_t)v * d + c] = (short)(uint16_t)(lane ^ 0x8000u);
+            }
+        }
+    }
+    auto conv = [&](void* dev, float* dst) -> int {
+        if (!dst || !M) return PGPU_OK;
+        std::vector<unsigned char> raw((size_t)M * vdp * payb);
+        CUDA_TRY(cudaMemcpy(raw.data(), dev, raw.size(), cudaMemcpyDeviceToHost));
+        for (uint32_t v = 0; v < M; ++v)
+            for (int c = 0; c < vd; ++c) {
+                const size_t idx = (size_t)v * vdp + c;
+                float f;
+                if (payload == kPayloadF32) f = ((float*)raw.data())[idx];
+                else if (payload == kPayloadF64) f = (float)((double*)raw.data())[idx];
+                else {
+                    const uint16_t h = ((uint16_t*)raw.data())[idx];
+                    f = payload == kPayloadF16 ? half_bits_to_float(h) : bf16_bits_to_float(h);
+                }
+                dst[(size_t)v * vd + c] = f;
+            }
+        return PGPU_OK;
+    };
+    if ((rc = conv(bsv.p, splat_vals))) return rc;
+    if ((rc = conv(bbv.p, blur_vals))) return rc;
+    return PGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,114 @@
+// Host-side declarations shared by the C-ABI entry points, the batched pipeline and the
+// request server.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+
+#include "../../include/permgpu.h"
+#include "lattice_ops.h"
+
+namespace pgpu {
+
+int fail(int code, const char* fmt, ...);
+void clear_error();
+const char* last_error();
+void set_stats(const pgpu_stats& s);
+bool get_stats(pgpu_stats* s);
+
+#define CUDA_TRY(x)                                                                     \
+    do {                                                                                \
+        cudaError_t e_ = (x);                                                           \
+        if (e_ != cudaSuccess)                                                          \
+            return ::pgpu::fail(PGPU_ERR_CUDA, "%s: %s (%s:%d)", #x, cudaGetErrorString(e_), \
+                                __FILE__, __LINE__);                                    \
+    } while (0)
+
+// grow-only device allocation
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t need);
+    void release();
+    ~DevBuf();
+};
+
+struct Engine {
+    int device = -1;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    // hash table (slot space)
+    DevBuf key0, keyn, tvals, ft, slot2vtx;
+    // compaction
+    DevBuf bitmap, offs, partials;
+    // vertex space
+    DevBuf vkey0, vkeyn, vv0, vv1, nbr;
+    DevBuf dstat;
+    // staging images for host-memory calls
+    DevBuf img_a, img_b, img_c, img_d;
+    unsigned* hstat = nullptr;
+    cudaEvent_t ev[8] = {};
+    std::map<int, double> ratio;   // learned vertices per point, by d
+    size_t last_cap = 0;
+    int init(int dev);
+};
+
+int get_engine(int dev, Engine** out);
+int device_count_sm100();
+
+struct LatticeJob {
+    int d = 0, vd = 0, payload = 0;
+    float load = 0.5f;
+    PointSource splat;
+    uint32_t n = 0;
+    bool replay = true;
+    PointSource slice;
+    uint32_t n_slice = 0;
+    OutView out;
+    int* rec_vtx = nullptr;
+    float* rec_w = nullptr;
+    void* dump_splat = nullptr;   // device copy of vertex values after the splat
+    void* dump_blur = nullptr;    // ... and after the blur
+    size_t dump_bytes = 0;
+    uint32_t* vertices_out = nullptr;
+};
+
+LatticeConsts make_consts(int d);
+int vdp_for(int vd);
+int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st);
+
+inline float half_bits_to_float(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h >> 15) << 31;
+    const int exp = (h >> 10) & 0x1F;
+    const uint32_t man = h & 0x3FF;
+    uint32_t bits;
+    if (exp == 0) {
+        if (man == 0) {
+            bits = sign;
+        } else {   // subnormal: value = man * 2^-24
+            float f = (float)man * (1.0f / 16777216.0f);
+            uint32_t fb;
+            memcpy(&fb, &f, 4);
+            bits = sign | fb;
+        }
+    } else if (exp == 31) {
+        bits = sign | 0x7F800000u | (man << 13);
+    } else {
+        bits = sign | ((uint32_t)(exp - 15 + 127) << 23) | (man << 13);
+    }
+    float out;
+    memcpy(&out, &bits, 4);
+    return out;
+}
+
+inline float bf16_bits_to_float(uint16_t h) {
+    const uint32_t bits = (uint32_t)h << 16;
+    float out;
+    memcpy(&out, &bits, 4);
+    return out;
+}
+
+}  // namespace pgpu

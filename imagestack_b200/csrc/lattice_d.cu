@@ -1,0 +1,77 @@
+// Per-dimension instantiation of the splat, neighbour and slice kernels.  This file is
+// compiled once for each d in 1..16 with -DPGPU_D=d, so the sixteen variants build in
+// parallel and each keeps its per-point arrays in registers.
+#include "lattice_ops.h"
+
+#ifndef PGPU_D
+#error "compile with -DPGPU_D=<number of position dimensions>"
+#endif
+
+namespace pgpu {
+namespace {
+
+constexpr int D = PGPU_D;
+
+int grid_cap(uint64_t work, int threads, int sms) {
+    uint64_t g = (work + threads - 1) / threads;
+    const uint64_t cap = (uint64_t)sms * 16;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+template <int VDP, typename Acc>
+void splat_t(const SplatArgs& a, cudaStream_t st) {
+    const uint32_t blocks = (a.n + kSplatThreads - 1) / kSplatThreads;
+    if (blocks) splat_kernel<D, VDP, Acc><<<blocks, kSplatThreads, 0, st>>>(a);
+}
+
+bool splat(const SplatArgs& a, int vdp, int payload, cudaStream_t st) {
+    const bool f64 = payload == kPayloadF64;
+    switch (vdp) {
+    case 2: f64 ? splat_t<2, double>(a, st) : splat_t<2, float>(a, st); return true;
+    case 4: f64 ? splat_t<4, double>(a, st) : splat_t<4, float>(a, st); return true;
+    case 8: f64 ? splat_t<8, double>(a, st) : splat_t<8, float>(a, st); return true;
+    }
+    return false;
+}
+
+void neighbours(const NbrArgs& a, uint32_t vmax, int sms, cudaStream_t st) {
+    neighbours_kernel<D><<<grid_cap(vmax, 256, sms), 256, 0, st>>>(a);
+}
+
+template <int VDP, typename P>
+void slice_t(const SliceArgs& a, cudaStream_t st) {
+    const uint32_t blocks = (a.n + kSliceThreads - 1) / kSliceThreads;
+    if (blocks) slice_kernel<D, VDP, P><<<blocks, kSliceThreads, 0, st>>>(a);
+}
+
+template <int VDP>
+bool slice_p(const SliceArgs& a, int payload, cudaStream_t st) {
+    switch (payload) {
+    case kPayloadF32: slice_t<VDP, float>(a, st); return true;
+    case kPayloadF16: slice_t<VDP, __half>(a, st); return true;
+    case kPayloadBF16: slice_t<VDP, __nv_bfloat16>(a, st); return true;
+    case kPayloadF64: slice_t<VDP, double>(a, st); return true;
+    }
+    return false;
+}
+
+bool slice(const SliceArgs& a, int vdp, int payload, cudaStream_t st) {
+    switch (vdp) {
+    case 2: return slice_p<2>(a, payload, st);
+    case 4: return slice_p<4>(a, payload, st);
+    case 8: return slice_p<8>(a, payload, st);
+    }
+    return false;
+}
+
+const DimOps kOps = {splat, neighbours, slice};
+
+}  // namespace
+
+#define PGPU_CAT2(a, b) a##b
+#define PGPU_CAT(a, b) PGPU_CAT2(a, b)
+const DimOps* PGPU_CAT(dim_ops_, PGPU_D)() { return &kOps; }
+
+}  // namespace pgpu

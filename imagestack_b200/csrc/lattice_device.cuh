@@ -1,0 +1,366 @@
+// Device-side building blocks of the permutohedral lattice for sm_100a.
+//
+// Each function here restates one step of ImageStack's src/Permutohedral.h for one
+// point per thread.  Everything that determines the lattice keys follows the
+// reference's single-precision evaluation order with explicitly rounded intrinsics
+// (__fmul_rn / __fadd_rn / __fsub_rn), so the keys, the occupied vertex set and the
+// per-point vertex indices are bit-exact with the reference's strict-IEEE build, and no
+// compiler contraction into FMA can change them.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pgpu {
+
+constexpr int kMaxD = 16;      // position dimensions supported by the kernels
+constexpr int kMaxProbe = 1 << 14;
+constexpr int kMaxSpin = 1 << 20;
+
+// status bits written by the kernels (atomicOr into the job's status word)
+constexpr unsigned kStatusProbeLimit = 1u;   // hash table too full: rerun with more slots
+constexpr unsigned kStatusSpinLimit = 2u;    // a pending slot never became ready
+constexpr unsigned kStatusKeyRange = 4u;     // an elevated coordinate left the int16 range
+
+// ---------------------------------------------------------------------------------
+// Keys.  A vertex key is d int16 coordinates (the (d+1)-th is implied, the keys of
+// src/Permutohedral.h:365-369).  On the device a key is KW 16-byte words:
+//   word 0: coordinates 0..6 in lanes 0..6, slot state in lane 7;
+//   word k>0: coordinates 7+8(k-1) .. 14+8(k-1).
+// Coordinates are stored XOR 0x8000, so that a 32-bit half of a word is all ones only
+// for the coordinate pair (32767, 32767); an all-ones word is how an empty slot looks.
+// ---------------------------------------------------------------------------------
+__host__ __device__ constexpr int key_words(int d) { return d <= 7 ? 1 : 1 + (d - 7 + 7) / 8; }
+
+constexpr uint32_t kStateReady = 0x0000u;
+constexpr uint32_t kStatePending = 0x0001u;
+constexpr uint32_t kStateEmpty = 0xFFFFu;
+
+template <int KW>
+struct Key {
+    uint4 w[KW];
+};
+
+__device__ __forceinline__ uint32_t enc_lane(int v) { return ((uint32_t)(uint16_t)(short)v) ^ 0x8000u; }
+__device__ __forceinline__ int dec_lane(uint32_t e) { return (int)(short)(uint16_t)(e ^ 0x8000u); }
+
+__device__ __forceinline__ uint32_t& word_u32(uint4& w, int i) {
+    return i == 0 ? w.x : i == 1 ? w.y : i == 2 ? w.z : w.w;
+}
+__device__ __forceinline__ uint32_t word_u32(const uint4& w, int i) {
+    return i == 0 ? w.x : i == 1 ? w.y : i == 2 ? w.z : w.w;
+}
+
+// Lane index of coordinate c inside the key words.
+__host__ __device__ constexpr int lane_word(int c) { return c < 7 ? 0 : 1 + (c - 7) / 8; }
+__host__ __device__ constexpr int lane_pos(int c) { return c < 7 ? c : (c - 7) % 8; }
+
+template <int D>
+__device__ __forceinline__ void pack_key(const int (&k)[D], Key<key_words(D)>& out) {
+    constexpr int KW = key_words(D);
+    uint32_t lanes[KW * 8];
+#pragma unroll
+    for (int i = 0; i < KW * 8; ++i) lanes[i] = enc_lane(0);
+#pragma unroll
+    for (int c = 0; c < D; ++c) lanes[lane_word(c) * 8 + lane_pos(c)] = enc_lane(k[c]);
+    lanes[7] = kStateReady;
+#pragma unroll
+    for (int w = 0; w < KW; ++w) {
+        out.w[w].x = lanes[w * 8 + 0] | (lanes[w * 8 + 1] << 16);
+        out.w[w].y = lanes[w * 8 + 2] | (lanes[w * 8 + 3] << 16);
+        out.w[w].z = lanes[w * 8 + 4] | (lanes[w * 8 + 5] << 16);
+        out.w[w].w = lanes[w * 8 + 6] | (lanes[w * 8 + 7] << 16);
+    }
+}
+
+template <int D>
+__device__ __forceinline__ void unpack_key(const Key<key_words(D)>& in, int (&k)[D]) {
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+        const uint4& w = in.w[lane_word(c)];
+        int p = lane_pos(c);
+        uint32_t u = word_u32(w, p >> 1);
+        k[c] = dec_lane((p & 1) ? (u >> 16) : (u & 0xFFFFu));
+    }
+}
+
+__device__ __forceinline__ uint32_t word_state(const uint4& w) { return w.w >> 16; }
+__device__ __forceinline__ bool maybe_empty(const uint4& w) {
+    return w.x == 0xFFFFFFFFu || w.y == 0xFFFFFFFFu || w.z == 0xFFFFFFFFu || w.w == 0xFFFFFFFFu;
+}
+__device__ __forceinline__ bool is_empty_word(const uint4& w) {
+    return w.x == 0xFFFFFFFFu && w.y == 0xFFFFFFFFu && w.z == 0xFFFFFFFFu && w.w == 0xFFFFFFFFu;
+}
+__device__ __forceinline__ bool words_equal(const uint4& a, const uint4& b) {
+    return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w;
+}
+// equal in coordinates 0..6 (the state lane is ignored)
+__device__ __forceinline__ bool prefix_equal(const uint4& a, const uint4& b) {
+    return a.x == b.x && a.y == b.y && a.z == b.z && (a.w & 0xFFFFu) == (b.w & 0xFFFFu);
+}
+__device__ __forceinline__ uint4 with_state(uint4 w, uint32_t s) {
+    w.w = (w.w & 0xFFFFu) | (s << 16);
+    return w;
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z ^= z >> 30;
+    z *= 0xBF58476D1CE4E5B9ull;
+    z ^= z >> 27;
+    z *= 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return z;
+}
+
+template <int KW>
+__device__ __forceinline__ uint32_t key_hash(const Key<KW>& k) {
+    uint64_t h = 0x2545F4914F6CDD1Dull;
+#pragma unroll
+    for (int w = 0; w < KW; ++w) {
+        uint4 q = k.w[w];
+        if (w == 0) q.w &= 0xFFFFu;   // the state lane is not part of the key
+        uint64_t a = (uint64_t)q.x | ((uint64_t)q.y << 32);
+        uint64_t b = (uint64_t)q.z | ((uint64_t)q.w << 32);
+        h = mix64(h ^ a);
+        h = mix64(h ^ b);
+    }
+    return (uint32_t)(h >> 32);
+}
+
+// ---------------------------------------------------------------------------------
+// Hash table: open addressing with linear probing over `cap` slots (any cap, mapped
+// with a multiply-high).  key0[s] holds word 0, keyn[(w-1)*cap + s] the later words.
+// The slot also owns an accumulator row vals[s*VDP..] and the first-touch entry ft[s]
+// (smallest point*(d+1)+remainder that reached it), which later fixes the vertex's
+// index: the reference numbers vertices in the order of their first insertion
+// (src/Permutohedral.h:69-75).
+// ---------------------------------------------------------------------------------
+struct TableView {
+    uint4* key0;
+    uint4* keyn;
+    uint32_t cap;
+};
+
+__device__ __forceinline__ uint32_t home_slot(uint32_t h, uint32_t cap) { return __umulhi(h, cap); }
+
+// Insert-or-find during the splat; returns the slot or -1 (status bit set).
+template <int KW>
+__device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t h, unsigned* status) {
+    const uint4 empty = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+    uint32_t s = home_slot(h, t.cap);
+    for (int probe = 0; probe < kMaxProbe; ++probe) {
+        uint4 w = __ldcg(&t.key0[s]);
+        if (maybe_empty(w)) {
+            // An empty slot, or a read that raced with the slot's one-time fill: the
+            // compare-and-swap decides, and returns the slot's real contents.
+            uint4 desired = (KW == 1) ? k.w[0] : with_state(k.w[0], kStatePending);
+            w = atomicCAS(&t.key0[s], empty, desired);
+            if (is_empty_word(w)) {
+                if (KW > 1) {
+#pragma unroll
+                    for (int i = 1; i < KW; ++i) __stcg(&t.keyn[(size_t)(i - 1) * t.cap + s], k.w[i]);
+                    __threadfence();
+                    atomicExch(&t.key0[s], k.w[0]);
+                }
+                return (int)s;
+            }
+        }
+        if (KW == 1) {
+            if (words_equal(w, k.w[0])) return (int)s;
+        } else if (prefix_equal(w, k.w[0])) {
+            int spins = 0;
+            while (word_state(w) == kStatePending) {
+                if (++spins > kMaxSpin) {
+                    atomicOr(status, kStatusSpinLimit);
+                    return -1;
+                }
+                __nanosleep(64);
+                w = __ldcg(&t.key0[s]);
+            }
+            __threadfence();
+            bool same = true;
+#pragma unroll
+            for (int i = 1; i < KW; ++i)
+                same = same && words_equal(__ldcg(&t.keyn[(size_t)(i - 1) * t.cap + s]), k.w[i]);
+            if (same) return (int)s;
+        }
+        s = (s + 1 == t.cap) ? 0u : s + 1;
+    }
+    atomicOr(status, kStatusProbeLimit);
+    return -1;
+}
+
+// Lookup in a table that no thread modifies any more (after the splat); -1 if absent.
+template <int KW>
+__device__ __forceinline__ int table_find(const TableView& t, const Key<KW>& k, uint32_t h) {
+    uint32_t s = home_slot(h, t.cap);
+    for (int probe = 0; probe < kMaxProbe; ++probe) {
+        uint4 w = __ldg(&t.key0[s]);
+        if (is_empty_word(w)) return -1;
+        if (KW == 1) {
+            if (words_equal(w, k.w[0])) return (int)s;
+        } else if (prefix_equal(w, k.w[0])) {
+            bool same = true;
+#pragma unroll
+            for (int i = 1; i < KW; ++i)
+                same = same && words_equal(__ldg(&t.keyn[(size_t)(i - 1) * t.cap + s]), k.w[i]);
+            if (same) return (int)s;
+        }
+        s = (s + 1 == t.cap) ? 0u : s + 1;
+    }
+    return -1;
+}
+
+// ---------------------------------------------------------------------------------
+// The simplex that encloses one point: src/Permutohedral.h:293-356.
+// ---------------------------------------------------------------------------------
+struct LatticeConsts {
+    float sf[kMaxD];   // scaleFactor[i] (src/Permutohedral.h:257-274), computed on the host
+    float inv_d1;      // 1.0f/(d+1), computed on the host
+};
+
+// gcc on x86-64 converts float to short through a 32-bit cvttss2si, which yields
+// INT_MIN for NaN and out-of-range values; the result is then truncated to 16 bits.
+__device__ __forceinline__ int x86_float_to_int(float f) {
+    return (fabsf(f) < 2147483648.0f) ? __float2int_rz(f) : (int)0x80000000;
+}
+
+template <int D>
+struct Simplex {
+    int g[D + 1];      // greedy[] after the hyperplane correction (int16 values)
+    int rank[D + 1];
+    float bary[D + 1]; // barycentric weight of remainder r
+};
+
+template <int D>
+__device__ __forceinline__ void compute_simplex(const float (&p)[D], const LatticeConsts& lc,
+                                                Simplex<D>& sx, unsigned* range_flag) {
+    float e[D + 1];
+    // elevated[d] = -d*position[d-1]*scaleFactor[d-1]
+    e[D] = __fmul_rn(__fmul_rn((float)(-D), p[D - 1]), lc.sf[D - 1]);
+#pragma unroll
+    for (int i = D - 1; i > 0; --i) {
+        float a = __fmul_rn(__fmul_rn((float)i, p[i - 1]), lc.sf[i - 1]);
+        float c = __fmul_rn(__fmul_rn((float)(i + 2), p[i]), lc.sf[i]);
+        e[i] = __fadd_rn(__fsub_rn(e[i + 1], a), c);
+    }
+    e[0] = __fadd_rn(e[1], __fmul_rn(__fmul_rn(2.0f, p[0]), lc.sf[0]));
+
+    const float scale = lc.inv_d1;
+    const float dp1 = (float)(D + 1);
+    int sum = 0;
+    bool out_of_range = false;
+#pragma unroll
+    for (int i = 0; i <= D; ++i) {
+        float v = __fmul_rn(e[i], scale);
+        float up = __fmul_rn(ceilf(v), dp1);
+        float down = __fmul_rn(floorf(v), dp1);
+        float pick = (__fsub_rn(up, e[i]) < __fsub_rn(e[i], down)) ? up : down;
+        out_of_range |= !(fabsf(pick) <= 32767.0f);
+        int gi = (int)(short)x86_float_to_int(pick);
+        sx.g[i] = gi;
+        sum += gi;
+    }
+    if (out_of_range && range_flag) atomicOr(range_flag, kStatusKeyRange);
+    sum /= (D + 1);   // C division: truncation toward zero
+
+    // rank differential; ties count for j (src/Permutohedral.h:321-324)
+    float diff[D + 1];
+#pragma unroll
+    for (int i = 0; i <= D; ++i) {
+        sx.rank[i] = 0;
+        diff[i] = __fsub_rn(e[i], (float)sx.g[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = i + 1; j <= D; ++j) {
+            if (diff[i] < diff[j]) sx.rank[i]++;
+            else sx.rank[j]++;
+        }
+
+    // back onto the hyperplane (src/Permutohedral.h:326-348)
+    if (sum > 0) {
+#pragma unroll
+        for (int i = 0; i <= D; ++i) {
+            if (sx.rank[i] >= D + 1 - sum) {
+                sx.g[i] = (int)(short)(sx.g[i] - (D + 1));
+                sx.rank[i] += sum - (D + 1);
+            } else {
+                sx.rank[i] += sum;
+            }
+        }
+    } else if (sum < 0) {
+#pragma unroll
+        for (int i = 0; i <= D; ++i) {
+            if (sx.rank[i] < -sum) {
+                sx.g[i] = (int)(short)(sx.g[i] + (D + 1));
+                sx.rank[i] += (D + 1) + sum;
+            } else {
+                sx.rank[i] += sum;
+            }
+        }
+    }
+
+    // Barycentric weights (src/Permutohedral.h:351-356).  b[k] receives +delta of the
+    // coordinate ranked d-k and -delta of the one ranked d+1-k; in IEEE arithmetic
+    // both accumulation orders give delta_plus - delta_minus, so the weights are
+    // formed by selection (no dynamically indexed arrays) and stay bit-exact.
+    float delta[D + 1];
+#pragma unroll
+    for (int i = 0; i <= D; ++i) delta[i] = __fmul_rn(__fsub_rn(e[i], (float)sx.g[i]), scale);
+    float top = 0.0f, bottom = 0.0f;   // coordinates ranked d and 0
+#pragma unroll
+    for (int i = 0; i <= D; ++i) {
+        if (sx.rank[i] == D) top = delta[i];
+        if (sx.rank[i] == 0) bottom = delta[i];
+    }
+    // b[0] = delta(rank d) + (1 + b[d+1]),  b[d+1] = -delta(rank 0)
+    sx.bary[0] = __fadd_rn(top, __fadd_rn(1.0f, -bottom));
+#pragma unroll
+    for (int k = 1; k <= D; ++k) {
+        float plus = 0.0f, minus = 0.0f;
+#pragma unroll
+        for (int i = 0; i <= D; ++i) {
+            if (sx.rank[i] == D - k) plus = delta[i];
+            if (sx.rank[i] == D + 1 - k) minus = delta[i];
+        }
+        sx.bary[k] = __fsub_rn(plus, minus);
+    }
+}
+
+// key of remainder r: greedy[i] + canonical[r*(d+1) + rank[i]] (src/Permutohedral.h:367-369),
+// with canonical[r*(d+1)+j] = r for j <= d-r, else r-(d+1) (src/Permutohedral.h:247-254).
+template <int D>
+__device__ __forceinline__ void vertex_coords(const Simplex<D>& sx, int r, int (&k)[D]) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        int c = (sx.rank[i] <= D - r) ? r : r - (D + 1);
+        k[i] = (int)(short)(sx.g[i] + c);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Payload (vertex value storage) conversions.
+// ---------------------------------------------------------------------------------
+template <typename P> struct Payload;
+template <> struct Payload<float> {
+    __device__ static float load(const float* p) { return *p; }
+    __device__ static void store(float* p, float v) { *p = v; }
+};
+template <> struct Payload<double> {
+    __device__ static double load(const double* p) { return *p; }
+    __device__ static void store(double* p, double v) { *p = v; }
+};
+template <> struct Payload<__half> {
+    __device__ static float load(const __half* p) { return __half2float(*p); }
+    __device__ static void store(__half* p, float v) { *p = __float2half_rn(v); }
+};
+template <> struct Payload<__nv_bfloat16> {
+    __device__ static float load(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+    __device__ static void store(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+};
+
+}  // namespace pgpu

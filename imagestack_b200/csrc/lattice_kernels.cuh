@@ -1,0 +1,433 @@
+// Kernels of the permutohedral-lattice Gauss transform (sm_100a).
+//
+// Pipeline for one lattice (one image, or one segment of a batch):
+//   splat      one thread per point: positions from the planar images, elevation and
+//              simplex (src/Permutohedral.h:293-356), d+1 vertex keys, warp-aggregated
+//              insert into the open-addressed table and vector atomics of the weighted
+//              values into the slot's accumulator row; atomicMin of the first touch.
+//   mark       one bit per (point, remainder) entry: the entry that first touched a
+//              vertex gets its bit set.
+//   scan       prefix popcount of that bitmap: the rank of a first-touch entry among
+//              all first touches is the vertex index the reference assigns
+//              (insertion order, src/Permutohedral.h:69-75).
+//   assign     vertex index per slot, compacted keys and values in vertex order.
+//   neighbours two neighbours per vertex and axis (src/Permutohedral.h:446-464).
+//   blur       d+1 passes of [1 2 1]/4 over the compacted vertex list (:466-470).
+//   slice      one thread per output point: the same simplex again, d+1 lookups,
+//              barycentric interpolation (:418-427 / :405-407), optional normalisation
+//              by the homogeneous channel (src/GaussTransform.cpp:673-676).
+#pragma once
+
+#include "lattice_device.cuh"
+
+namespace pgpu {
+
+// A planar float32 image: element (x, y, t, c) at base + c*cstride + t*tstride + y*ystride + x
+// (the addressing of ImageStack's Image, src/Image.h:57-67).
+struct PlanarView {
+    const float* base;
+    long long ystride, tstride, cstride;
+};
+
+// Where the points of a lattice come from.  Point i is pixel (x, y, t) of a
+// width x height x frames grid, i = (t*height + y)*width + x, the loop order of
+// src/GaussTransform.cpp:173-185.  Position channel c (c < pos_channels) is
+// view(c) * pos_scale[c]; then the enabled pixel coordinates follow, each multiplied by
+// its scale (the X()/Y()/T() positions of src/GaussTransform.cpp:657-667).  Values are
+// the val_channels of the value view, then a homogeneous 1 if `homogeneous`.
+struct PointSource {
+    int width, height, frames;
+    PlanarView pos;
+    int pos_channels;
+    float pos_scale[kMaxD];
+    int coord_mask;            // bit 0: x, bit 1: y, bit 2: t
+    float coord_scale[3];
+    PlanarView val;
+    int val_channels;
+    int homogeneous;
+};
+
+struct OutView {
+    float* base;
+    long long ystride, tstride, cstride;
+    int channels;     // channels written
+    int normalize;    // 1: out[c] = acc[c] / acc[vd-1] (JointBilateral), 0: out[c] = acc[c]
+};
+
+struct SplatArgs {
+    PointSource src;
+    uint32_t n;
+    LatticeConsts lc;
+    TableView table;
+    void* vals;        // cap * VDP accumulators (float or double), zeroed
+    uint32_t* ft;      // cap first-touch entries, all ones
+    unsigned* status;
+};
+
+struct CompactArgs {
+    TableView table;
+    const uint32_t* ft;
+    uint32_t* bitmap;      // words covering n*(d+1) entries
+    uint32_t nwords;
+    const uint32_t* offs;  // exclusive prefix popcount per word
+    uint32_t* slot2vtx;
+    uint4* vkey0;          // vertex keys, word 0 ...
+    uint4* vkeyn;          // ... and later words, (KW-1) x vcap
+    uint32_t vcap;
+    const void* tvals;     // slot accumulators
+    void* vvals;           // vertex values (payload type)
+};
+
+struct NbrArgs {
+    TableView table;
+    const uint32_t* slot2vtx;
+    const uint4* vkey0;
+    const uint4* vkeyn;
+    uint32_t vcap;
+    const uint32_t* nverts;
+    int2* nbr;             // (d+1) x vcap pairs
+};
+
+struct BlurArgs {
+    const int2* nbr;       // neighbours of this axis
+    const uint32_t* nverts;
+    const void* src;
+    void* dst;
+};
+
+struct SliceArgs {
+    PointSource src;
+    uint32_t n;
+    LatticeConsts lc;
+    TableView table;
+    const uint32_t* slot2vtx;
+    const void* vvals;
+    int vd;
+    OutView out;
+    int* rec_vtx;          // optional n*(d+1) vertex indices (parity dumps)
+    float* rec_w;          // optional n*(d+1) weights
+    unsigned* status;
+};
+
+// ---------------------------------------------------------------------------------
+// point loading
+// ---------------------------------------------------------------------------------
+template <int D, int VDP>
+__device__ __forceinline__ void load_point(const PointSource& s, uint32_t i, float (&p)[D],
+                                           float (&v)[VDP]) {
+    const uint32_t w = (uint32_t)s.width, h = (uint32_t)s.height;
+    const uint32_t x = i % w;
+    const uint32_t q = i / w;
+    const uint32_t y = q % h;
+    const uint32_t t = q / h;
+    const long long off_p = (long long)t * s.pos.tstride + (long long)y * s.pos.ystride + x;
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        if (k < s.pos_channels) {
+            p[k] = __fmul_rn(__ldg(s.pos.base + off_p + (long long)k * s.pos.cstride), s.pos_scale[k]);
+        }
+    }
+    c = s.pos_channels;
+    if (s.coord_mask & 1) { float f = __fmul_rn((float)x, s.coord_scale[0]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    if (s.coord_mask & 2) { float f = __fmul_rn((float)y, s.coord_scale[1]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    if (s.coord_mask & 4) { float f = __fmul_rn((float)t, s.coord_scale[2]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    const long long off_v = (long long)t * s.val.tstride + (long long)y * s.val.ystride + x;
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) {
+        float f = 0.0f;
+        if (k < s.val_channels) f = __ldg(s.val.base + off_v + (long long)k * s.val.cstride);
+        else if (k == s.val_channels && s.homogeneous) f = 1.0f;
+        v[k] = f;
+    }
+}
+
+template <int D>
+__device__ __forceinline__ void load_position(const PointSource& s, uint32_t i, float (&p)[D]) {
+    const uint32_t w = (uint32_t)s.width, h = (uint32_t)s.height;
+    const uint32_t x = i % w;
+    const uint32_t q = i / w;
+    const uint32_t y = q % h;
+    const uint32_t t = q / h;
+    const long long off_p = (long long)t * s.pos.tstride + (long long)y * s.pos.ystride + x;
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+        if (k < s.pos_channels)
+            p[k] = __fmul_rn(__ldg(s.pos.base + off_p + (long long)k * s.pos.cstride), s.pos_scale[k]);
+    int c = s.pos_channels;
+    if (s.coord_mask & 1) { float f = __fmul_rn((float)x, s.coord_scale[0]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    if (s.coord_mask & 2) { float f = __fmul_rn((float)y, s.coord_scale[1]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    if (s.coord_mask & 4) { float f = __fmul_rn((float)t, s.coord_scale[2]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+}
+
+// ---------------------------------------------------------------------------------
+// accumulator rows
+// ---------------------------------------------------------------------------------
+template <int VDP>
+__device__ __forceinline__ void atomic_add_row(float* dst, const float (&c)[VDP]) {
+    if constexpr (VDP == 2) {
+        atomicAdd(reinterpret_cast<float2*>(dst), make_float2(c[0], c[1]));
+    } else {
+#pragma unroll
+        for (int k = 0; k < VDP; k += 4)
+            atomicAdd(reinterpret_cast<float4*>(dst + k), make_float4(c[k], c[k + 1], c[k + 2], c[k + 3]));
+    }
+}
+template <int VDP>
+__device__ __forceinline__ void atomic_add_row(double* dst, const double (&c)[VDP]) {
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) atomicAdd(dst + k, c[k]);
+}
+
+template <typename Acc> __device__ __forceinline__ Acc acc_mul(float a, float b);
+template <> __device__ __forceinline__ float acc_mul<float>(float a, float b) { return __fmul_rn(a, b); }
+template <> __device__ __forceinline__ double acc_mul<double>(float a, float b) { return (double)a * (double)b; }
+__device__ __forceinline__ float acc_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double acc_add(double a, double b) { return __dadd_rn(a, b); }
+
+// ---------------------------------------------------------------------------------
+// splat
+// ---------------------------------------------------------------------------------
+constexpr int kSplatThreads = 256;
+
+template <int D, int VDP, typename Acc>
+__global__ void __launch_bounds__(kSplatThreads) splat_kernel(SplatArgs a) {
+    constexpr int KW = key_words(D);
+    __shared__ Acc stage[kSplatThreads / 32][32][VDP];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t i = blockIdx.x * (uint32_t)kSplatThreads + threadIdx.x;
+    const bool valid = i < a.n;
+    const unsigned active = __ballot_sync(0xFFFFFFFFu, valid);
+    if (!valid) return;
+
+    float p[D], v[VDP];
+    load_point<D, VDP>(a.src, i, p, v);
+    Simplex<D> sx;
+    compute_simplex<D>(p, a.lc, sx, a.status);
+    const uint32_t e0 = i * (uint32_t)(D + 1);
+    Acc* vals = reinterpret_cast<Acc*>(a.vals);
+
+#pragma unroll
+    for (int r = 0; r <= D; ++r) {
+        int kc[D];
+        vertex_coords<D>(sx, r, kc);
+        Key<KW> key;
+        pack_key<D>(kc, key);
+        unsigned peers = active;
+#pragma unroll
+        for (int w = 0; w < KW; ++w) {
+            peers &= __match_any_sync(active, ((unsigned long long)key.w[w].y << 32) | key.w[w].x);
+            peers &= __match_any_sync(active, ((unsigned long long)key.w[w].w << 32) | key.w[w].z);
+        }
+        const unsigned leader = __ffs(peers) - 1;
+        Acc c[VDP];
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) c[k] = acc_mul<Acc>(sx.bary[r], v[k]);
+        const bool grouped = peers != (1u << lane);
+        if (grouped && lane != leader) {
+#pragma unroll
+            for (int k = 0; k < VDP; ++k) stage[warp][lane][k] = c[k];
+        }
+        __syncwarp(active);
+        if (lane == leader) {
+            unsigned rest = peers & ~(1u << lane);
+            while (rest) {
+                const int src = __ffs(rest) - 1;
+                rest &= rest - 1;
+#pragma unroll
+                for (int k = 0; k < VDP; ++k) c[k] = acc_add(c[k], stage[warp][src][k]);
+            }
+            const int s = table_insert<KW>(a.table, key, key_hash<KW>(key), a.status);
+            if (s >= 0) {
+                atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
+                const uint32_t e = e0 + (uint32_t)r;   // smallest entry of the group
+                if (__ldcg(&a.ft[s]) > e) atomicMin(&a.ft[s], e);
+            }
+        }
+        __syncwarp(active);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// compaction
+// ---------------------------------------------------------------------------------
+__global__ void mark_kernel(const uint32_t* __restrict__ ft, uint32_t cap, uint32_t* bitmap);
+
+// exclusive prefix popcount over the bitmap words, three phases
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;    // words per thread
+__global__ void scan_reduce_kernel(const uint32_t* __restrict__ bitmap, uint32_t nwords,
+                                   uint32_t* partials);
+__global__ void scan_partials_kernel(uint32_t* partials, uint32_t nparts, uint32_t* total);
+__global__ void scan_down_kernel(const uint32_t* __restrict__ bitmap, uint32_t nwords,
+                                 const uint32_t* __restrict__ partials, uint32_t* offs);
+
+template <int KW, int VDP, typename Acc, typename P>
+__global__ void assign_kernel(CompactArgs a) {
+    const Acc* tvals = reinterpret_cast<const Acc*>(a.tvals);
+    P* vvals = reinterpret_cast<P*>(a.vvals);
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.table.cap;
+         s += gridDim.x * blockDim.x) {
+        const uint32_t f = a.ft[s];
+        if (f == 0xFFFFFFFFu) continue;
+        const uint32_t w = f >> 5;
+        const uint32_t vtx = a.offs[w] + __popc(a.bitmap[w] & ((1u << (f & 31u)) - 1u));
+        a.slot2vtx[s] = vtx;
+        a.vkey0[vtx] = a.table.key0[s];
+#pragma unroll
+        for (int k = 1; k < KW; ++k)
+            a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.cap + s];
+#pragma unroll
+        for (int k = 0; k < VDP; ++k)
+            Payload<P>::store(vvals + (size_t)vtx * VDP + k, tvals[(size_t)s * VDP + k]);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// neighbours: n1 = key + 1 except n1[j] = key[j] - d; n2 = key - 1 except n2[j] = key[j] + d
+// (for j == d every stored coordinate moves by one), src/Permutohedral.h:446-451.
+// ---------------------------------------------------------------------------------
+template <int D>
+__global__ void neighbours_kernel(NbrArgs a) {
+    constexpr int KW = key_words(D);
+    const uint32_t m = *a.nverts;
+    for (uint32_t vtx = blockIdx.x * blockDim.x + threadIdx.x; vtx < m;
+         vtx += gridDim.x * blockDim.x) {
+        Key<KW> key;
+        key.w[0] = a.vkey0[vtx];
+#pragma unroll
+        for (int k = 1; k < KW; ++k) key.w[k] = a.vkeyn[(size_t)(k - 1) * a.vcap + vtx];
+        int kc[D];
+        unpack_key<D>(key, kc);
+#pragma unroll 1
+        for (int j = 0; j <= D; ++j) {
+            int n1[D], n2[D];
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                n1[c] = (int)(short)(kc[c] + ((c == j) ? -D : 1));
+                n2[c] = (int)(short)(kc[c] + ((c == j) ? D : -1));
+            }
+            Key<KW> k1, k2;
+            pack_key<D>(n1, k1);
+            pack_key<D>(n2, k2);
+            const int s1 = table_find<KW>(a.table, k1, key_hash<KW>(k1));
+            const int s2 = table_find<KW>(a.table, k2, key_hash<KW>(k2));
+            a.nbr[(size_t)j * a.vcap + vtx] =
+                make_int2(s1 >= 0 ? (int)a.slot2vtx[s1] : -1, s2 >= 0 ? (int)a.slot2vtx[s2] : -1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// blur along one axis: new = 0.25*v(n1) + 0.5*old + 0.25*v(n2), absent neighbour = 0
+// ---------------------------------------------------------------------------------
+template <typename Acc> struct AccOf;   // arithmetic type of a payload
+template <> struct AccOf<float> { using T = float; };
+template <> struct AccOf<__half> { using T = float; };
+template <> struct AccOf<__nv_bfloat16> { using T = float; };
+template <> struct AccOf<double> { using T = double; };
+
+__device__ __forceinline__ float blur3(float a, float b, float c) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(0.25f, a), __fmul_rn(0.5f, b)), __fmul_rn(0.25f, c));
+}
+__device__ __forceinline__ double blur3(double a, double b, double c) {
+    return __dadd_rn(__dadd_rn(0.25 * a, 0.5 * b), 0.25 * c);
+}
+
+template <int VDP, typename P>
+__global__ void blur_kernel(BlurArgs a) {
+    using A = typename AccOf<P>::T;
+    const P* src = reinterpret_cast<const P*>(a.src);
+    P* dst = reinterpret_cast<P*>(a.dst);
+    const uint32_t m = *a.nverts;
+    for (uint32_t vtx = blockIdx.x * blockDim.x + threadIdx.x; vtx < m;
+         vtx += gridDim.x * blockDim.x) {
+        const int2 nb = a.nbr[vtx];
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) {
+            const A x1 = nb.x >= 0 ? (A)Payload<P>::load(src + (size_t)nb.x * VDP + k) : (A)0;
+            const A x2 = nb.y >= 0 ? (A)Payload<P>::load(src + (size_t)nb.y * VDP + k) : (A)0;
+            const A x0 = (A)Payload<P>::load(src + (size_t)vtx * VDP + k);
+            Payload<P>::store(dst + (size_t)vtx * VDP + k, blur3(x1, x0, x2));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// slice
+// ---------------------------------------------------------------------------------
+constexpr int kSliceThreads = 256;
+
+template <int D, int VDP, typename P>
+__global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
+    constexpr int KW = key_words(D);
+    using A = typename AccOf<P>::T;
+    const uint32_t i = blockIdx.x * (uint32_t)kSliceThreads + threadIdx.x;
+    if (i >= a.n) return;
+    float p[D];
+    load_position<D>(a.src, i, p);
+    Simplex<D> sx;
+    compute_simplex<D>(p, a.lc, sx, a.status);
+    const P* vv = reinterpret_cast<const P*>(a.vvals);
+    A acc[VDP];
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) acc[k] = (A)0;
+#pragma unroll
+    for (int r = 0; r <= D; ++r) {
+        int kc[D];
+        vertex_coords<D>(sx, r, kc);
+        Key<KW> key;
+        pack_key<D>(kc, key);
+        const int s = table_find<KW>(a.table, key, key_hash<KW>(key));
+        const int vtx = s >= 0 ? (int)__ldg(a.slot2vtx + s) : -1;
+        const float w = sx.bary[r];
+        if (a.rec_vtx) {
+            a.rec_vtx[(size_t)i * (D + 1) + r] = vtx;
+            a.rec_w[(size_t)i * (D + 1) + r] = w;
+        }
+        if (vtx >= 0) {
+#pragma unroll
+            for (int k = 0; k < VDP; ++k)
+                acc[k] = acc_add(acc[k], (A)w * (A)Payload<P>::load(vv + (size_t)vtx * VDP + k));
+        }
+    }
+    // write
+    const uint32_t wdt = (uint32_t)a.src.width, hgt = (uint32_t)a.src.height;
+    const uint32_t x = i % wdt, q = i / wdt, y = q % hgt, t = q / hgt;
+    float* o = a.out.base + (long long)t * a.out.tstride + (long long)y * a.out.ystride + x;
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) {
+        if (k < a.out.channels) {
+            float r;
+            if (a.out.normalize) {
+                A wsum = acc[0];
+#pragma unroll
+                for (int j = 0; j < VDP; ++j) if (j == a.vd - 1) wsum = acc[j];
+                r = (float)(acc[k] / wsum);
+            } else {
+                r = (float)acc[k];
+            }
+            o[(long long)k * a.out.cstride] = r;
+        }
+    }
+}
+
+}  // namespace pgpu

@@ -1,0 +1,40 @@
+// Launch interface between the host pipeline (engine.cu) and the kernels.
+#pragma once
+
+#include "lattice_kernels.cuh"
+
+namespace pgpu {
+
+enum PayloadKind { kPayloadF32 = 0, kPayloadF16 = 1, kPayloadBF16 = 2, kPayloadF64 = 3 };
+
+inline int payload_bytes(int payload) {
+    return payload == kPayloadF64 ? 8 : payload == kPayloadF32 ? 4 : 2;
+}
+// splat accumulators are FP32, or FP64 for the FP64 lattice
+inline int accum_bytes(int payload) { return payload == kPayloadF64 ? 8 : 4; }
+
+// kernels whose code depends on the number of position dimensions d
+struct DimOps {
+    bool (*splat)(const SplatArgs&, int vdp, int payload, cudaStream_t);
+    void (*neighbours)(const NbrArgs&, uint32_t vmax, int sms, cudaStream_t);
+    bool (*slice)(const SliceArgs&, int vdp, int payload, cudaStream_t);
+};
+
+// one definition per d, in lattice_d.cu compiled once per d
+#define PGPU_DECLARE_DIM(D) const DimOps* dim_ops_##D();
+PGPU_DECLARE_DIM(1) PGPU_DECLARE_DIM(2) PGPU_DECLARE_DIM(3) PGPU_DECLARE_DIM(4)
+PGPU_DECLARE_DIM(5) PGPU_DECLARE_DIM(6) PGPU_DECLARE_DIM(7) PGPU_DECLARE_DIM(8)
+PGPU_DECLARE_DIM(9) PGPU_DECLARE_DIM(10) PGPU_DECLARE_DIM(11) PGPU_DECLARE_DIM(12)
+PGPU_DECLARE_DIM(13) PGPU_DECLARE_DIM(14) PGPU_DECLARE_DIM(15) PGPU_DECLARE_DIM(16)
+#undef PGPU_DECLARE_DIM
+
+const DimOps* dim_ops(int d);
+
+void launch_mark(const uint32_t* ft, uint32_t cap, uint32_t* bitmap, int sms, cudaStream_t st);
+uint32_t scan_parts(uint32_t nwords);
+void launch_scan(const uint32_t* bitmap, uint32_t nwords, uint32_t* partials, uint32_t* offs,
+                 uint32_t* total, cudaStream_t st);
+bool launch_assign(const CompactArgs& a, int kw, int vdp, int payload, int sms, cudaStream_t st);
+bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, int sms, cudaStream_t st);
+
+}  // namespace pgpu

@@ -1,0 +1,128 @@
+/* permgpu.h — C ABI of the B200 (sm_100a) permutohedral-lattice Gauss transform.
+ *
+ * A drop-in GPU replacement for the PERMUTOHEDRAL method of ImageStack's Gauss
+ * transform operations.  Every function takes plain pointers and sizes, returns a
+ * status code (PGPU_OK == 0) and records a message for pgpu_last_error() on failure;
+ * no C++ or CUDA type crosses this boundary.  Calls are synchronous: when one returns,
+ * its output is in the caller's memory.  There is no CPU fallback: without a usable
+ * sm_100 device every compute call fails with PGPU_ERR_NO_DEVICE.
+ *
+ * Memory: image views point at HOST memory (ImageStack images, pageable or pinned) when
+ * options.memory == PGPU_MEM_HOST, or at DEVICE memory when options.memory ==
+ * PGPU_MEM_DEVICE.  The library never frees caller memory; it keeps its own device
+ * workspace (hash table, vertex arrays, staging images) per device and reuses it.
+ */
+#ifndef PERMGPU_H
+#define PERMGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A planar float32 image view: element (x, y, t, c) lives at
+ * base + c*cstride + t*tstride + y*ystride + x.
+ * Mirrors ImageStack::Image (src/Image.h:26-27, element access src/Image.h:57-67);
+ * a fresh Image has ystride = width, tstride = width*height,
+ * cstride = width*height*frames. */
+typedef struct pgpu_image {
+    float *base;
+    int width, height, frames, channels;
+    long long ystride, tstride, cstride;
+} pgpu_image;
+
+/* status codes */
+#define PGPU_OK 0
+#define PGPU_ERR_ARGUMENT 1     /* bad sizes, mismatched images (the reference asserts) */
+#define PGPU_ERR_UNSUPPORTED 2  /* position dimensions > 16 or value channels > 8 */
+#define PGPU_ERR_CUDA 3         /* a CUDA call failed; see pgpu_last_error() */
+#define PGPU_ERR_MEMORY 4       /* device or pinned allocation failed */
+#define PGPU_ERR_CAPACITY 5     /* hash table still overfull after the retries */
+#define PGPU_ERR_NO_DEVICE 7    /* no CUDA device with compute capability 10.x */
+#define PGPU_ERR_ADMISSION 8    /* request larger than the serving memory budget */
+#define PGPU_ERR_TIMEOUT 9      /* a bounded wait ran out */
+
+/* value payload stored in the lattice (splat accumulation is always FP32, or FP64 for
+ * PGPU_PAYLOAD_FP64) */
+#define PGPU_PAYLOAD_FP32 0
+#define PGPU_PAYLOAD_FP16 1
+#define PGPU_PAYLOAD_BF16 2
+#define PGPU_PAYLOAD_FP64 3
+
+#define PGPU_MEM_HOST 0
+#define PGPU_MEM_DEVICE 1
+
+typedef struct pgpu_options {
+    int payload;        /* PGPU_PAYLOAD_* (default FP32, the reference's arithmetic) */
+    int memory;         /* PGPU_MEM_HOST or PGPU_MEM_DEVICE */
+    int device;         /* CUDA device ordinal */
+    void *stream;       /* cudaStream_t for PGPU_MEM_DEVICE calls; NULL: library stream */
+    float load_factor;  /* hash-table target load in (0, 0.9]; 0: default 0.5 */
+    int flags;          /* reserved, 0 */
+} pgpu_options;
+
+typedef struct pgpu_stats {
+    long long points;      /* splatted points */
+    long long vertices;    /* occupied lattice vertices M */
+    long long capacity;    /* hash-table slots used */
+    int d, vd, payload, retries;
+    float ms_splat, ms_compact, ms_neighbours, ms_blur, ms_slice, ms_total;
+} pgpu_stats;
+
+/* Fill *opt with the defaults. */
+void pgpu_default_options(pgpu_options *opt);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *pgpu_last_error(void);
+
+/* Library version, major*10000 + minor*100 + patch. */
+int pgpu_version(void);
+
+/* Number of usable devices (compute capability 10.x); 0 when none. */
+int pgpu_device_count(void);
+
+/* GaussTransform::apply, PERMUTOHEDRAL branch (src/GaussTransform.cpp:115-133, 163-226).
+ * Positions are splat(x,y,t,c) * (1/sigmas[c]); `out` (slice's width, height, frames and
+ * values->channels channels, caller-allocated) receives the un-normalised transform.
+ * When `slice` is NULL or describes exactly the same view as `splat` (the reference's
+ * `slice == splat`, src/GaussTransform.cpp:196), the splat points are sliced; otherwise
+ * the lattice is sliced at the slice positions, where vertices the splat never created
+ * contribute zero (src/Permutohedral.h:405-407). */
+int pgpu_gauss_transform(const pgpu_image *slice, const pgpu_image *splat,
+                         const pgpu_image *values, const float *sigmas, int n_sigmas,
+                         pgpu_image *out, const pgpu_options *opt);
+
+/* JointBilateral::apply with the permutohedral method, in place on `im`
+ * (src/GaussTransform.cpp:504-678): degenerate-axis recursion, positions
+ * (ref*(1/color_sigma), x*(1/filter_width), y*(1/filter_height), t*(1/filter_frames)),
+ * values (im, 1), normalisation by the homogeneous channel. */
+int pgpu_joint_bilateral(pgpu_image *im, const pgpu_image *ref, float filter_width,
+                         float filter_height, float filter_frames, float color_sigma,
+                         const pgpu_options *opt);
+
+/* Bilateral::apply with the permutohedral method (src/GaussTransform.cpp:730-734). */
+int pgpu_bilateral(pgpu_image *im, float filter_width, float filter_height,
+                   float filter_frames, float color_sigma, const pgpu_options *opt);
+
+/* Statistics of the last successful lattice run on this thread. */
+int pgpu_last_stats(pgpu_stats *out);
+
+/* Parity dump of one lattice over n interleaved points (pos n*d already scaled by
+ * 1/sigma, val n*vd), host memory.  Outputs, each optional (NULL to skip):
+ *   *n_vertices              M
+ *   keys        [n*(d+1)*d]  vertex keys in vertex order (reference insertion order)
+ *   replay_vtx  [n*(d+1)]    vertex index per (point, remainder)
+ *   replay_w    [n*(d+1)]    barycentric weight per (point, remainder)
+ *   splat_vals  [n*(d+1)*vd] vertex values after the splat
+ *   blur_vals   [n*(d+1)*vd] vertex values after the blur
+ *   out         [n*vd]       replay slice of the points
+ * Buffers sized for the worst case M = n*(d+1); the first M rows are written.
+ * Mirrors what src/Permutohedral.h computes: keys :365-369, replay :385-390,
+ * values after splat :375-378 and blur :430-488, slice :418-427. */
+int pgpu_lattice_dump(int d, int vd, int n, const float *pos, const float *val, int payload,
+                      int *n_vertices, short *keys, int *replay_vtx, float *replay_w,
+                      float *splat_vals, float *blur_vals, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PERMGPU_H */

@@ -1,0 +1,204 @@
+"""Parity of the CUDA lattice (through the C ABI) with the reference ImageStack.
+
+Bit-exact: lattice keys, the occupied-vertex set in the reference's vertex order, the
+per-point vertex indices and barycentric weights.  Within 1e-5 relative (FP32 payload):
+vertex values after splat and blur and the filtered outputs; the splat's atomics sum in
+a different order than the reference's serial loop, so only these may differ.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden
+from imagestack_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+RTOL_FP32 = 1e-5
+
+
+def rel_err(a, b, floor_frac=1e-6):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    floor = max(np.abs(b).max() * floor_frac, 1e-30)
+    return float((np.abs(a - b) / np.maximum(np.abs(b), floor)).max()) if b.size else 0.0
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def check_dump(d, g, rtol=RTOL_FP32):
+    np.testing.assert_array_equal(d["keys"], g["keys"])
+    np.testing.assert_array_equal(d["replay_vtx"], g["replay_vtx"])
+    np.testing.assert_array_equal(d["replay_w"], g["replay_w"])
+    assert rel_err(d["splat"], g["splat"]) <= rtol
+    assert rel_err(d["blur"], g["blur"]) <= rtol
+    assert rel_err(d["out"], g["out"]) <= rtol
+
+
+@pytest.mark.parametrize("name", ["lattice_rgb_d5", "joint_gray_d3", "lattice_d16"])
+def test_lattice_dump_matches_reference(gpu, name):
+    g = golden(name)
+    check_dump(gpu.lattice_dump(g["pos"], g["val"]), g)
+
+
+def test_bilateral_matches_reference(gpu):
+    g = golden("lattice_rgb_d5")
+    img = g["image"].copy()
+    gpu.Bilateral.apply(img, float(g["sigma_s"]), float(g["sigma_s"]), 0.0, float(g["sigma_r"]))
+    assert rel_err(img, g["bilateral"]) <= RTOL_FP32
+
+
+def test_joint_bilateral_gray_d3_matches_reference(gpu):
+    g = golden("joint_gray_d3")
+    im = g["image"].copy()
+    gpu.JointBilateral.apply(im, g["image"].copy(), 8.0, 8.0, 0.0, 0.1)
+    assert rel_err(im, g["joint"]) <= RTOL_FP32
+
+
+def test_gauss_transform_reference_test_shape(gpu):
+    g = golden("gt_reference_test")
+    out = gpu.GaussTransform.apply(g["slice"], g["splat"], g["values"], list(g["sigmas"]))
+    assert rel_err(out, g["out_distinct"]) <= RTOL_FP32
+    out = gpu.GaussTransform.apply(None, g["splat"], g["values"], list(g["sigmas"]))
+    assert rel_err(out, g["out_same"]) <= RTOL_FP32
+
+
+def test_joint_bilateral_reference_test_shape_d6(gpu):
+    g = golden("jb_reference_test")
+    im = g["image"].copy()
+    gpu.JointBilateral.apply(im, g["reference"], float(g["fw"]), float(g["fh"]), float(g["ft"]),
+                             float(g["cs"]))
+    assert rel_err(im, g["out"]) <= RTOL_FP32
+
+
+def config1_points():
+    rgb = synth.image(512, 512, 3, rects=16, seed=606)
+    h, w = 512, 512
+    p = np.empty((h, w, 5), np.float32)
+    p[:, :, 0] = np.arange(w, dtype=np.float32)[None, :] * (np.float32(1) / np.float32(8))
+    p[:, :, 1] = np.arange(h, dtype=np.float32)[:, None] * (np.float32(1) / np.float32(8))
+    for k in range(3):
+        p[:, :, 2 + k] = rgb[k] * (np.float32(1) / np.float32(0.1))
+    v = np.concatenate([rgb.transpose(1, 2, 0), np.ones((h, w, 1), np.float32)], 2)
+    return p.reshape(-1, 5), v.reshape(-1, 4).astype(np.float32)
+
+
+def test_config1_512_bit_exact_keys_and_replay(gpu):
+    g = golden("gt_config1_512")
+    p, v = config1_points()
+    d = gpu.lattice_dump(p, v)
+    assert d["keys"].shape[0] == int(g["vertices"])
+    assert sha(d["keys"]) == str(g["keys_sha256"])
+    assert sha(d["replay_vtx"]) == str(g["replay_vtx_sha256"])
+    assert sha(d["replay_w"]) == str(g["replay_w_sha256"])
+    assert rel_err(d["out"][g["rows"]], g["out_rows"]) <= RTOL_FP32
+    # a checksum of checksums: per-channel sums of the vertex values
+    np.testing.assert_allclose(d["splat"].astype(np.float64).sum(0), g["sum_splat"], rtol=1e-5)
+    np.testing.assert_allclose(d["blur"].astype(np.float64).sum(0), g["sum_blur"], rtol=1e-5)
+
+
+def test_runs_are_deterministic_in_keys(gpu):
+    p, v = config1_points()
+    a = gpu.lattice_dump(p[:50000], v[:50000])
+    b = gpu.lattice_dump(p[:50000], v[:50000])
+    np.testing.assert_array_equal(a["keys"], b["keys"])
+    np.testing.assert_array_equal(a["replay_vtx"], b["replay_vtx"])
+
+
+def test_device_memory_path_matches_host(gpu):
+    import torch
+    img = synth.image(300, 200, 3, rects=10, seed=7)
+    host = img.copy()
+    gpu.Bilateral.apply(host, 6.0, 6.0, 0.0, 0.12)
+    dev = torch.from_numpy(img.copy()).cuda()
+    gpu.Bilateral.apply(dev, 6.0, 6.0, 0.0, 0.12)
+    torch.cuda.synchronize()
+    assert rel_err(dev.cpu().numpy(), host) <= RTOL_FP32
+
+
+def test_strided_region_views(gpu):
+    """A region of a larger image (the reference's Image views share the payload)."""
+    big = synth.image(160, 120, 4, rects=6, seed=8)
+    sub = big[:3, 10:90, 20:140]
+    expect = np.ascontiguousarray(sub).copy()
+    gpu.Bilateral.apply(expect, 5.0, 5.0, 0.0, 0.1)
+    work = big.copy()
+    gpu.Bilateral.apply(work[:3, 10:90, 20:140], 5.0, 5.0, 0.0, 0.1)
+    assert rel_err(work[:3, 10:90, 20:140], expect) <= RTOL_FP32
+    np.testing.assert_array_equal(work[3], big[3])            # untouched channel
+    np.testing.assert_array_equal(work[:3, :10], big[:3, :10])  # untouched rows
+
+
+@pytest.mark.parametrize("shape,fw,fh", [
+    ((3, 1, 1), 4.0, 4.0),      # one pixel
+    ((3, 1, 37), 4.0, 4.0),     # one row: the height axis drops out
+    ((3, 29, 1), 4.0, 4.0),     # one column
+    ((3, 12, 17), 0.0, 3.0),    # filter width 0: each column independently
+    ((3, 12, 17), 3.0, 0.0),    # filter height 0: each row independently
+    ((3, 20, 30), 500.0, 3.0),  # sigma > 10 x width: x is not a position
+])
+def test_degenerate_axes_match_reference_rules(gpu, shape, fw, fh):
+    img = synth.image(shape[2], shape[1], shape[0], rects=2, seed=9)
+    ours = img.copy()
+    gpu.JointBilateral.apply(ours, img.copy(), fw, fh, 0.0, 0.2)
+    if oracle.reference_available():
+        ref, _ = oracle.reference_joint_bilateral(img, img, fw, 0.2, sigma_s_y=fh)
+        assert rel_err(ours, ref) <= RTOL_FP32
+    assert np.isfinite(ours).all()
+
+
+def test_errors_are_reported(gpu):
+    img = np.zeros((3, 8, 8), np.float32)
+    with pytest.raises(gpu.PgpuError) as e:
+        gpu.JointBilateral.apply(img, np.zeros((3, 8, 9), np.float32), 2.0, 2.0, 0.0, 0.1)
+    assert e.value.code == gpu.ERR_ARGUMENT
+    with pytest.raises(gpu.PgpuError) as e:
+        gpu.GaussTransform.apply(None, np.zeros((17, 1, 4, 4), np.float32),
+                                 np.ones((2, 1, 4, 4), np.float32), [1.0] * 17)
+    assert e.value.code == gpu.ERR_UNSUPPORTED
+    with pytest.raises(gpu.PgpuError) as e:   # keys would leave the int16 range
+        gpu.GaussTransform.apply(None, np.full((3, 1, 4, 4), 1e6, np.float32),
+                                 np.ones((2, 1, 4, 4), np.float32), [1.0] * 3)
+    assert e.value.code == gpu.ERR_ARGUMENT
+
+
+def test_full_size_4k_bit_exact_vs_oracle(gpu):
+    """3840x2160 RGB, sigma_s 16, sigma_r 0.1: the whole vertex set and output."""
+    img = synth.image(3840, 2160, 3, rects=64, seed=2)
+    pos, val = oracle.bilateral_points(img, img, 16.0, 0.1)
+    ref = oracle.oracle_lattice(pos, val)
+    d = gpu.lattice_dump(pos, val)
+    assert d["keys"].shape == ref.keys.shape
+    assert sha(d["keys"]) == sha(ref.keys)
+    assert sha(d["replay_vtx"]) == sha(ref.replay_vtx)
+    assert sha(d["replay_w"]) == sha(ref.replay_w)
+    assert rel_err(d["out"], ref.out) <= RTOL_FP32
+    out = img.copy()
+    gpu.Bilateral.apply(out, 16.0, 16.0, 0.0, 0.1)
+    norm = (ref.out[:, :3] / ref.out[:, 3:4]).reshape(2160, 3840, 3).transpose(2, 0, 1)
+    assert rel_err(out, norm) <= RTOL_FP32
+
+
+def test_fp64_payload_matches_fp64_oracle(gpu):
+    g = golden("lattice_rgb_d5")
+    d = gpu.lattice_dump(g["pos"], g["val"], payload="fp64")
+    ref = oracle.oracle_lattice(g["pos"], g["val"], fp64=True)
+    np.testing.assert_array_equal(d["keys"], ref.keys)
+    # outputs are returned as float32
+    assert rel_err(d["out"], ref.out) <= 1e-6
+
+
+@pytest.mark.parametrize("payload,tol", [("fp16", 1e-3), ("bf16", 1e-2)])
+def test_low_precision_payload_error_vs_fp64(gpu, payload, tol):
+    img = synth.image(512, 512, 3, rects=16, seed=11)
+    ref = img.copy()
+    gpu.Bilateral.apply(ref, 8.0, 8.0, 0.0, 0.1, payload="fp64")
+    out = img.copy()
+    gpu.Bilateral.apply(out, 8.0, 8.0, 0.0, 0.1, payload=payload)
+    err = rel_err(out, ref, floor_frac=1e-2)
+    print(payload, "max relative error vs FP64 lattice:", err)
+    assert err <= tol
