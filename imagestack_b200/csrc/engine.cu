@@ -154,6 +154,9 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
     const float load = (J.load > 0.05f && J.load <= 0.9f) ? J.load : 0.5f;
     const LatticeConsts lc = make_consts(d);
     const size_t accb = accum_bytes(J.payload), payb = payload_bytes(J.payload);
+    // 16-bit payloads of a lattice whose last value channel is the homogeneous weight store
+    // rows normalised by that weight (see assign_kernel)
+    const bool homog = J.homog && (J.payload == kPayloadF16 || J.payload == kPayloadBF16);
 
     double ratio = 1.0;
     {
@@ -178,7 +181,8 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
             (rc = E.partials.ensure((size_t)scan_parts(nwords) * 4 + 16)) ||
             (rc = E.vkey0.ensure(cap * 16)) || (rc = E.vkeyn.ensure((kw - 1) * cap * 16)) ||
             (rc = E.vv0.ensure(cap * vdp * payb)) || (rc = E.vv1.ensure(cap * vdp * payb)) ||
-            (rc = E.nbr.ensure((size_t)(d + 1) * cap * 8)) || (rc = E.dstat.ensure(64)))
+            (rc = E.nbr.ensure((size_t)(d + 1) * cap * 8)) || (rc = E.dstat.ensure(64)) ||
+            (homog && (rc = E.vf32.ensure(cap * vdp * 4))))
             return rc;
 
         unsigned* dstatus = (unsigned*)E.dstat.p;
@@ -217,8 +221,10 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
         ca.vkeyn = (uint4*)E.vkeyn.p;
         ca.vcap = (uint32_t)cap;
         ca.tvals = E.tvals.p;
-        ca.vvals = E.vv0.p;
-        if (!launch_assign(ca, kw, vdp, J.payload, E.sms, st)) return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
+        ca.vvals = homog ? E.vf32.p : E.vv0.p;
+        ca.wc = vd - 1;
+        if (!launch_assign(ca, kw, vdp, J.payload, homog, E.sms, st))
+            return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
         CUDA_TRY(cudaGetLastError());
         if (J.dump_splat)
             CUDA_TRY(cudaMemcpyAsync(J.dump_splat, E.vv0.p, std::min<size_t>(cap * vdp * payb, J.dump_bytes),
@@ -242,9 +248,11 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
             BlurArgs ba;
             ba.nbr = (const int2*)E.nbr.p + (size_t)j * cap;
             ba.nverts = dM;
-            ba.src = bufs[j & 1];
+            ba.src = (homog && j == 0) ? E.vf32.p : bufs[j & 1];
+            ba.wc = vd - 1;
             ba.dst = bufs[(j + 1) & 1];
-            if (!launch_blur(ba, (uint32_t)cap, vdp, J.payload, E.sms, st)) return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
+            if (!launch_blur(ba, (uint32_t)cap, vdp, J.payload, homog, homog && j == 0, E.sms, st))
+                return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
         }
         CUDA_TRY(cudaGetLastError());
         void* final_vals = bufs[(d + 1) & 1];
@@ -265,7 +273,7 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
         sl.rec_vtx = J.rec_vtx;
         sl.rec_w = J.rec_w;
         sl.status = dstatus;
-        if (!ops->slice(sl, vdp, J.payload, st)) return fail(PGPU_ERR_UNSUPPORTED, "slice variant");
+        if (!ops->slice(sl, vdp, J.payload, homog, st)) return fail(PGPU_ERR_UNSUPPORTED, "slice variant");
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaEventRecord(E.ev[5], st));
         CUDA_TRY(cudaMemcpyAsync(E.hstat, E.dstat.p, 16, cudaMemcpyDeviceToHost, st));
@@ -507,6 +515,7 @@ int joint_bilateral_device(Engine& E, const pgpu_image& im, const pgpu_image& re
     s.val = planar(im);
     s.val_channels = im.channels;
     s.homogeneous = 1;
+    J.homog = true;
     J.replay = true;
     J.out = outview(im, im.channels, 1);
     return run_lattice(E, J, st);
@@ -696,7 +705,12 @@ int pgpu_lattice_dump(int d, int vd, int n, const float* pos, const float* val, 
     rc = run_lattice(E, J, st);
     if (rc) return rc;
     if (n_vertices) *n_vertices = (int)M;
-    if (out) CUDA_TRY(cudaMemcpy(out, bo.p, (size_t)n * vd * 4, cudaMemcpyDeviceToHost));
+    if (out) {   // the slice wrote channel-major; the dump is point-major
+        std::vector<float> planar_out((size_t)n * vd);
+        CUDA_TRY(cudaMemcpy(planar_out.data(), bo.p, planar_out.size() * 4, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < vd; ++c) out[(size_t)i * vd + c] = planar_out[(size_t)c * n + i];
+    }
     if (replay_vtx) CUDA_TRY(cudaMemcpy(replay_vtx, brv.p, rows * 4, cudaMemcpyDeviceToHost));
     if (replay_w) CUDA_TRY(cudaMemcpy(replay_w, brw.p, rows * 4, cudaMemcpyDeviceToHost));
     const int kw = key_words(d);

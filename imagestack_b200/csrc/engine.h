@@ -46,6 +46,7 @@ struct Engine {
     DevBuf bitmap, offs, partials;
     // vertex space
     DevBuf vkey0, vkeyn, vv0, vv1, nbr;
+    DevBuf vf32;   // FP32 normalised rows feeding the first blur pass (16-bit homogeneous)
     DevBuf dstat;
     // staging images for host-memory calls
     DevBuf img_a, img_b, img_c, img_d;
@@ -74,6 +75,7 @@ struct LatticeJob {
     void* dump_blur = nullptr;    // ... and after the blur
     size_t dump_bytes = 0;
     uint32_t* vertices_out = nullptr;
+    bool homog = false;   // the last value channel is the homogeneous weight
 };
 
 LatticeConsts make_consts(int d);

@@ -143,62 +143,82 @@ void launch_scan(const uint32_t* bitmap, uint32_t nwords, uint32_t* partials, ui
     scan_down_kernel<<<parts, kScanThreads, 0, st>>>(bitmap, nwords, partials, offs);
 }
 
-template <int KW, int VDP, typename Acc, typename P>
+template <int KW, int VDP, typename Acc, typename P, bool HOMOG>
 static void assign_t(const CompactArgs& a, int sms, cudaStream_t st) {
-    assign_kernel<KW, VDP, Acc, P><<<grid_for(a.table.cap, 256, sms), 256, 0, st>>>(a);
+    assign_kernel<KW, VDP, Acc, P, HOMOG><<<grid_for(a.table.cap, 256, sms), 256, 0, st>>>(a);
 }
 
 template <int KW, int VDP>
-static bool assign_p(const CompactArgs& a, int payload, int sms, cudaStream_t st) {
+static bool assign_p(const CompactArgs& a, int payload, bool homog, int sms, cudaStream_t st) {
+    if (homog) {   // 16-bit homogeneous lattices: FP32 normalised rows for the first blur pass
+        if (payload != kPayloadF16 && payload != kPayloadBF16) return false;
+        assign_t<KW, VDP, float, float, true>(a, sms, st);
+        return true;
+    }
     switch (payload) {
-    case kPayloadF32: assign_t<KW, VDP, float, float>(a, sms, st); return true;
-    case kPayloadF16: assign_t<KW, VDP, float, __half>(a, sms, st); return true;
-    case kPayloadBF16: assign_t<KW, VDP, float, __nv_bfloat16>(a, sms, st); return true;
-    case kPayloadF64: assign_t<KW, VDP, double, double>(a, sms, st); return true;
+    case kPayloadF32: assign_t<KW, VDP, float, float, false>(a, sms, st); return true;
+    case kPayloadF16: assign_t<KW, VDP, float, __half, false>(a, sms, st); return true;
+    case kPayloadBF16: assign_t<KW, VDP, float, __nv_bfloat16, false>(a, sms, st); return true;
+    case kPayloadF64: assign_t<KW, VDP, double, double, false>(a, sms, st); return true;
     }
     return false;
 }
 
 template <int KW>
-static bool assign_v(const CompactArgs& a, int vdp, int payload, int sms, cudaStream_t st) {
+static bool assign_v(const CompactArgs& a, int vdp, int payload, bool homog, int sms,
+                     cudaStream_t st) {
     switch (vdp) {
-    case 2: return assign_p<KW, 2>(a, payload, sms, st);
-    case 4: return assign_p<KW, 4>(a, payload, sms, st);
-    case 8: return assign_p<KW, 8>(a, payload, sms, st);
+    case 2: return assign_p<KW, 2>(a, payload, homog, sms, st);
+    case 4: return assign_p<KW, 4>(a, payload, homog, sms, st);
+    case 8: return assign_p<KW, 8>(a, payload, homog, sms, st);
     }
     return false;
 }
 
-bool launch_assign(const CompactArgs& a, int kw, int vdp, int payload, int sms, cudaStream_t st) {
+bool launch_assign(const CompactArgs& a, int kw, int vdp, int payload, bool homog, int sms,
+                   cudaStream_t st) {
     switch (kw) {
-    case 1: return assign_v<1>(a, vdp, payload, sms, st);
-    case 2: return assign_v<2>(a, vdp, payload, sms, st);
-    case 3: return assign_v<3>(a, vdp, payload, sms, st);
+    case 1: return assign_v<1>(a, vdp, payload, homog, sms, st);
+    case 2: return assign_v<2>(a, vdp, payload, homog, sms, st);
+    case 3: return assign_v<3>(a, vdp, payload, homog, sms, st);
     }
     return false;
+}
+
+template <int VDP, typename PS, typename PD, bool HOMOG>
+static void blur_t(const BlurArgs& a, uint32_t vmax, int sms, cudaStream_t st) {
+    blur_kernel<VDP, PS, PD, HOMOG><<<grid_for(vmax, 256, sms), 256, 0, st>>>(a);
 }
 
 template <int VDP, typename P>
-static void blur_t(const BlurArgs& a, uint32_t vmax, int sms, cudaStream_t st) {
-    blur_kernel<VDP, P><<<grid_for(vmax, 256, sms), 256, 0, st>>>(a);
+static void blur_homog(const BlurArgs& a, uint32_t vmax, bool from_f32, int sms, cudaStream_t st) {
+    if (from_f32) blur_t<VDP, float, P, true>(a, vmax, sms, st);
+    else blur_t<VDP, P, P, true>(a, vmax, sms, st);
 }
 
 template <int VDP>
-static bool blur_p(const BlurArgs& a, uint32_t vmax, int payload, int sms, cudaStream_t st) {
+static bool blur_p(const BlurArgs& a, uint32_t vmax, int payload, bool homog, bool from_f32,
+                   int sms, cudaStream_t st) {
+    if (homog) {
+        if (payload == kPayloadF16) { blur_homog<VDP, __half>(a, vmax, from_f32, sms, st); return true; }
+        if (payload == kPayloadBF16) { blur_homog<VDP, __nv_bfloat16>(a, vmax, from_f32, sms, st); return true; }
+        return false;
+    }
     switch (payload) {
-    case kPayloadF32: blur_t<VDP, float>(a, vmax, sms, st); return true;
-    case kPayloadF16: blur_t<VDP, __half>(a, vmax, sms, st); return true;
-    case kPayloadBF16: blur_t<VDP, __nv_bfloat16>(a, vmax, sms, st); return true;
-    case kPayloadF64: blur_t<VDP, double>(a, vmax, sms, st); return true;
+    case kPayloadF32: blur_t<VDP, float, float, false>(a, vmax, sms, st); return true;
+    case kPayloadF16: blur_t<VDP, __half, __half, false>(a, vmax, sms, st); return true;
+    case kPayloadBF16: blur_t<VDP, __nv_bfloat16, __nv_bfloat16, false>(a, vmax, sms, st); return true;
+    case kPayloadF64: blur_t<VDP, double, double, false>(a, vmax, sms, st); return true;
     }
     return false;
 }
 
-bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, int sms, cudaStream_t st) {
+bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, bool homog,
+                 bool from_f32, int sms, cudaStream_t st) {
     switch (vdp) {
-    case 2: return blur_p<2>(a, vmax, payload, sms, st);
-    case 4: return blur_p<4>(a, vmax, payload, sms, st);
-    case 8: return blur_p<8>(a, vmax, payload, sms, st);
+    case 2: return blur_p<2>(a, vmax, payload, homog, from_f32, sms, st);
+    case 4: return blur_p<4>(a, vmax, payload, homog, from_f32, sms, st);
+    case 8: return blur_p<8>(a, vmax, payload, homog, from_f32, sms, st);
     }
     return false;
 }

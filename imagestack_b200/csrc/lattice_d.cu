@@ -40,28 +40,33 @@ void neighbours(const NbrArgs& a, uint32_t vmax, int sms, cudaStream_t st) {
     neighbours_kernel<D><<<grid_cap(vmax, 256, sms), 256, 0, st>>>(a);
 }
 
-template <int VDP, typename P>
+template <int VDP, typename P, bool HOMOG>
 void slice_t(const SliceArgs& a, cudaStream_t st) {
     const uint32_t blocks = (a.n + kSliceThreads - 1) / kSliceThreads;
-    if (blocks) slice_kernel<D, VDP, P><<<blocks, kSliceThreads, 0, st>>>(a);
+    if (blocks) slice_kernel<D, VDP, P, HOMOG><<<blocks, kSliceThreads, 0, st>>>(a);
 }
 
+// homogeneous rows exist only for the 16-bit payloads
 template <int VDP>
-bool slice_p(const SliceArgs& a, int payload, cudaStream_t st) {
+bool slice_p(const SliceArgs& a, int payload, bool homog, cudaStream_t st) {
     switch (payload) {
-    case kPayloadF32: slice_t<VDP, float>(a, st); return true;
-    case kPayloadF16: slice_t<VDP, __half>(a, st); return true;
-    case kPayloadBF16: slice_t<VDP, __nv_bfloat16>(a, st); return true;
-    case kPayloadF64: slice_t<VDP, double>(a, st); return true;
+    case kPayloadF32: slice_t<VDP, float, false>(a, st); return !homog;
+    case kPayloadF16:
+        homog ? slice_t<VDP, __half, true>(a, st) : slice_t<VDP, __half, false>(a, st);
+        return true;
+    case kPayloadBF16:
+        homog ? slice_t<VDP, __nv_bfloat16, true>(a, st) : slice_t<VDP, __nv_bfloat16, false>(a, st);
+        return true;
+    case kPayloadF64: slice_t<VDP, double, false>(a, st); return !homog;
     }
     return false;
 }
 
-bool slice(const SliceArgs& a, int vdp, int payload, cudaStream_t st) {
+bool slice(const SliceArgs& a, int vdp, int payload, bool homog, cudaStream_t st) {
     switch (vdp) {
-    case 2: return slice_p<2>(a, payload, st);
-    case 4: return slice_p<4>(a, payload, st);
-    case 8: return slice_p<8>(a, payload, st);
+    case 2: return slice_p<2>(a, payload, homog, st);
+    case 4: return slice_p<4>(a, payload, homog, st);
+    case 8: return slice_p<8>(a, payload, homog, st);
     }
     return false;
 }

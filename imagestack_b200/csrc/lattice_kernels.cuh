@@ -76,6 +76,7 @@ struct CompactArgs {
     uint32_t vcap;
     const void* tvals;     // slot accumulators
     void* vvals;           // vertex values (payload type)
+    int wc;                // homogeneous weight channel (homogeneous rows only)
 };
 
 struct NbrArgs {
@@ -93,6 +94,7 @@ struct BlurArgs {
     const uint32_t* nverts;
     const void* src;
     void* dst;
+    int wc;                // homogeneous weight channel (homogeneous rows only)
 };
 
 struct SliceArgs {
@@ -280,10 +282,38 @@ __global__ void scan_partials_kernel(uint32_t* partials, uint32_t nparts, uint32
 __global__ void scan_down_kernel(const uint32_t* __restrict__ bitmap, uint32_t nwords,
                                  const uint32_t* __restrict__ partials, uint32_t* offs);
 
-template <int KW, int VDP, typename Acc, typename P>
+// HOMOG: the last value channel (index wc) is the homogeneous weight w; the vertex row is
+// stored as (v_0/w, ..., v_{wc-1}/w, w) — homogeneous coordinates normalised by their own
+// weight.  A filtered value is then a convex combination of stored values, so a 16-bit
+// payload's rounding of w enters the normalised output only at second order.
+template <int KW, int VDP, typename Acc, typename P, bool HOMOG>
 __global__ void assign_kernel(CompactArgs a) {
     const Acc* tvals = reinterpret_cast<const Acc*>(a.tvals);
     P* vvals = reinterpret_cast<P*>(a.vvals);
+    if constexpr (HOMOG) {
+        for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.table.cap;
+             s += gridDim.x * blockDim.x) {
+            const uint32_t f = a.ft[s];
+            if (f == 0xFFFFFFFFu) continue;
+            const uint32_t w = f >> 5;
+            const uint32_t vtx = a.offs[w] + __popc(a.bitmap[w] & ((1u << (f & 31u)) - 1u));
+            a.slot2vtx[s] = vtx;
+            a.vkey0[vtx] = a.table.key0[s];
+#pragma unroll
+            for (int k = 1; k < KW; ++k)
+                a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.cap + s];
+            Acc wt = tvals[(size_t)s * VDP];
+#pragma unroll
+            for (int k = 0; k < VDP; ++k) if (k == a.wc) wt = tvals[(size_t)s * VDP + k];
+#pragma unroll
+            for (int k = 0; k < VDP; ++k) {
+                const Acc t = tvals[(size_t)s * VDP + k];
+                const Acc m = (k == a.wc) ? wt : (k < a.wc && wt != (Acc)0) ? t / wt : (Acc)0;
+                Payload<P>::store(vvals + (size_t)vtx * VDP + k, m);
+            }
+        }
+        return;
+    }
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.table.cap;
          s += gridDim.x * blockDim.x) {
         const uint32_t f = a.ft[s];
@@ -352,21 +382,49 @@ __device__ __forceinline__ double blur3(double a, double b, double c) {
     return __dadd_rn(__dadd_rn(0.25 * a, 0.5 * b), 0.25 * c);
 }
 
-template <int VDP, typename P>
+// PS/PD: payload read / written (they differ only for the first pass of a homogeneous
+// 16-bit lattice, which reads the FP32 rows written by the compaction).
+template <int VDP, typename PS, typename PD, bool HOMOG>
 __global__ void blur_kernel(BlurArgs a) {
-    using A = typename AccOf<P>::T;
-    const P* src = reinterpret_cast<const P*>(a.src);
-    P* dst = reinterpret_cast<P*>(a.dst);
+    using A = typename AccOf<PD>::T;
+    const PS* src = reinterpret_cast<const PS*>(a.src);
+    PD* dst = reinterpret_cast<PD*>(a.dst);
     const uint32_t m = *a.nverts;
     for (uint32_t vtx = blockIdx.x * blockDim.x + threadIdx.x; vtx < m;
          vtx += gridDim.x * blockDim.x) {
         const int2 nb = a.nbr[vtx];
+        if constexpr (HOMOG) {
+            // rows hold (m_0..m_{wc-1}, w): blur w and the products w*m, renormalise
+            A r1[VDP], r0[VDP], r2[VDP];
+#pragma unroll
+            for (int k = 0; k < VDP; ++k) {
+                r1[k] = nb.x >= 0 ? (A)Payload<PS>::load(src + (size_t)nb.x * VDP + k) : (A)0;
+                r2[k] = nb.y >= 0 ? (A)Payload<PS>::load(src + (size_t)nb.y * VDP + k) : (A)0;
+                r0[k] = (A)Payload<PS>::load(src + (size_t)vtx * VDP + k);
+            }
+            A w1 = r1[0], w0 = r0[0], w2 = r2[0];
+#pragma unroll
+            for (int k = 0; k < VDP; ++k)
+                if (k == a.wc) { w1 = r1[k]; w0 = r0[k]; w2 = r2[k]; }
+            const A nw = blur3(w1, w0, w2);
+#pragma unroll
+            for (int k = 0; k < VDP; ++k) {
+                A out;
+                if (k == a.wc) out = nw;
+                else if (k < a.wc && nw != (A)0) out = blur3(w1 * r1[k], w0 * r0[k], w2 * r2[k]) / nw;
+                else out = (A)0;
+                Payload<PD>::store(dst + (size_t)vtx * VDP + k, out);
+            }
+            continue;
+        }
+        const PS* srcp = src;
+        PD* dstp = dst;
 #pragma unroll
         for (int k = 0; k < VDP; ++k) {
-            const A x1 = nb.x >= 0 ? (A)Payload<P>::load(src + (size_t)nb.x * VDP + k) : (A)0;
-            const A x2 = nb.y >= 0 ? (A)Payload<P>::load(src + (size_t)nb.y * VDP + k) : (A)0;
-            const A x0 = (A)Payload<P>::load(src + (size_t)vtx * VDP + k);
-            Payload<P>::store(dst + (size_t)vtx * VDP + k, blur3(x1, x0, x2));
+            const A x1 = nb.x >= 0 ? (A)Payload<PS>::load(srcp + (size_t)nb.x * VDP + k) : (A)0;
+            const A x2 = nb.y >= 0 ? (A)Payload<PS>::load(srcp + (size_t)nb.y * VDP + k) : (A)0;
+            const A x0 = (A)Payload<PS>::load(srcp + (size_t)vtx * VDP + k);
+            Payload<PD>::store(dstp + (size_t)vtx * VDP + k, blur3(x1, x0, x2));
         }
     }
 }
@@ -376,12 +434,15 @@ __global__ void blur_kernel(BlurArgs a) {
 // ---------------------------------------------------------------------------------
 constexpr int kSliceThreads = 256;
 
-template <int D, int VDP, typename P>
+template <int D, int VDP, typename P, bool HOMOG>
 __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
     constexpr int KW = key_words(D);
     using A = typename AccOf<P>::T;
     const uint32_t i = blockIdx.x * (uint32_t)kSliceThreads + threadIdx.x;
     if (i >= a.n) return;
+    // A splat that overflowed the table is rerun by the host with more slots; its
+    // output may be the caller's input image (in-place filtering), so write nothing.
+    if (__ldcg(a.status) & (kStatusProbeLimit | kStatusSpinLimit | kStatusKeyRange)) return;
     float p[D];
     load_position<D>(a.src, i, p);
     Simplex<D> sx;
@@ -404,9 +465,22 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
             a.rec_w[(size_t)i * (D + 1) + r] = w;
         }
         if (vtx >= 0) {
+            if constexpr (HOMOG) {   // row (m_0.., w): accumulate (w*m_k, w)
+                A row[VDP];
 #pragma unroll
-            for (int k = 0; k < VDP; ++k)
-                acc[k] = acc_add(acc[k], (A)w * (A)Payload<P>::load(vv + (size_t)vtx * VDP + k));
+                for (int k = 0; k < VDP; ++k) row[k] = (A)Payload<P>::load(vv + (size_t)vtx * VDP + k);
+                A wt = row[0];
+#pragma unroll
+                for (int k = 0; k < VDP; ++k) if (k == a.vd - 1) wt = row[k];
+                const A bw = (A)w * wt;
+#pragma unroll
+                for (int k = 0; k < VDP; ++k)
+                    acc[k] = acc_add(acc[k], (k == a.vd - 1) ? bw : bw * row[k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < VDP; ++k)
+                    acc[k] = acc_add(acc[k], (A)w * (A)Payload<P>::load(vv + (size_t)vtx * VDP + k));
+            }
         }
     }
     // write

@@ -17,7 +17,7 @@ inline int accum_bytes(int payload) { return payload == kPayloadF64 ? 8 : 4; }
 struct DimOps {
     bool (*splat)(const SplatArgs&, int vdp, int payload, cudaStream_t);
     void (*neighbours)(const NbrArgs&, uint32_t vmax, int sms, cudaStream_t);
-    bool (*slice)(const SliceArgs&, int vdp, int payload, cudaStream_t);
+    bool (*slice)(const SliceArgs&, int vdp, int payload, bool homog, cudaStream_t);
 };
 
 // one definition per d, in lattice_d.cu compiled once per d
@@ -34,7 +34,11 @@ void launch_mark(const uint32_t* ft, uint32_t cap, uint32_t* bitmap, int sms, cu
 uint32_t scan_parts(uint32_t nwords);
 void launch_scan(const uint32_t* bitmap, uint32_t nwords, uint32_t* partials, uint32_t* offs,
                  uint32_t* total, cudaStream_t st);
-bool launch_assign(const CompactArgs& a, int kw, int vdp, int payload, int sms, cudaStream_t st);
-bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, int sms, cudaStream_t st);
+// homog: rows normalised by the homogeneous weight, written as FP32 for the first blur pass
+bool launch_assign(const CompactArgs& a, int kw, int vdp, int payload, bool homog, int sms,
+                   cudaStream_t st);
+// homog + from_f32: the first pass of a homogeneous 16-bit lattice reads FP32 rows
+bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, bool homog,
+                 bool from_f32, int sms, cudaStream_t st);
 
 }  // namespace pgpu

@@ -151,6 +151,23 @@ def test_degenerate_axes_match_reference_rules(gpu, shape, fw, fh):
     assert np.isfinite(ours).all()
 
 
+def test_overfull_table_retry_keeps_input_intact(gpu):
+    """A smooth frame teaches the engine a small vertex-per-pixel ratio; the next, noisy
+    frame with the same d overflows the first table and is rerun with more slots.  The
+    in-place output must equal a clean run's."""
+    flat = np.full((3, 64, 64), 0.5, np.float32)
+    gpu.Bilateral.apply(flat, 16.0, 16.0, 0.0, 0.5)
+    rng = np.random.default_rng(5)
+    noisy = rng.random((3, 64, 64), dtype=np.float32)
+    out = noisy.copy()
+    gpu.Bilateral.apply(out, 1.0, 1.0, 0.0, 0.02)
+    assert gpu.last_stats()["retries"] >= 1
+    pos, val = oracle.bilateral_points(noisy, noisy, 1.0, 0.02)
+    ref = oracle.oracle_lattice(pos, val)
+    norm = (ref.out[:, :3] / ref.out[:, 3:4]).reshape(64, 64, 3).transpose(2, 0, 1)
+    assert rel_err(out, norm) <= RTOL_FP32
+
+
 def test_errors_are_reported(gpu):
     img = np.zeros((3, 8, 8), np.float32)
     with pytest.raises(gpu.PgpuError) as e:
