@@ -1,0 +1,207 @@
+// ImageStack plugin: the `permutohedral_gpu` method for -gausstransform, -jointbilateral
+// and -bilateral.
+//
+//     ImageStack -plugin libpermgpu_imagestack.so -load im.tmp \
+//                -bilateral 0.1 16 16 0 permutohedral_gpu -save out.tmp
+//
+// The reference loads plugins with dlopen and hands its operation map to
+// init_imagestack_plugin (src/Plugin.cpp:27-36).  This plugin replaces the three
+// operations with subclasses whose parse() accepts the extra method token (same argument
+// grammar as src/GaussTransform.cpp:79-113, 473-502, 699-728) and forwards every other
+// method to the original operation, so the CPU methods keep working unchanged.  The
+// reference's GaussTransform::Method enum cannot grow without editing the reference, so
+// the method is selected here, in parse().
+//
+// The GPU work goes through the C ABI of libpermgpu.so (include/permgpu.h) on the
+// images' host memory; a failing call becomes panic(), the reference's error convention
+// (src/Exception.cpp:18-33).  Built against the reference's headers; the ImageStack
+// symbols resolve from the executable, which links with -rdynamic.
+#include <string>
+#include <vector>
+
+#include "GaussTransform.h"
+#include "Statistics.h"
+#include "permgpu.h"
+
+using namespace ImageStack;
+
+namespace {
+
+const char* kMethod = "permutohedral_gpu";
+
+pgpu_image view_of(const Image& im) {
+    pgpu_image v;
+    v.base = im.baseAddress();
+    v.width = im.width;
+    v.height = im.height;
+    v.frames = im.frames;
+    v.channels = im.channels;
+    v.ystride = im.ystride;
+    v.tstride = im.tstride;
+    v.cstride = im.cstride;
+    return v;
+}
+
+void check(int rc) {
+    if (rc != PGPU_OK) panic("permutohedral_gpu: %s\n", pgpu_last_error());
+}
+
+pgpu_options host_options() {
+    pgpu_options o;
+    pgpu_default_options(&o);
+    o.memory = PGPU_MEM_HOST;
+    return o;
+}
+
+// GaussTransform::apply for the GPU method: a new un-normalised image with the slice
+// positions' size and the values' channels (src/GaussTransform.cpp:194).
+Image gauss_transform_gpu(Image slice, Image splat, Image values, const vector<float>& sigmas) {
+    assert(splat.width == values.width && splat.height == values.height &&
+               splat.frames == values.frames,
+           "Weights and locations of the Gaussians must be the same size\n");
+    assert(slice.channels == splat.channels,
+           "The evaluation locations and the locations of the Gaussians must have"
+           " the same number of channels.\n");
+    Image out(slice.width, slice.height, slice.frames, values.channels);
+    pgpu_image s = view_of(slice), p = view_of(splat), v = view_of(values), o = view_of(out);
+    const pgpu_options opt = host_options();
+    check(pgpu_gauss_transform(slice == splat ? nullptr : &s, &p, &v, sigmas.data(),
+                               (int)sigmas.size(), &o, &opt));
+    return out;
+}
+
+void joint_bilateral_gpu(Image im, Image ref, float fw, float fh, float ft, float cs) {
+    pgpu_image a = view_of(im), b = view_of(ref);
+    const pgpu_options opt = host_options();
+    check(pgpu_joint_bilateral(&a, &b, fw, fh, ft, cs, &opt));
+}
+
+class GpuGaussTransform : public GaussTransform {
+public:
+    void help() {
+        GaussTransform::help();
+        pprintf("With -plugin libpermgpu_imagestack.so the method may also be"
+                " permutohedral_gpu: the permutohedral lattice on a B200 GPU.\n");
+    }
+
+    bool test() {
+        if (!GaussTransform::test()) return false;
+        // the GPU method against the CPU lattice on GaussTransform::test's shapes
+        Image splat(56, 34, 2, 3), slice(56, 34, 2, 3), values(56, 34, 2, 2);
+        Noise::apply(splat, 0, 1);
+        Noise::apply(slice, 0, 1);
+        Noise::apply(values, 0, 1);
+        values.channel(1).set(1.0f);
+        vector<float> sigma(3);
+        sigma[0] = 0.2f;
+        sigma[1] = 0.3f;
+        sigma[2] = 0.4f;
+        Image cpu = GaussTransform::apply(slice, splat, values, sigma, PERMUTOHEDRAL);
+        Image gpu = gauss_transform_gpu(slice, splat, values, sigma);
+        return nearlyEqual(gpu, cpu);
+    }
+
+    void parse(vector<string> args) {
+        if (args.empty() || args[0] != kMethod) {
+            GaussTransform::parse(args);
+            return;
+        }
+        vector<float> sigmas;   // src/GaussTransform.cpp:96-108
+        if (args.size() == 1) {
+            sigmas = vector<float>(stack(0).channels, 1.0f);
+        } else if (args.size() == 2) {
+            sigmas = vector<float>(stack(0).channels, readFloat(args[1]));
+        } else if ((int)args.size() == 1 + stack(1).channels) {
+            for (int i = 0; i < stack(0).channels; i++) sigmas.push_back(readFloat(args[i + 1]));
+        } else {
+            panic("-gausstransform takes one argument, two arguments, or one plus the"
+                  " number of channels in the second image on the stack arguments\n");
+        }
+        Image im = gauss_transform_gpu(stack(0), stack(1), stack(2), sigmas);
+        pop();
+        push(im);
+    }
+};
+
+// shared argument grammar of -jointbilateral and -bilateral (src/GaussTransform.cpp:473-499)
+bool parse_bilateral_args(const vector<string>& args, const char* name, float* cs, float* fw,
+                          float* fh, float* ft) {
+    if (args.size() != 5 || args[4] != kMethod) return false;
+    *cs = readFloat(args[0]);
+    *fw = *fh = readFloat(args[1]);
+    *fh = readFloat(args[2]);
+    *ft = readFloat(args[3]);
+    (void)name;
+    return true;
+}
+
+class GpuJointBilateral : public JointBilateral {
+public:
+    void help() {
+        JointBilateral::help();
+        pprintf("With -plugin libpermgpu_imagestack.so the method may also be"
+                " permutohedral_gpu.\n");
+    }
+
+    bool test() {
+        if (!JointBilateral::test()) return false;
+        Image im(60, 50, 3, 3), ref(60, 50, 3, 3);   // JointBilateral::test's shape
+        Noise::apply(im, 0, 1);
+        Noise::apply(ref, 0, 1);
+        Image cpu = im.copy(), gpu = im.copy();
+        JointBilateral::apply(cpu, ref, 3, 4, 1, 0.25, GaussTransform::PERMUTOHEDRAL);
+        joint_bilateral_gpu(gpu, ref, 3, 4, 1, 0.25);
+        return nearlyEqual(gpu, cpu);
+    }
+
+    void parse(vector<string> args) {
+        float cs, fw, fh, ft;
+        if (!parse_bilateral_args(args, "-jointbilateral", &cs, &fw, &fh, &ft)) {
+            JointBilateral::parse(args);
+            return;
+        }
+        joint_bilateral_gpu(stack(0), stack(1), fw, fh, ft, cs);
+    }
+};
+
+class GpuBilateral : public Bilateral {
+public:
+    void help() {
+        Bilateral::help();
+        pprintf("With -plugin libpermgpu_imagestack.so the method may also be"
+                " permutohedral_gpu.\n");
+    }
+
+    bool test() {
+        Image im(80, 60, 1, 3);
+        Noise::apply(im, 0, 1);
+        Image cpu = im.copy(), gpu = im.copy();
+        Bilateral::apply(cpu, 4, 4, 0, 0.2, GaussTransform::PERMUTOHEDRAL);
+        joint_bilateral_gpu(gpu, gpu, 4, 4, 0, 0.2);
+        return nearlyEqual(gpu, cpu);
+    }
+
+    void parse(vector<string> args) {
+        float cs, fw, fh, ft;
+        if (!parse_bilateral_args(args, "-bilateral", &cs, &fw, &fh, &ft)) {
+            Bilateral::parse(args);
+            return;
+        }
+        Image im = stack(0);
+        joint_bilateral_gpu(im, im, fw, fh, ft, cs);
+    }
+};
+
+void install(map<string, Operation*>& ops, const char* name, Operation* op) {
+    map<string, Operation*>::iterator it = ops.find(name);
+    if (it != ops.end()) delete it->second;
+    ops[name] = op;
+}
+
+}  // namespace
+
+extern "C" void init_imagestack_plugin(map<string, Operation*>& operationMap) {
+    install(operationMap, "-gausstransform", new GpuGaussTransform());
+    install(operationMap, "-jointbilateral", new GpuJointBilateral());
+    install(operationMap, "-bilateral", new GpuBilateral());
+}
