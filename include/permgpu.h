@@ -122,6 +122,30 @@ int pgpu_lattice_dump(int d, int vd, int n, const float *pos, const float *val, 
                       int *n_vertices, short *keys, int *replay_vtx, float *replay_w,
                       float *splat_vals, float *blur_vals, float *out);
 
+/* Bilateral filtering that allocates nothing (no counterpart in the reference, which
+ * only runs on the CPU).  For callers that cannot call cudaMalloc: hosts that own all
+ * device memory through their own pool or allocator, and loops that must not stall the
+ * device (cudaMalloc and cudaFree synchronise it).  Same result as pgpu_bilateral with
+ * the permutohedral method on one frame with both pixel axes filtered, but every
+ * intermediate lives in a fixed 72 MiB device array inside the library, which each GPU
+ * that loads it keeps until the process exits.
+ *   d_in, d_out  device memory, planar (channels, height, width) float32, dense; they may
+ *                be the same buffer (in place)
+ *   limits       width*height <= 262144 (512x512), channels 1..3,
+ *                0 < filter_width < 10*width, 0 < filter_height < 10*height;
+ *                anything else is rejected with PGPU_ERR_UNSUPPORTED before any work
+ *   stream       cudaStream_t to run on (NULL: the legacy default stream); the call
+ *                returns after that stream has finished the filter
+ * The first call on a device looks up the array's device address (once per device,
+ * with that device current); make that first call before any stream capture.  All calls
+ * on a device share the one array: calls that overlap on the GPU (other streams, other
+ * host threads) race and corrupt each other, so serialise them.  A frame whose lattice
+ * needs more hash slots than the array holds returns PGPU_ERR_CAPACITY and leaves d_out
+ * unwritten. */
+int pgpu_bilateral_noalloc(const float *d_in, float *d_out, int width, int height,
+                           int channels, float filter_width, float filter_height,
+                           float color_sigma, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
