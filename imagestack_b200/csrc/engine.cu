@@ -182,7 +182,9 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
             (rc = E.vkey0.ensure(cap * 16)) || (rc = E.vkeyn.ensure((kw - 1) * cap * 16)) ||
             (rc = E.vv0.ensure(cap * vdp * payb)) || (rc = E.vv1.ensure(cap * vdp * payb)) ||
             (rc = E.nbr.ensure((size_t)(d + 1) * cap * 8)) || (rc = E.dstat.ensure(64)) ||
-            (homog && (rc = E.vf32.ensure(cap * vdp * 4))))
+            (homog && (rc = E.vf32.ensure(cap * vdp * 4))) ||
+            (rc = E.vtx2slot.ensure(cap * 4)) || (rc = E.sval.ensure(cap * vdp * accb)) ||
+            (J.replay && (rc = E.rec.ensure((size_t)entries * 4))))
             return rc;
 
         unsigned* dstatus = (unsigned*)E.dstat.p;
@@ -202,6 +204,7 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
         sa.table = tv;
         sa.vals = E.tvals.p;
         sa.ft = (uint32_t*)E.ft.p;
+        sa.rec_slot = J.replay ? (uint32_t*)E.rec.p : nullptr;
         sa.status = dstatus;
         if (!ops->splat(sa, vdp, J.payload, st)) return fail(PGPU_ERR_UNSUPPORTED, "splat variant");
         CUDA_TRY(cudaGetLastError());
@@ -217,6 +220,7 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
         ca.nwords = nwords;
         ca.offs = (const uint32_t*)E.offs.p;
         ca.slot2vtx = (uint32_t*)E.slot2vtx.p;
+        ca.vtx2slot = (uint32_t*)E.vtx2slot.p;
         ca.vkey0 = (uint4*)E.vkey0.p;
         ca.vkeyn = (uint4*)E.vkeyn.p;
         ca.vcap = (uint32_t)cap;
@@ -243,22 +247,25 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaEventRecord(E.ev[3], st));
 
-        void* bufs[2] = {E.vv0.p, E.vv1.p};
-        for (int j = 0; j <= d; ++j) {
-            BlurArgs ba;
-            ba.nbr = (const int2*)E.nbr.p + (size_t)j * cap;
-            ba.nverts = dM;
-            ba.src = (homog && j == 0) ? E.vf32.p : bufs[j & 1];
-            ba.wc = vd - 1;
-            ba.dst = bufs[(j + 1) & 1];
-            if (!launch_blur(ba, (uint32_t)cap, vdp, J.payload, homog, homog && j == 0, E.sms, st))
-                return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
-        }
+        BlurPlan bp;
+        bp.d = d;
+        bp.vdp = vdp;
+        bp.payload = J.payload;
+        bp.homog = homog;
+        bp.src_f32 = homog;
+        bp.nbr = (const int2*)E.nbr.p;
+        bp.nbr_stride = cap;
+        bp.nverts = dM;
+        bp.vmax = (uint32_t)cap;
+        bp.src = homog ? E.vf32.p : E.vv0.p;
+        bp.bufs[0] = E.vv1.p;
+        bp.bufs[1] = E.vv0.p;
+        bp.sval = E.sval.p;
+        bp.vtx2slot = (const uint32_t*)E.vtx2slot.p;
+        bp.wc = vd - 1;
+        bp.sms = E.sms;
+        if (blur_all_axes(bp, st)) return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
         CUDA_TRY(cudaGetLastError());
-        void* final_vals = bufs[(d + 1) & 1];
-        if (J.dump_blur)
-            CUDA_TRY(cudaMemcpyAsync(J.dump_blur, final_vals, std::min<size_t>(cap * vdp * payb, J.dump_bytes),
-                                     cudaMemcpyDeviceToDevice, st));
         CUDA_TRY(cudaEventRecord(E.ev[4], st));
 
         SliceArgs sl;
@@ -267,7 +274,8 @@ int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
         sl.lc = lc;
         sl.table = tv;
         sl.slot2vtx = (const uint32_t*)E.slot2vtx.p;
-        sl.vvals = final_vals;
+        sl.rec_slot = J.replay ? (const uint32_t*)E.rec.p : nullptr;
+        sl.svals = E.sval.p;
         sl.vd = vd;
         sl.out = J.out;
         sl.rec_vtx = J.rec_vtx;
@@ -664,7 +672,7 @@ int pgpu_lattice_dump(int d, int vd, int n, const float* pos, const float* val, 
     const int vdp = vdp_for(vd);
     const size_t rows = (size_t)n * (d + 1);
     const size_t payb = payload_bytes(payload);
-    DevBuf bp, bv, bo, brv, brw, bsv, bbv;
+    DevBuf bp, bv, bo, brv, brw, bsv;
     int rc;
     if ((rc = bp.ensure(hp.size() * 4)) || (rc = bv.ensure(hv.size() * 4)) ||
         (rc = bo.ensure((size_t)n * vd * 4)) || (rc = brv.ensure(rows * 4)) ||
@@ -672,7 +680,7 @@ int pgpu_lattice_dump(int d, int vd, int n, const float* pos, const float* val, 
         return rc;
     // at most n*(d+1) vertices: the dumps copy that many rows of the vertex buffers
     const size_t dump_bytes = rows * vdp * payb;
-    if ((rc = bsv.ensure(dump_bytes)) || (rc = bbv.ensure(dump_bytes))) return rc;
+    if ((rc = bsv.ensure(dump_bytes))) return rc;
     CUDA_TRY(cudaMemcpyAsync(bp.p, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(bv.p, hv.data(), hv.size() * 4, cudaMemcpyHostToDevice, st));
     pgpu_image vpos = {(float*)bp.p, n, 1, 1, d, n, n, n};
@@ -698,7 +706,6 @@ int pgpu_lattice_dump(int d, int vd, int n, const float* pos, const float* val, 
     J.rec_vtx = (int*)brv.p;
     J.rec_w = (float*)brw.p;
     J.dump_splat = bsv.p;
-    J.dump_blur = bbv.p;
     J.dump_bytes = dump_bytes;
     uint32_t M = 0;
     J.vertices_out = &M;
@@ -750,7 +757,19 @@ int pgpu_lattice_dump(int d, int vd, int n, const float* pos, const float* val, 
         return PGPU_OK;
     };
     if ((rc = conv(bsv.p, splat_vals))) return rc;
-    if ((rc = conv(bbv.p, blur_vals))) return rc;
+    if (blur_vals && M) {   // the filtered rows live in slot space, in the arithmetic type
+        const size_t accb = accum_bytes(payload);
+        std::vector<uint32_t> v2s(M);
+        std::vector<unsigned char> rows((size_t)E.last_cap * vdp * accb);
+        CUDA_TRY(cudaMemcpy(v2s.data(), E.vtx2slot.p, (size_t)M * 4, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(rows.data(), E.sval.p, rows.size(), cudaMemcpyDeviceToHost));
+        for (uint32_t v = 0; v < M; ++v)
+            for (int c = 0; c < vd; ++c) {
+                const size_t idx = (size_t)v2s[v] * vdp + c;
+                blur_vals[(size_t)v * vd + c] = accb == 8 ? (float)((double*)rows.data())[idx]
+                                                          : ((float*)rows.data())[idx];
+            }
+    }
     return PGPU_OK;
 }
 

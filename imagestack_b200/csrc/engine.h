@@ -47,6 +47,9 @@ struct Engine {
     // vertex space
     DevBuf vkey0, vkeyn, vv0, vv1, nbr;
     DevBuf vf32;   // FP32 normalised rows feeding the first blur pass (16-bit homogeneous)
+    DevBuf vtx2slot;   // slot of each vertex
+    DevBuf sval;       // filtered rows in slot space, arithmetic type, read by the slice
+    DevBuf rec;        // slot of every (point, remainder), [r][n], recorded by the splat
     DevBuf dstat;
     // staging images for host-memory calls
     DevBuf img_a, img_b, img_c, img_d;
@@ -72,7 +75,6 @@ struct LatticeJob {
     int* rec_vtx = nullptr;
     float* rec_w = nullptr;
     void* dump_splat = nullptr;   // device copy of vertex values after the splat
-    void* dump_blur = nullptr;    // ... and after the blur
     size_t dump_bytes = 0;
     uint32_t* vertices_out = nullptr;
     bool homog = false;   // the last value channel is the homogeneous weight

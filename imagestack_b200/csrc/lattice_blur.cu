@@ -1,0 +1,96 @@
+// Blur launchers: one or two axes per pass, every payload and row-type combination the
+// pass plan uses (its own file so the variants compile in parallel with the rest).
+#include "lattice_ops.h"
+
+namespace pgpu {
+namespace {
+
+int grid_blur(uint64_t work, int sms) {
+    uint64_t g = (work + 255) / 256;
+    const uint64_t cap = (uint64_t)sms * 16;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+template <int VDP, typename PS, typename PD, bool HOMOG>
+void blur_t(const BlurArgs& a, bool pair, uint32_t vmax, int sms, cudaStream_t st) {
+    if (pair) blur_kernel<VDP, PS, PD, HOMOG, true><<<grid_blur(vmax, sms), 256, 0, st>>>(a);
+    else blur_kernel<VDP, PS, PD, HOMOG, false><<<grid_blur(vmax, sms), 256, 0, st>>>(a);
+}
+
+// 16-bit payload P: rows are P between passes, FP32 when read from the compaction
+// (homogeneous lattices) or written for the slice (last pass)
+template <int VDP, typename P, bool HOMOG>
+void blur_16(const BlurArgs& a, bool src_f32, bool dst_acc, bool pair, uint32_t vmax, int sms,
+             cudaStream_t st) {
+    if (src_f32 && dst_acc) blur_t<VDP, float, float, HOMOG>(a, pair, vmax, sms, st);
+    else if (src_f32) blur_t<VDP, float, P, HOMOG>(a, pair, vmax, sms, st);
+    else if (dst_acc) blur_t<VDP, P, float, HOMOG>(a, pair, vmax, sms, st);
+    else blur_t<VDP, P, P, HOMOG>(a, pair, vmax, sms, st);
+}
+
+template <int VDP>
+bool blur_v(const BlurArgs& a, int payload, bool homog, bool src_f32, bool dst_acc, bool pair,
+            uint32_t vmax, int sms, cudaStream_t st) {
+    switch (payload) {
+    case kPayloadF32:
+        if (homog) return false;
+        blur_t<VDP, float, float, false>(a, pair, vmax, sms, st);
+        return true;
+    case kPayloadF64:
+        if (homog) return false;
+        blur_t<VDP, double, double, false>(a, pair, vmax, sms, st);
+        return true;
+    case kPayloadF16:
+        if (homog) blur_16<VDP, __half, true>(a, src_f32, dst_acc, pair, vmax, sms, st);
+        else blur_16<VDP, __half, false>(a, src_f32, dst_acc, pair, vmax, sms, st);
+        return true;
+    case kPayloadBF16:
+        if (homog) blur_16<VDP, __nv_bfloat16, true>(a, src_f32, dst_acc, pair, vmax, sms, st);
+        else blur_16<VDP, __nv_bfloat16, false>(a, src_f32, dst_acc, pair, vmax, sms, st);
+        return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, bool homog, bool src_f32,
+                 bool dst_acc, bool pair, int sms, cudaStream_t st) {
+    switch (vdp) {
+    case 2: return blur_v<2>(a, payload, homog, src_f32, dst_acc, pair, vmax, sms, st);
+    case 4: return blur_v<4>(a, payload, homog, src_f32, dst_acc, pair, vmax, sms, st);
+    case 8: return blur_v<8>(a, payload, homog, src_f32, dst_acc, pair, vmax, sms, st);
+    }
+    return false;
+}
+
+int blur_all_axes(const BlurPlan& p, cudaStream_t st) {
+    const int axes = p.d + 1;
+    const void* src = p.src;
+    bool src_f32 = p.src_f32;
+    int flip = 0;
+    for (int j = 0; j < axes;) {
+        const bool pair = j + 1 < axes;
+        const int step = pair ? 2 : 1;
+        const bool last = j + step >= axes;
+        BlurArgs ba;
+        ba.nbrA = p.nbr + (size_t)j * p.nbr_stride;
+        ba.nbrB = pair ? p.nbr + (size_t)(j + 1) * p.nbr_stride : nullptr;
+        ba.nverts = p.nverts;
+        ba.src = src;
+        ba.dst = last ? p.sval : p.bufs[flip];
+        ba.dst_map = last ? p.vtx2slot : nullptr;
+        ba.wc = p.wc;
+        if (!launch_blur(ba, p.vmax, p.vdp, p.payload, p.homog, src_f32, last, pair, p.sms, st))
+            return 1;
+        src = p.bufs[flip];
+        flip ^= 1;
+        src_f32 = false;
+        j += step;
+    }
+    return 0;
+}
+
+}  // namespace pgpu

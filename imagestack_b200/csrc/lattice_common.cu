@@ -185,42 +185,4 @@ bool launch_assign(const CompactArgs& a, int kw, int vdp, int payload, bool homo
     return false;
 }
 
-template <int VDP, typename PS, typename PD, bool HOMOG>
-static void blur_t(const BlurArgs& a, uint32_t vmax, int sms, cudaStream_t st) {
-    blur_kernel<VDP, PS, PD, HOMOG><<<grid_for(vmax, 256, sms), 256, 0, st>>>(a);
-}
-
-template <int VDP, typename P>
-static void blur_homog(const BlurArgs& a, uint32_t vmax, bool from_f32, int sms, cudaStream_t st) {
-    if (from_f32) blur_t<VDP, float, P, true>(a, vmax, sms, st);
-    else blur_t<VDP, P, P, true>(a, vmax, sms, st);
-}
-
-template <int VDP>
-static bool blur_p(const BlurArgs& a, uint32_t vmax, int payload, bool homog, bool from_f32,
-                   int sms, cudaStream_t st) {
-    if (homog) {
-        if (payload == kPayloadF16) { blur_homog<VDP, __half>(a, vmax, from_f32, sms, st); return true; }
-        if (payload == kPayloadBF16) { blur_homog<VDP, __nv_bfloat16>(a, vmax, from_f32, sms, st); return true; }
-        return false;
-    }
-    switch (payload) {
-    case kPayloadF32: blur_t<VDP, float, float, false>(a, vmax, sms, st); return true;
-    case kPayloadF16: blur_t<VDP, __half, __half, false>(a, vmax, sms, st); return true;
-    case kPayloadBF16: blur_t<VDP, __nv_bfloat16, __nv_bfloat16, false>(a, vmax, sms, st); return true;
-    case kPayloadF64: blur_t<VDP, double, double, false>(a, vmax, sms, st); return true;
-    }
-    return false;
-}
-
-bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, bool homog,
-                 bool from_f32, int sms, cudaStream_t st) {
-    switch (vdp) {
-    case 2: return blur_p<2>(a, vmax, payload, homog, from_f32, sms, st);
-    case 4: return blur_p<4>(a, vmax, payload, homog, from_f32, sms, st);
-    case 8: return blur_p<8>(a, vmax, payload, homog, from_f32, sms, st);
-    }
-    return false;
-}
-
 }  // namespace pgpu

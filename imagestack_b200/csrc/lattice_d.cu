@@ -40,22 +40,21 @@ void neighbours(const NbrArgs& a, uint32_t vmax, int sms, cudaStream_t st) {
     neighbours_kernel<D><<<grid_cap(vmax, 256, sms), 256, 0, st>>>(a);
 }
 
-template <int VDP, typename P, bool HOMOG>
+template <int VDP, typename A, bool HOMOG>
 void slice_t(const SliceArgs& a, cudaStream_t st) {
     const uint32_t blocks = (a.n + kSliceThreads - 1) / kSliceThreads;
-    if (blocks) slice_kernel<D, VDP, P, HOMOG><<<blocks, kSliceThreads, 0, st>>>(a);
+    if (blocks) slice_kernel<D, VDP, A, HOMOG><<<blocks, kSliceThreads, 0, st>>>(a);
 }
 
+// the slice reads the last blur pass's rows: FP64 for the FP64 lattice, FP32 otherwise;
 // homogeneous rows exist only for the 16-bit payloads
 template <int VDP>
 bool slice_p(const SliceArgs& a, int payload, bool homog, cudaStream_t st) {
     switch (payload) {
     case kPayloadF32: slice_t<VDP, float, false>(a, st); return !homog;
     case kPayloadF16:
-        homog ? slice_t<VDP, __half, true>(a, st) : slice_t<VDP, __half, false>(a, st);
-        return true;
     case kPayloadBF16:
-        homog ? slice_t<VDP, __nv_bfloat16, true>(a, st) : slice_t<VDP, __nv_bfloat16, false>(a, st);
+        homog ? slice_t<VDP, float, true>(a, st) : slice_t<VDP, float, false>(a, st);
         return true;
     case kPayloadF64: slice_t<VDP, double, false>(a, st); return !homog;
     }

@@ -105,15 +105,9 @@ __device__ __forceinline__ uint4 with_state(uint4 w, uint32_t s) {
     return w;
 }
 
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {
-    z ^= z >> 30;
-    z *= 0xBF58476D1CE4E5B9ull;
-    z ^= z >> 27;
-    z *= 0x94D049BB133111EBull;
-    z ^= z >> 31;
-    return z;
-}
-
+// Multiplicative hash over the key's 64-bit halves: each step multiplies by an odd
+// constant, which carries every input bit into the high half; the final fold brings the
+// high half down.  The slot is then taken from the top bits (home_slot).
 template <int KW>
 __device__ __forceinline__ uint32_t key_hash(const Key<KW>& k) {
     uint64_t h = 0x2545F4914F6CDD1Dull;
@@ -121,12 +115,13 @@ __device__ __forceinline__ uint32_t key_hash(const Key<KW>& k) {
     for (int w = 0; w < KW; ++w) {
         uint4 q = k.w[w];
         if (w == 0) q.w &= 0xFFFFu;   // the state lane is not part of the key
-        uint64_t a = (uint64_t)q.x | ((uint64_t)q.y << 32);
-        uint64_t b = (uint64_t)q.z | ((uint64_t)q.w << 32);
-        h = mix64(h ^ a);
-        h = mix64(h ^ b);
+        const uint64_t a = (uint64_t)q.x | ((uint64_t)q.y << 32);
+        const uint64_t b = (uint64_t)q.z | ((uint64_t)q.w << 32);
+        h = (h ^ a) * 0x9E3779B97F4A7C15ull;
+        h = (h ^ b) * 0xC2B2AE3D27D4EB4Full;
     }
-    return (uint32_t)(h >> 32);
+    h ^= h >> 29;
+    return (uint32_t)(h >> 32) ^ (uint32_t)h;
 }
 
 // ---------------------------------------------------------------------------------
@@ -145,13 +140,16 @@ struct TableView {
 
 __device__ __forceinline__ uint32_t home_slot(uint32_t h, uint32_t cap) { return __umulhi(h, cap); }
 
-// Insert-or-find during the splat; returns the slot or -1 (status bit set).
+// Insert-or-find during the splat, starting at slot `home` whose word 0 the caller has
+// already loaded into `first` (so the loads of several keys can be in flight at once);
+// returns the slot or -1 (status bit set).
 template <int KW>
-__device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t h, unsigned* status) {
+__device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home, uint4 first,
+                            unsigned* status) {
     const uint4 empty = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
-    uint32_t s = home_slot(h, t.cap);
+    uint32_t s = home;
     for (int probe = 0; probe < kMaxProbe; ++probe) {
-        uint4 w = __ldcg(&t.key0[s]);
+        uint4 w = probe == 0 ? first : __ldcg(&t.key0[s]);
         if (maybe_empty(w)) {
             // An empty slot, or a read that raced with the slot's one-time fill: the
             // compare-and-swap decides, and returns the slot's real contents.

@@ -61,6 +61,7 @@ struct SplatArgs {
     TableView table;
     void* vals;        // cap * VDP accumulators (float or double), zeroed
     uint32_t* ft;      // cap first-touch entries, all ones
+    uint32_t* rec_slot;   // optional [r][n] slot of every (point, remainder), for the slice
     unsigned* status;
 };
 
@@ -71,6 +72,7 @@ struct CompactArgs {
     uint32_t nwords;
     const uint32_t* offs;  // exclusive prefix popcount per word
     uint32_t* slot2vtx;
+    uint32_t* vtx2slot;
     uint4* vkey0;          // vertex keys, word 0 ...
     uint4* vkeyn;          // ... and later words, (KW-1) x vcap
     uint32_t vcap;
@@ -89,12 +91,16 @@ struct NbrArgs {
     int2* nbr;             // (d+1) x vcap pairs
 };
 
+// One launch blurs along one axis (nbrA) or, fused, along two consecutive axes (nbrA then
+// nbrB): the first axis's result stays in registers instead of being stored and reloaded.
 struct BlurArgs {
-    const int2* nbr;       // neighbours of this axis
+    const int2* nbrA;           // neighbours along the first axis of the pass
+    const int2* nbrB;           // neighbours along the second axis (fused passes)
     const uint32_t* nverts;
-    const void* src;
-    void* dst;
-    int wc;                // homogeneous weight channel (homogeneous rows only)
+    const void* src;            // rows in vertex order
+    void* dst;                  // rows in vertex order, or in slot space with dst_map
+    const uint32_t* dst_map;    // row index of vertex v in dst (vertex -> slot); null: v
+    int wc;                     // homogeneous weight channel (homogeneous rows only)
 };
 
 struct SliceArgs {
@@ -102,8 +108,9 @@ struct SliceArgs {
     uint32_t n;
     LatticeConsts lc;
     TableView table;
-    const uint32_t* slot2vtx;
-    const void* vvals;
+    const uint32_t* slot2vtx;   // parity dumps only
+    const uint32_t* rec_slot;   // slots recorded by the splat, [r][n]; null: look keys up
+    const void* svals;          // filtered rows in slot space (float, or double)
     int vd;
     OutView out;
     int* rec_vtx;          // optional n*(d+1) vertex indices (parity dumps)
@@ -209,9 +216,17 @@ __device__ __forceinline__ double acc_add(double a, double b) { return __dadd_rn
 // splat
 // ---------------------------------------------------------------------------------
 constexpr int kSplatThreads = 256;
+// Tuning (measured on the 4K d=5 bilateral): the splat is latency bound, so resident warps
+// matter more than a few spilled registers — 4 blocks of 256 per SM up to d=6, fewer for
+// the larger per-point state of higher d.  Leaders issue the home-slot loads of all
+// remainders before resolving any for d <= PGPU_SPLAT_AHEAD_MAX_D.
+#ifndef PGPU_SPLAT_AHEAD_MAX_D
+#define PGPU_SPLAT_AHEAD_MAX_D 8
+#endif
+__host__ __device__ constexpr int splat_min_blocks(int d) { return d <= 6 ? 4 : d <= 8 ? 3 : 2; }
 
 template <int D, int VDP, typename Acc>
-__global__ void __launch_bounds__(kSplatThreads) splat_kernel(SplatArgs a) {
+__global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kernel(SplatArgs a) {
     constexpr int KW = key_words(D);
     __shared__ Acc stage[kSplatThreads / 32][32][VDP];
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -227,44 +242,88 @@ __global__ void __launch_bounds__(kSplatThreads) splat_kernel(SplatArgs a) {
     const uint32_t e0 = i * (uint32_t)(D + 1);
     Acc* vals = reinterpret_cast<Acc*>(a.vals);
 
+    // Phase 1: group the lanes that share each vertex key (exact match on all key words);
+    // each group's leader starts loading its home slot.  For d <= 8 the loads of all d+1
+    // remainders are in flight together before any is needed.
+    constexpr bool kAhead = D <= PGPU_SPLAT_AHEAD_MAX_D;
+    unsigned peers[D + 1];
+    uint32_t home[D + 1];
+    uint4 first[D + 1];
 #pragma unroll
     for (int r = 0; r <= D; ++r) {
         int kc[D];
         vertex_coords<D>(sx, r, kc);
         Key<KW> key;
         pack_key<D>(kc, key);
-        unsigned peers = active;
+        unsigned pr = active;
 #pragma unroll
         for (int w = 0; w < KW; ++w) {
-            peers &= __match_any_sync(active, ((unsigned long long)key.w[w].y << 32) | key.w[w].x);
-            peers &= __match_any_sync(active, ((unsigned long long)key.w[w].w << 32) | key.w[w].z);
+            pr &= __match_any_sync(active, ((unsigned long long)key.w[w].y << 32) | key.w[w].x);
+            pr &= __match_any_sync(active, ((unsigned long long)key.w[w].w << 32) | key.w[w].z);
         }
-        const unsigned leader = __ffs(peers) - 1;
+        peers[r] = pr;
+        home[r] = home_slot(key_hash<KW>(key), a.table.cap);
+        first[r] = make_uint4(0u, 0u, 0u, 0u);
+        if (kAhead && lane == (unsigned)(__ffs(pr) - 1)) first[r] = __ldcg(&a.table.key0[home[r]]);
+    }
+
+    // Phase 2: per remainder, the group's weighted values are summed by its leader, which
+    // finds or inserts the vertex and adds them with one vector atomic; the first touch
+    // is a fire-and-forget atomicMin.  Every lane records the slot for the slice.
+#pragma unroll
+    for (int r = 0; r <= D; ++r) {
+        const unsigned pr = peers[r];
+        const unsigned leader = __ffs(pr) - 1;
         Acc c[VDP];
 #pragma unroll
         for (int k = 0; k < VDP; ++k) c[k] = acc_mul<Acc>(sx.bary[r], v[k]);
-        const bool grouped = peers != (1u << lane);
-        if (grouped && lane != leader) {
+        // Neighbouring pixels usually share a vertex, so groups are mostly runs of
+        // consecutive lanes: then one segmented suffix sum over the warp (5 shuffle steps)
+        // leaves each run's total in its first lane.  Otherwise the leader adds its
+        // group's rows from shared memory one by one.
+        const unsigned run = pr >> leader;
+        if (__all_sync(active, (run & (run + 1u)) == 0u)) {
+            const unsigned last = 31u - __clz(pr);
 #pragma unroll
-            for (int k = 0; k < VDP; ++k) stage[warp][lane][k] = c[k];
-        }
-        __syncwarp(active);
-        if (lane == leader) {
-            unsigned rest = peers & ~(1u << lane);
-            while (rest) {
-                const int src = __ffs(rest) - 1;
-                rest &= rest - 1;
+            for (int o = 1; o < 32; o <<= 1) {
 #pragma unroll
-                for (int k = 0; k < VDP; ++k) c[k] = acc_add(c[k], stage[warp][src][k]);
+                for (int k = 0; k < VDP; ++k) {
+                    const Acc t = __shfl_down_sync(active, c[k], o);
+                    if (lane + o <= last) c[k] = acc_add(c[k], t);
+                }
             }
-            const int s = table_insert<KW>(a.table, key, key_hash<KW>(key), a.status);
+        } else {
+            if (pr != (1u << lane) && lane != leader) {
+#pragma unroll
+                for (int k = 0; k < VDP; ++k) stage[warp][lane][k] = c[k];
+            }
+            __syncwarp(active);
+            if (lane == leader) {
+                unsigned rest = pr & ~(1u << lane);
+                while (rest) {
+                    const int src = __ffs(rest) - 1;
+                    rest &= rest - 1;
+#pragma unroll
+                    for (int k = 0; k < VDP; ++k) c[k] = acc_add(c[k], stage[warp][src][k]);
+                }
+            }
+            __syncwarp(active);
+        }
+        int s = -1;
+        if (lane == leader) {
+            int kc[D];
+            vertex_coords<D>(sx, r, kc);
+            Key<KW> key;
+            pack_key<D>(kc, key);
+            const uint4 w0 = kAhead ? first[r] : __ldcg(&a.table.key0[home[r]]);
+            s = table_insert<KW>(a.table, key, home[r], w0, a.status);
             if (s >= 0) {
                 atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
-                const uint32_t e = e0 + (uint32_t)r;   // smallest entry of the group
-                if (__ldcg(&a.ft[s]) > e) atomicMin(&a.ft[s], e);
+                atomicMin(&a.ft[s], e0 + (uint32_t)r);   // the leader's entry is the group's smallest
             }
         }
-        __syncwarp(active);
+        s = __shfl_sync(active, s, leader);
+        if (a.rec_slot) a.rec_slot[(size_t)r * a.n + i] = (uint32_t)s;
     }
 }
 
@@ -298,6 +357,7 @@ __global__ void assign_kernel(CompactArgs a) {
             const uint32_t w = f >> 5;
             const uint32_t vtx = a.offs[w] + __popc(a.bitmap[w] & ((1u << (f & 31u)) - 1u));
             a.slot2vtx[s] = vtx;
+            a.vtx2slot[vtx] = s;
             a.vkey0[vtx] = a.table.key0[s];
 #pragma unroll
             for (int k = 1; k < KW; ++k)
@@ -321,6 +381,7 @@ __global__ void assign_kernel(CompactArgs a) {
         const uint32_t w = f >> 5;
         const uint32_t vtx = a.offs[w] + __popc(a.bitmap[w] & ((1u << (f & 31u)) - 1u));
         a.slot2vtx[s] = vtx;
+        a.vtx2slot[vtx] = s;
         a.vkey0[vtx] = a.table.key0[s];
 #pragma unroll
         for (int k = 1; k < KW; ++k)
@@ -382,9 +443,59 @@ __device__ __forceinline__ double blur3(double a, double b, double c) {
     return __dadd_rn(__dadd_rn(0.25 * a, 0.5 * b), 0.25 * c);
 }
 
-// PS/PD: payload read / written (they differ only for the first pass of a homogeneous
-// 16-bit lattice, which reads the FP32 rows written by the compaction).
-template <int VDP, typename PS, typename PD, bool HOMOG>
+// Row of vertex u (zeros for an absent vertex, u < 0), in arithmetic type A.
+template <int VDP, typename PS, typename A>
+__device__ __forceinline__ void load_row(const PS* src, int u, A (&r)[VDP]) {
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) r[k] = u >= 0 ? (A)Payload<PS>::load(src + (size_t)u * VDP + k) : (A)0;
+}
+
+// [1 2 1]/4 of three rows.  Homogeneous rows (m_0..m_{wc-1}, w): blur w and the products
+// w*m, then renormalise, which is the same linear filter in homogeneous coordinates.
+template <int VDP, typename A, bool HOMOG>
+__device__ __forceinline__ void combine3(const A (&r1)[VDP], const A (&r0)[VDP], const A (&r2)[VDP],
+                                         int wc, A (&out)[VDP]) {
+    if constexpr (HOMOG) {
+        A w1 = r1[0], w0 = r0[0], w2 = r2[0];
+#pragma unroll
+        for (int k = 0; k < VDP; ++k)
+            if (k == wc) { w1 = r1[k]; w0 = r0[k]; w2 = r2[k]; }
+        const A nw = blur3(w1, w0, w2);
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) {
+            if (k == wc) out[k] = nw;
+            else if (k < wc && nw != (A)0) out[k] = blur3(w1 * r1[k], w0 * r0[k], w2 * r2[k]) / nw;
+            else out[k] = (A)0;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) out[k] = blur3(r1[k], r0[k], r2[k]);
+    }
+}
+
+// the first-axis blur at vertex u (zeros when u is absent)
+template <int VDP, typename PS, typename A, bool HOMOG>
+__device__ __forceinline__ void blurred_row(const PS* src, const int2* nbr, int u, int wc,
+                                            A (&out)[VDP]) {
+    if (u < 0) {
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) out[k] = (A)0;
+        return;
+    }
+    const int2 nb = __ldg(nbr + u);
+    A r1[VDP], r0[VDP], r2[VDP];
+    load_row<VDP, PS, A>(src, nb.x, r1);
+    load_row<VDP, PS, A>(src, u, r0);
+    load_row<VDP, PS, A>(src, nb.y, r2);
+    combine3<VDP, A, HOMOG>(r1, r0, r2, wc, out);
+}
+
+// PS/PD: row types read and written.  They differ for the first pass of a homogeneous
+// 16-bit lattice (FP32 rows from the compaction) and for the last pass of a 16-bit
+// lattice (FP32 rows in slot space for the slice).  A fused pair computes the first
+// axis's rows in registers with the same arithmetic a separate pass would store, so in
+// FP32 it is bit-identical to two passes.
+template <int VDP, typename PS, typename PD, bool HOMOG, bool PAIR>
 __global__ void blur_kernel(BlurArgs a) {
     using A = typename AccOf<PD>::T;
     const PS* src = reinterpret_cast<const PS*>(a.src);
@@ -392,40 +503,20 @@ __global__ void blur_kernel(BlurArgs a) {
     const uint32_t m = *a.nverts;
     for (uint32_t vtx = blockIdx.x * blockDim.x + threadIdx.x; vtx < m;
          vtx += gridDim.x * blockDim.x) {
-        const int2 nb = a.nbr[vtx];
-        if constexpr (HOMOG) {
-            // rows hold (m_0..m_{wc-1}, w): blur w and the products w*m, renormalise
+        A out[VDP];
+        if constexpr (PAIR) {
+            const int2 nb = __ldg(a.nbrB + vtx);
             A r1[VDP], r0[VDP], r2[VDP];
-#pragma unroll
-            for (int k = 0; k < VDP; ++k) {
-                r1[k] = nb.x >= 0 ? (A)Payload<PS>::load(src + (size_t)nb.x * VDP + k) : (A)0;
-                r2[k] = nb.y >= 0 ? (A)Payload<PS>::load(src + (size_t)nb.y * VDP + k) : (A)0;
-                r0[k] = (A)Payload<PS>::load(src + (size_t)vtx * VDP + k);
-            }
-            A w1 = r1[0], w0 = r0[0], w2 = r2[0];
-#pragma unroll
-            for (int k = 0; k < VDP; ++k)
-                if (k == a.wc) { w1 = r1[k]; w0 = r0[k]; w2 = r2[k]; }
-            const A nw = blur3(w1, w0, w2);
-#pragma unroll
-            for (int k = 0; k < VDP; ++k) {
-                A out;
-                if (k == a.wc) out = nw;
-                else if (k < a.wc && nw != (A)0) out = blur3(w1 * r1[k], w0 * r0[k], w2 * r2[k]) / nw;
-                else out = (A)0;
-                Payload<PD>::store(dst + (size_t)vtx * VDP + k, out);
-            }
-            continue;
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.x, a.wc, r1);
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, r0);
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.y, a.wc, r2);
+            combine3<VDP, A, HOMOG>(r1, r0, r2, a.wc, out);
+        } else {
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, out);
         }
-        const PS* srcp = src;
-        PD* dstp = dst;
+        const size_t row = a.dst_map ? (size_t)__ldg(a.dst_map + vtx) : (size_t)vtx;
 #pragma unroll
-        for (int k = 0; k < VDP; ++k) {
-            const A x1 = nb.x >= 0 ? (A)Payload<PS>::load(srcp + (size_t)nb.x * VDP + k) : (A)0;
-            const A x2 = nb.y >= 0 ? (A)Payload<PS>::load(srcp + (size_t)nb.y * VDP + k) : (A)0;
-            const A x0 = (A)Payload<PS>::load(srcp + (size_t)vtx * VDP + k);
-            Payload<PD>::store(dstp + (size_t)vtx * VDP + k, blur3(x1, x0, x2));
-        }
+        for (int k = 0; k < VDP; ++k) Payload<PD>::store(dst + row * VDP + k, out[k]);
     }
 }
 
@@ -434,10 +525,14 @@ __global__ void blur_kernel(BlurArgs a) {
 // ---------------------------------------------------------------------------------
 constexpr int kSliceThreads = 256;
 
-template <int D, int VDP, typename P, bool HOMOG>
+// A: arithmetic and storage type of the filtered rows (float, or double for the FP64
+// lattice); rows live in slot space (svals[slot*VDP ..]).  With rec_slot the slots come
+// from the splat's record of this very point (the reference's replay slice,
+// src/Permutohedral.h:418-427); without it the keys are looked up (re-elevation slice at
+// other positions, :405-407), and a vertex the splat never created contributes zero.
+template <int D, int VDP, typename A, bool HOMOG>
 __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
     constexpr int KW = key_words(D);
-    using A = typename AccOf<P>::T;
     const uint32_t i = blockIdx.x * (uint32_t)kSliceThreads + threadIdx.x;
     if (i >= a.n) return;
     // A splat that overflowed the table is rerun by the host with more slots; its
@@ -447,28 +542,33 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
     load_position<D>(a.src, i, p);
     Simplex<D> sx;
     compute_simplex<D>(p, a.lc, sx, a.status);
-    const P* vv = reinterpret_cast<const P*>(a.vvals);
+    const A* sv = reinterpret_cast<const A*>(a.svals);
     A acc[VDP];
 #pragma unroll
     for (int k = 0; k < VDP; ++k) acc[k] = (A)0;
 #pragma unroll
     for (int r = 0; r <= D; ++r) {
-        int kc[D];
-        vertex_coords<D>(sx, r, kc);
-        Key<KW> key;
-        pack_key<D>(kc, key);
-        const int s = table_find<KW>(a.table, key, key_hash<KW>(key));
-        const int vtx = s >= 0 ? (int)__ldg(a.slot2vtx + s) : -1;
+        int s;
+        if (a.rec_slot) {
+            s = (int)__ldg(a.rec_slot + (size_t)r * a.n + i);
+        } else {
+            int kc[D];
+            vertex_coords<D>(sx, r, kc);
+            Key<KW> key;
+            pack_key<D>(kc, key);
+            const uint32_t h = key_hash<KW>(key);
+            s = table_find<KW>(a.table, key, h);
+        }
         const float w = sx.bary[r];
         if (a.rec_vtx) {
-            a.rec_vtx[(size_t)i * (D + 1) + r] = vtx;
+            a.rec_vtx[(size_t)i * (D + 1) + r] = s >= 0 ? (int)__ldg(a.slot2vtx + s) : -1;
             a.rec_w[(size_t)i * (D + 1) + r] = w;
         }
-        if (vtx >= 0) {
-            if constexpr (HOMOG) {   // row (m_0.., w): accumulate (w*m_k, w)
-                A row[VDP];
+        if (s >= 0) {
+            A row[VDP];
 #pragma unroll
-                for (int k = 0; k < VDP; ++k) row[k] = (A)Payload<P>::load(vv + (size_t)vtx * VDP + k);
+            for (int k = 0; k < VDP; ++k) row[k] = __ldg(sv + (size_t)s * VDP + k);
+            if constexpr (HOMOG) {   // row (m_0.., w): accumulate (w*m_k, w)
                 A wt = row[0];
 #pragma unroll
                 for (int k = 0; k < VDP; ++k) if (k == a.vd - 1) wt = row[k];
@@ -478,8 +578,7 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
                     acc[k] = acc_add(acc[k], (k == a.vd - 1) ? bw : bw * row[k]);
             } else {
 #pragma unroll
-                for (int k = 0; k < VDP; ++k)
-                    acc[k] = acc_add(acc[k], (A)w * (A)Payload<P>::load(vv + (size_t)vtx * VDP + k));
+                for (int k = 0; k < VDP; ++k) acc[k] = acc_add(acc[k], (A)w * row[k]);
             }
         }
     }

@@ -37,8 +37,28 @@ void launch_scan(const uint32_t* bitmap, uint32_t nwords, uint32_t* partials, ui
 // homog: rows normalised by the homogeneous weight, written as FP32 for the first blur pass
 bool launch_assign(const CompactArgs& a, int kw, int vdp, int payload, bool homog, int sms,
                    cudaStream_t st);
-// homog + from_f32: the first pass of a homogeneous 16-bit lattice reads FP32 rows
-bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, bool homog,
-                 bool from_f32, int sms, cudaStream_t st);
+// src_f32: the pass reads FP32 rows (first pass of a homogeneous 16-bit lattice);
+// dst_acc: it writes rows of the arithmetic type (the last pass, for the slice);
+// pair: it blurs along two consecutive axes
+bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, bool homog, bool src_f32,
+                 bool dst_acc, bool pair, int sms, cudaStream_t st);
+
+// All d+1 blur axes in fused pairs; intermediate rows ping-pong between bufs[0] and
+// bufs[1] (payload type); the last pass writes the arithmetic type into slot space
+// through vtx2slot, where the slice reads it.
+struct BlurPlan {
+    int d, vdp, payload;
+    bool homog, src_f32;
+    const int2* nbr;       // (d+1) x nbr_stride neighbour pairs
+    size_t nbr_stride;
+    const uint32_t* nverts;
+    uint32_t vmax;
+    const void* src;       // the compaction's rows in vertex order
+    void* bufs[2];
+    void* sval;
+    const uint32_t* vtx2slot;
+    int wc, sms;
+};
+int blur_all_axes(const BlurPlan& p, cudaStream_t st);   // 0 on success
 
 }  // namespace pgpu

@@ -25,7 +25,7 @@ constexpr int kNoAllocMaxPixels = 512 * 512;
 constexpr int kNoAllocMaxChannels = 3;                 // d = channels + 2 <= 5, 4 values
 constexpr int kNoAllocMaxD = kNoAllocMaxChannels + 2;
 constexpr int kNoAllocVdp = 4;
-constexpr uint32_t kNoAllocSlots = 1u << 19;           // hash slots (and vertex rows)
+constexpr uint32_t kNoAllocSlots = 3u << 17;           // hash slots (and vertex rows)
 constexpr size_t kAlign = 256;
 
 constexpr size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
@@ -46,7 +46,10 @@ constexpr size_t kOffVkey0 = align_up(kOffParts + kParts * 4 + 16);
 constexpr size_t kOffVv0 = align_up(kOffVkey0 + (size_t)kNoAllocSlots * 16);
 constexpr size_t kOffVv1 = align_up(kOffVv0 + (size_t)kNoAllocSlots * kNoAllocVdp * 4);
 constexpr size_t kOffNbr = align_up(kOffVv1 + (size_t)kNoAllocSlots * kNoAllocVdp * 4);
-constexpr size_t kUsed = align_up(kOffNbr + (size_t)(kNoAllocMaxD + 1) * kNoAllocSlots * 8);
+constexpr size_t kOffVtx2Slot = align_up(kOffNbr + (size_t)(kNoAllocMaxD + 1) * kNoAllocSlots * 8);
+constexpr size_t kOffSval = align_up(kOffVtx2Slot + (size_t)kNoAllocSlots * 4);
+constexpr size_t kOffRec = align_up(kOffSval + (size_t)kNoAllocSlots * kNoAllocVdp * 4);
+constexpr size_t kUsed = align_up(kOffRec + kEntries * 4);
 
 // 72 MiB, held by every GPU that loads this part of the library until the process exits
 constexpr size_t kScratchBytes = 72ull << 20;
@@ -159,6 +162,7 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     sa.table = tv;
     sa.vals = base + kOffTvals;
     sa.ft = (uint32_t*)(base + kOffFt);
+    sa.rec_slot = (uint32_t*)(base + kOffRec);
     sa.status = dstatus;
     if (!ops->splat(sa, vdp, kPayloadF32, st)) return fail(PGPU_ERR_UNSUPPORTED, "splat variant");
     CUDA_TRY(cudaGetLastError());
@@ -174,6 +178,7 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     ca.nwords = nwords;
     ca.offs = (const uint32_t*)(base + kOffOffs);
     ca.slot2vtx = (uint32_t*)(base + kOffSlot2Vtx);
+    ca.vtx2slot = (uint32_t*)(base + kOffVtx2Slot);
     ca.vkey0 = (uint4*)(base + kOffVkey0);
     ca.vkeyn = (uint4*)(base + kOffVkey0);
     ca.vcap = cap;
@@ -193,17 +198,24 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     na.nbr = (int2*)(base + kOffNbr);
     ops->neighbours(na, cap, sms, st);
 
-    void* bufs[2] = {base + kOffVv0, base + kOffVv1};
-    for (int j = 0; j <= d; ++j) {
-        BlurArgs ba;
-        ba.nbr = (const int2*)(base + kOffNbr) + (size_t)j * cap;
-        ba.nverts = dM;
-        ba.src = bufs[j & 1];
-        ba.dst = bufs[(j + 1) & 1];
-        ba.wc = vd - 1;
-        if (!launch_blur(ba, cap, vdp, kPayloadF32, false, false, sms, st))
-            return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
-    }
+    BlurPlan bp;
+    bp.d = d;
+    bp.vdp = vdp;
+    bp.payload = kPayloadF32;
+    bp.homog = false;
+    bp.src_f32 = false;
+    bp.nbr = (const int2*)(base + kOffNbr);
+    bp.nbr_stride = cap;
+    bp.nverts = dM;
+    bp.vmax = cap;
+    bp.src = base + kOffVv0;
+    bp.bufs[0] = base + kOffVv1;
+    bp.bufs[1] = base + kOffVv0;
+    bp.sval = base + kOffSval;
+    bp.vtx2slot = (const uint32_t*)(base + kOffVtx2Slot);
+    bp.wc = vd - 1;
+    bp.sms = sms;
+    if (blur_all_axes(bp, st)) return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
 
     SliceArgs sl;
     memset(&sl, 0, sizeof(sl));
@@ -212,7 +224,8 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     sl.lc = lc;
     sl.table = tv;
     sl.slot2vtx = (const uint32_t*)(base + kOffSlot2Vtx);
-    sl.vvals = bufs[(d + 1) & 1];
+    sl.rec_slot = (const uint32_t*)(base + kOffRec);
+    sl.svals = base + kOffSval;
     sl.vd = vd;
     sl.out.base = d_out;
     sl.out.ystride = width;
