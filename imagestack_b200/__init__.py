@@ -63,7 +63,7 @@ class Stats(C.Structure):
 
 EXPORTS = ["pgpu_default_options", "pgpu_last_error", "pgpu_version", "pgpu_device_count",
            "pgpu_gauss_transform", "pgpu_joint_bilateral", "pgpu_bilateral", "pgpu_last_stats",
-           "pgpu_lattice_dump"]
+           "pgpu_lattice_dump", "pgpu_bilateral_batch"]
 
 _lib = None
 
@@ -85,6 +85,7 @@ def lib():
                                        C.c_float, P(Options)]
     L.pgpu_bilateral.argtypes = [P(Image), C.c_float, C.c_float, C.c_float, C.c_float, P(Options)]
     L.pgpu_last_stats.argtypes = [P(Stats)]
+    L.pgpu_bilateral_batch.argtypes = [P(Image), C.c_int, P(C.c_float), P(C.c_float), P(Options)]
     L.pgpu_lattice_dump.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                     P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p]
@@ -218,6 +219,36 @@ class Bilateral:
         _check(lib().pgpu_bilateral(C.byref(im), filter_width, filter_height, filter_frames,
                                     color_sigma, C.byref(opt)))
         return image
+
+
+FLAG_GRAPH = 1
+
+
+def bilateral_batch(images, filter_widths, color_sigmas, payload: str = "fp32",
+                    graph: bool = False, load_factor: float = 0.5):
+    """Bilateral filter of many images (same channel count, any sizes) in one set of
+    launches, each in place with its own sigmas; the result of each equals
+    Bilateral.apply on it.  All numpy (host) or all torch CUDA tensors (device, run on
+    torch's current stream)."""
+    n = len(images)
+    if len(filter_widths) != n or len(color_sigmas) != n:
+        raise PgpuError(ERR_ARGUMENT, "one filter width and colour sigma per image")
+    views = (Image * max(n, 1))()
+    mem = MEM_HOST
+    for i, im in enumerate(images):
+        views[i], m = _view(im, "image %d" % i)
+        if i == 0:
+            mem = m
+        elif m != mem:
+            raise PgpuError(ERR_ARGUMENT, "images must all be on the host or all on the device")
+    fw = (C.c_float * max(n, 1))(*[float(x) for x in filter_widths])
+    cs = (C.c_float * max(n, 1))(*[float(x) for x in color_sigmas])
+    stream = _torch_stream(images[0]) if (n and mem == MEM_DEVICE) else None
+    opt = _options(mem, payload, stream=stream, load_factor=load_factor,
+                   device=(images[0].device.index or 0) if (n and mem == MEM_DEVICE) else 0)
+    opt.flags = FLAG_GRAPH if graph else 0
+    _check(lib().pgpu_bilateral_batch(views, n, fw, cs, C.byref(opt)))
+    return images
 
 
 def lattice_dump(pos: np.ndarray, val: np.ndarray, payload: str = "fp32") -> dict:

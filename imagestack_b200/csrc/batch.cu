@@ -1,0 +1,397 @@
+// The launch sequence of a batch of lattices — many images of one kind (same number of
+// position dimensions, value channels and payload) per launch; a single image is a batch
+// of one.  Every image owns a range of the shared hash-slot array sized from its learned
+// vertices-per-pixel ratio; an image whose range overflows is rerun with a larger range.
+// A batch can be captured as a CUDA graph and replayed for the next batch of the same
+// shape: the per-image descriptors are data uploaded by the graph's first node, so only
+// sizes are baked into it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace pgpu {
+
+int Engine::ensure_hmeta(size_t bytes) {
+    if (bytes <= hmeta_bytes) return PGPU_OK;
+    if (hmeta) cudaFreeHost(hmeta);
+    hmeta = nullptr;
+    hmeta_bytes = 0;
+    const size_t nb = bytes + bytes / 4 + 4096;
+    if (cudaHostAlloc((void**)&hmeta, nb, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PGPU_ERR_MEMORY, "pinned allocation of %zu bytes failed", nb);
+    }
+    hmeta_bytes = nb;
+    return PGPU_OK;
+}
+
+void Engine::drop_graphs() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    graphs.clear();
+}
+
+namespace {
+
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// an image's key for the learned vertex ratio: its shape and position scales
+std::string item_signature(int d, const PointSource& s) {
+    char buf[320];
+    int n = snprintf(buf, sizeof(buf), "%d:%dx%dx%d:%x", d, s.width, s.height, s.frames, s.coord_mask);
+    for (int c = 0; c < s.pos_channels && c < kMaxD && n < 240; ++c)
+        n += snprintf(buf + n, sizeof(buf) - n, ":%a", (double)s.pos_scale[c]);
+    for (int c = 0; c < 3 && n < 300; ++c) n += snprintf(buf + n, sizeof(buf) - n, ":%a", (double)s.coord_scale[c]);
+    return std::string(buf);
+}
+
+// device (and pinned host) metadata of one batch
+struct MetaLayout {
+    size_t segstat, counts, slotbase, entry, segs, slsegs, total;
+};
+
+MetaLayout layout(int nseg, bool slice_segs) {
+    MetaLayout L;
+    // bytes [0, 64): [0] spare status word, [1] total vertices
+    L.segstat = 64;
+    L.counts = align16(L.segstat + 4 * (size_t)nseg);
+    L.slotbase = align16(L.counts + 4 * (size_t)nseg);
+    L.entry = align16(L.slotbase + 4 * (size_t)(nseg + 1));
+    L.segs = align16(L.entry + 4 * (size_t)(nseg + 1));
+    L.slsegs = align16(L.segs + sizeof(Segment) * nseg);
+    L.total = align16(L.slsegs + (slice_segs ? sizeof(Segment) * nseg : 0));
+    return L;
+}
+
+}  // namespace
+
+int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
+    const int d = B.d, vd = B.vd;
+    const int nseg = (int)B.items.size();
+    if (nseg == 0) return PGPU_OK;
+    const DimOps* ops = dim_ops(d);
+    if (!ops) return fail(PGPU_ERR_UNSUPPORTED, "%d position dimensions (supported: 1..%d)", d, kMaxD);
+    const int vdp = vdp_for(vd);
+    if (!vdp) return fail(PGPU_ERR_UNSUPPORTED, "%d value channels (supported: 1..8)", vd);
+    if (B.payload < 0 || B.payload > 3) return fail(PGPU_ERR_ARGUMENT, "unknown payload %d", B.payload);
+    const int kw = key_words(d);
+    // 16-bit payloads of lattices whose last value channel is the homogeneous weight keep
+    // rows normalised by that weight (see assign_kernel)
+    const bool homog = B.homog && (B.payload == kPayloadF16 || B.payload == kPayloadBF16);
+    const float load = (B.load > 0.05f && B.load <= 0.9f) ? B.load : 0.5f;
+    const size_t accb = accum_bytes(B.payload), payb = payload_bytes(B.payload);
+    const LatticeConsts lc = make_consts(d);
+    const bool dumps = B.rec_vtx || B.dump_splat;
+    const bool graph = B.use_graph && !dumps;
+
+    // points, blocks and first-touch entries, lattice after lattice
+    uint64_t n_total = 0, ns_total = 0;
+    uint64_t blocks = 0, slice_blocks = 0;
+    std::vector<uint32_t> pbase(nseg), bbase(nseg), spbase(nseg), sbbase(nseg);
+    for (int k = 0; k < nseg; ++k) {
+        const BatchItem& it = B.items[k];
+        pbase[k] = (uint32_t)n_total;
+        bbase[k] = (uint32_t)blocks;
+        n_total += it.n;
+        blocks += (it.n + kSplatThreads - 1) / kSplatThreads;
+        const uint64_t ns = B.replay ? it.n : it.n_slice;
+        spbase[k] = (uint32_t)ns_total;
+        sbbase[k] = (uint32_t)slice_blocks;
+        ns_total += ns;
+        slice_blocks += (ns + kSliceThreads - 1) / kSliceThreads;
+    }
+    const uint64_t entries = n_total * (uint64_t)(d + 1);
+    if (entries >= 0xFFFFFFFFull || ns_total * (uint64_t)(d + 1) >= 0xFFFFFFFFull || blocks >= 0x7FFFFFFFull)
+        return fail(PGPU_ERR_UNSUPPORTED, "too many points for one batch (%llu)",
+                    (unsigned long long)n_total);
+    const uint32_t nwords = (uint32_t)((entries + 31) / 32);
+
+    // slots per lattice: (learned vertices per point) x 1.3 x points / load
+    std::vector<std::string> sig(nseg);
+    std::vector<double> ratio(nseg);
+    const double dflt = E.ratio.count(d) ? E.ratio[d] : 1.0;
+    for (int k = 0; k < nseg; ++k) {
+        sig[k] = item_signature(d, B.items[k].splat);
+        auto it = E.ratio_by_sig.find(sig[k]);
+        ratio[k] = it != E.ratio_by_sig.end() ? it->second : dflt;
+    }
+    std::vector<uint64_t> cap(nseg);
+    for (int k = 0; k < nseg; ++k) {
+        const uint64_t n = B.items[k].n;
+        uint64_t est = (uint64_t)std::ceil(ratio[k] * 1.3 * (double)n) + 256;
+        est = std::min<uint64_t>(est, n * (uint64_t)(d + 1) + 256);
+        const uint64_t c = (uint64_t)std::ceil((double)est / load);
+        cap[k] = std::max<uint64_t>((c + 31) & ~31ull, 256);
+    }
+
+    const MetaLayout L = layout(nseg, !B.replay);
+    int rc;
+    if ((rc = E.ensure_hmeta(L.total)) || (rc = E.meta.ensure(L.total))) return rc;
+
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        std::vector<uint64_t> sbase(nseg + 1);
+        uint64_t cap_total = 0;
+        for (int k = 0; k < nseg; ++k) {
+            sbase[k] = cap_total;
+            cap_total += cap[k];
+        }
+        sbase[nseg] = cap_total;
+        if (cap_total > 0x7FFFFF00ull) return fail(PGPU_ERR_CAPACITY, "batch needs more than 2^31 hash slots");
+
+        if ((rc = E.key0.ensure(cap_total * 16)) || (rc = E.keyn.ensure((kw - 1) * cap_total * 16)) ||
+            (rc = E.tvals.ensure(cap_total * vdp * accb)) || (rc = E.ft.ensure(cap_total * 4)) ||
+            (rc = E.slot2vtx.ensure(cap_total * 4)) || (rc = E.bitmap.ensure((size_t)nwords * 4)) ||
+            (rc = E.offs.ensure((size_t)nwords * 4)) ||
+            (rc = E.partials.ensure((size_t)scan_parts(nwords) * 4 + 16)) ||
+            (rc = E.vkey0.ensure(cap_total * 16)) || (rc = E.vkeyn.ensure((kw - 1) * cap_total * 16)) ||
+            (rc = E.vv0.ensure(cap_total * vdp * payb)) || (rc = E.vv1.ensure(cap_total * vdp * payb)) ||
+            (rc = E.nbr.ensure((size_t)(d + 1) * cap_total * 8)) ||
+            (homog && (rc = E.vf32.ensure(cap_total * vdp * 4))) ||
+            (rc = E.vtx2slot.ensure(cap_total * 4)) || (rc = E.sval.ensure(cap_total * vdp * accb)) ||
+            (B.replay && (rc = E.rec.ensure((size_t)entries * 4))))
+            return rc;
+
+        // per-lattice descriptors, staged in pinned memory and uploaded by the first copy
+        unsigned char* h = E.hmeta;
+        uint32_t* hslot = (uint32_t*)(h + L.slotbase);
+        uint32_t* hentry = (uint32_t*)(h + L.entry);
+        Segment* hseg = (Segment*)(h + L.segs);
+        Segment* hsl = (Segment*)(h + L.slsegs);
+        for (int k = 0; k <= nseg; ++k) {
+            hslot[k] = (uint32_t)sbase[k];
+            hentry[k] = k < nseg ? pbase[k] * (uint32_t)(d + 1) : (uint32_t)entries;
+        }
+        for (int k = 0; k < nseg; ++k) {
+            const BatchItem& it = B.items[k];
+            Segment s;
+            memset(&s, 0, sizeof(s));
+            s.src = it.splat;
+            s.out = it.out;
+            s.n = it.n;
+            s.point_base = pbase[k];
+            s.block_base = bbase[k];
+            s.slot_base = (uint32_t)sbase[k];
+            s.cap = (uint32_t)cap[k];
+            hseg[k] = s;
+            if (!B.replay) {
+                s.src = it.slice;
+                s.n = it.n_slice;
+                s.point_base = spbase[k];
+                s.block_base = sbbase[k];
+                hsl[k] = s;
+            }
+        }
+
+        unsigned char* dmeta = (unsigned char*)E.meta.p;
+        uint32_t* dM = (uint32_t*)dmeta + 1;
+        auto enqueue = [&](bool timed) -> int {
+            CUDA_TRY(cudaMemcpyAsync(dmeta + L.slotbase, h + L.slotbase, L.total - L.slotbase,
+                                     cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaMemsetAsync(dmeta, 0, L.slotbase, st));
+            CUDA_TRY(cudaMemsetAsync(E.key0.p, 0xFF, cap_total * 16, st));
+            CUDA_TRY(cudaMemsetAsync(E.tvals.p, 0, cap_total * vdp * accb, st));
+            CUDA_TRY(cudaMemsetAsync(E.ft.p, 0xFF, cap_total * 4, st));
+            CUDA_TRY(cudaMemsetAsync(E.bitmap.p, 0, (size_t)nwords * 4, st));
+            if (timed) CUDA_TRY(cudaEventRecord(E.ev[0], st));
+
+            SplatArgs sa;
+            sa.segs = (const Segment*)(dmeta + L.segs);
+            sa.nseg = nseg;
+            sa.n_total = (uint32_t)n_total;
+            sa.lc = lc;
+            sa.key0 = (uint4*)E.key0.p;
+            sa.keyn = (uint4*)E.keyn.p;
+            sa.cap_total = (uint32_t)cap_total;
+            sa.vals = E.tvals.p;
+            sa.ft = (uint32_t*)E.ft.p;
+            sa.rec_slot = B.replay ? (uint32_t*)E.rec.p : nullptr;
+            sa.seg_status = (unsigned*)(dmeta + L.segstat);
+            sa.blocks = (uint32_t)blocks;
+            if (!ops->splat(sa, vdp, B.payload, st)) return fail(PGPU_ERR_UNSUPPORTED, "splat variant");
+            CUDA_TRY(cudaGetLastError());
+            if (timed) CUDA_TRY(cudaEventRecord(E.ev[1], st));
+
+            launch_mark((const uint32_t*)E.ft.p, (uint32_t)cap_total, (uint32_t*)E.bitmap.p, E.sms, st);
+            launch_scan((const uint32_t*)E.bitmap.p, nwords, (uint32_t*)E.partials.p,
+                        (uint32_t*)E.offs.p, dM, st);
+            launch_segment_counts((const uint32_t*)E.bitmap.p, (const uint32_t*)E.offs.p, nwords, dM,
+                                  (const uint32_t*)(dmeta + L.entry), nseg,
+                                  (uint32_t*)(dmeta + L.counts), st);
+            CompactArgs ca;
+            memset(&ca, 0, sizeof(ca));
+            ca.table = TableView{(uint4*)E.key0.p, (uint4*)E.keyn.p, (uint32_t)cap_total, (uint32_t)cap_total};
+            ca.ft = (const uint32_t*)E.ft.p;
+            ca.bitmap = (uint32_t*)E.bitmap.p;
+            ca.nwords = nwords;
+            ca.offs = (const uint32_t*)E.offs.p;
+            ca.slot2vtx = (uint32_t*)E.slot2vtx.p;
+            ca.vtx2slot = (uint32_t*)E.vtx2slot.p;
+            ca.vkey0 = (uint4*)E.vkey0.p;
+            ca.vkeyn = (uint4*)E.vkeyn.p;
+            ca.vcap = (uint32_t)cap_total;
+            ca.tvals = E.tvals.p;
+            ca.vvals = homog ? E.vf32.p : E.vv0.p;
+            ca.wc = vd - 1;
+            if (!launch_assign(ca, kw, vdp, B.payload, homog, E.sms, st))
+                return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
+            CUDA_TRY(cudaGetLastError());
+            if (B.dump_splat)
+                CUDA_TRY(cudaMemcpyAsync(B.dump_splat, E.vv0.p,
+                                         std::min<size_t>(cap_total * vdp * payb, B.dump_bytes),
+                                         cudaMemcpyDeviceToDevice, st));
+            if (timed) CUDA_TRY(cudaEventRecord(E.ev[2], st));
+
+            NbrArgs na;
+            na.key0 = (uint4*)E.key0.p;
+            na.keyn = (uint4*)E.keyn.p;
+            na.cap_total = (uint32_t)cap_total;
+            na.seg_slot_base = (const uint32_t*)(dmeta + L.slotbase);
+            na.nseg = nseg;
+            na.vtx2slot = (const uint32_t*)E.vtx2slot.p;
+            na.slot2vtx = (const uint32_t*)E.slot2vtx.p;
+            na.vkey0 = (const uint4*)E.vkey0.p;
+            na.vkeyn = (const uint4*)E.vkeyn.p;
+            na.vcap = (uint32_t)cap_total;
+            na.nverts = dM;
+            na.nbr = (int2*)E.nbr.p;
+            ops->neighbours(na, (uint32_t)cap_total, E.sms, st);
+            CUDA_TRY(cudaGetLastError());
+            if (timed) CUDA_TRY(cudaEventRecord(E.ev[3], st));
+
+            BlurPlan bp;
+            bp.d = d;
+            bp.vdp = vdp;
+            bp.payload = B.payload;
+            bp.homog = homog;
+            bp.src_f32 = homog;
+            bp.nbr = (const int2*)E.nbr.p;
+            bp.nbr_stride = cap_total;
+            bp.nverts = dM;
+            bp.vmax = (uint32_t)cap_total;
+            bp.src = homog ? E.vf32.p : E.vv0.p;
+            bp.bufs[0] = E.vv1.p;
+            bp.bufs[1] = E.vv0.p;
+            bp.sval = E.sval.p;
+            bp.vtx2slot = (const uint32_t*)E.vtx2slot.p;
+            bp.wc = vd - 1;
+            bp.sms = E.sms;
+            if (blur_all_axes(bp, st)) return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
+            CUDA_TRY(cudaGetLastError());
+            if (timed) CUDA_TRY(cudaEventRecord(E.ev[4], st));
+
+            SliceArgs sl;
+            sl.segs = (const Segment*)(dmeta + (B.replay ? L.segs : L.slsegs));
+            sl.nseg = nseg;
+            sl.n_total = (uint32_t)n_total;
+            sl.lc = lc;
+            sl.key0 = (uint4*)E.key0.p;
+            sl.keyn = (uint4*)E.keyn.p;
+            sl.cap_total = (uint32_t)cap_total;
+            sl.slot2vtx = (const uint32_t*)E.slot2vtx.p;
+            sl.rec_slot = B.replay ? (const uint32_t*)E.rec.p : nullptr;
+            sl.svals = E.sval.p;
+            sl.vd = vd;
+            sl.rec_vtx = B.rec_vtx;
+            sl.rec_w = B.rec_w;
+            sl.seg_status = (unsigned*)(dmeta + L.segstat);
+            sl.blocks = (uint32_t)slice_blocks;
+            if (!ops->slice(sl, vdp, B.payload, homog, st)) return fail(PGPU_ERR_UNSUPPORTED, "slice variant");
+            CUDA_TRY(cudaGetLastError());
+            if (timed) CUDA_TRY(cudaEventRecord(E.ev[5], st));
+            CUDA_TRY(cudaMemcpyAsync(h, dmeta, L.slotbase, cudaMemcpyDeviceToHost, st));
+            return PGPU_OK;
+        };
+
+        if (graph) {
+            // the graph bakes in sizes and buffer addresses, so both key it
+            char key[256];
+            snprintf(key, sizeof(key), "%d:%d:%d:%d:%d:%d:%llu:%llu:%llu:%u:%p:%p:%p:%p:%p:%p:%p", d, vd,
+                     B.payload, (int)homog, (int)B.replay, nseg, (unsigned long long)n_total,
+                     (unsigned long long)ns_total, (unsigned long long)cap_total, nwords, E.key0.p,
+                     E.tvals.p, E.nbr.p, E.rec.p, E.meta.p, (void*)E.hmeta, E.sval.p);
+            std::string gk(key);
+            for (int k = 0; k < nseg; ++k) gk += ":" + std::to_string(cap[k]) + "/" + std::to_string(B.items[k].n);
+            auto it = E.graphs.find(gk);
+            if (it == E.graphs.end()) {
+                if (E.graphs.size() >= 32) E.drop_graphs();
+                cudaGraph_t g = nullptr;
+                CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                const int erc = enqueue(false);
+                const cudaError_t ce = cudaStreamEndCapture(st, &g);
+                if (erc) {
+                    if (g) cudaGraphDestroy(g);
+                    return erc;
+                }
+                if (ce != cudaSuccess) return fail(PGPU_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+                cudaGraphExec_t ex = nullptr;
+                const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+                cudaGraphDestroy(g);
+                if (ie != cudaSuccess) return fail(PGPU_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+                it = E.graphs.emplace(gk, ex).first;
+            }
+            CUDA_TRY(cudaEventRecord(E.ev[0], st));
+            CUDA_TRY(cudaGraphLaunch(it->second, st));
+            CUDA_TRY(cudaEventRecord(E.ev[5], st));
+        } else {
+            if ((rc = enqueue(true))) return rc;
+        }
+        CUDA_TRY(cudaStreamSynchronize(st));
+
+        const uint32_t M = ((const uint32_t*)h)[1];
+        const unsigned* segstat = (const unsigned*)(h + L.segstat);
+        const uint32_t* counts = (const uint32_t*)(h + L.counts);
+        bool retry = false;
+        for (int k = 0; k < nseg; ++k) {
+            if (segstat[k] & kStatusKeyRange)
+                return fail(PGPU_ERR_ARGUMENT,
+                            "image %d: positions leave the lattice's int16 key range (the reference's "
+                            "keys wrap there and its rank indices leave [0, d]); scale them down", k);
+            if (segstat[k] & (kStatusProbeLimit | kStatusSpinLimit)) {
+                cap[k] = std::max<uint64_t>((uint64_t)(cap[k] * 2.5), (uint64_t)(counts[k] / load * 2));
+                cap[k] = (cap[k] + 31) & ~31ull;
+                retry = true;
+            }
+        }
+        if (retry) continue;
+
+        double rmax = 0.0;
+        for (int k = 0; k < nseg; ++k) {
+            if (!B.items[k].n) continue;
+            const double r = (double)counts[k] / (double)B.items[k].n;
+            E.ratio_by_sig[sig[k]] = r;
+            rmax = std::max(rmax, r);
+        }
+        if (E.ratio_by_sig.size() > 4096) E.ratio_by_sig.clear();
+        E.ratio[d] = rmax;
+        E.last_cap = cap_total;
+        if (B.vertices_out) B.vertices_out->assign(counts, counts + nseg);
+
+        pgpu_stats s;
+        memset(&s, 0, sizeof(s));
+        s.points = (long long)n_total;
+        s.vertices = M;
+        s.capacity = (long long)cap_total;
+        s.d = d;
+        s.vd = vd;
+        s.payload = B.payload;
+        s.retries = attempt;
+        if (!graph) {
+            cudaEventElapsedTime(&s.ms_splat, E.ev[0], E.ev[1]);
+            cudaEventElapsedTime(&s.ms_compact, E.ev[1], E.ev[2]);
+            cudaEventElapsedTime(&s.ms_neighbours, E.ev[2], E.ev[3]);
+            cudaEventElapsedTime(&s.ms_blur, E.ev[3], E.ev[4]);
+            cudaEventElapsedTime(&s.ms_slice, E.ev[4], E.ev[5]);
+        }
+        cudaEventElapsedTime(&s.ms_total, E.ev[0], E.ev[5]);
+        set_stats(s);
+        return PGPU_OK;
+    }
+    return fail(PGPU_ERR_CAPACITY, "hash table overfull after retries (d=%d, %d images)", d, nseg);
+}
+
+}  // namespace pgpu

@@ -141,184 +141,29 @@ int vdp_for(int vd) { return vd <= 2 ? 2 : vd <= 4 ? 4 : vd <= 8 ? 8 : 0; }
 // one lattice: splat, compact, neighbours, blur, slice
 // ---------------------------------------------------------------------------------
 int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
-    const int d = J.d, vd = J.vd;
-    const DimOps* ops = dim_ops(d);
-    if (!ops) return fail(PGPU_ERR_UNSUPPORTED, "%d position dimensions (supported: 1..%d)", d, kMaxD);
-    const int vdp = vdp_for(vd);
-    if (!vdp) return fail(PGPU_ERR_UNSUPPORTED, "%d value channels (supported: 1..8)", vd);
-    if (J.payload < 0 || J.payload > 3) return fail(PGPU_ERR_ARGUMENT, "unknown payload %d", J.payload);
-    const int kw = key_words(d);
-    const uint64_t entries = (uint64_t)J.n * (uint64_t)(d + 1);
-    if (entries >= 0xFFFFFFFFull) return fail(PGPU_ERR_UNSUPPORTED, "too many points for one lattice (%u)", J.n);
-    const uint32_t nwords = (uint32_t)((entries + 31) / 32);
-    const float load = (J.load > 0.05f && J.load <= 0.9f) ? J.load : 0.5f;
-    const LatticeConsts lc = make_consts(d);
-    const size_t accb = accum_bytes(J.payload), payb = payload_bytes(J.payload);
-    // 16-bit payloads of a lattice whose last value channel is the homogeneous weight store
-    // rows normalised by that weight (see assign_kernel)
-    const bool homog = J.homog && (J.payload == kPayloadF16 || J.payload == kPayloadBF16);
-
-    double ratio = 1.0;
-    {
-        auto it = E.ratio.find(d);
-        if (it != E.ratio.end()) ratio = it->second;
-    }
-    uint64_t cap = 0;
-    for (int attempt = 0; attempt < 4; ++attempt) {
-        uint64_t est = (uint64_t)std::ceil(ratio * 1.3 * (double)J.n) + 1024;
-        if (est > entries + 1024) est = entries + 1024;
-        uint64_t want = (uint64_t)std::ceil((double)est / load);
-        if (attempt > 0 && want <= cap) want = cap * 2;
-        cap = (want + 255) & ~255ull;
-        if (cap < 1024) cap = 1024;
-        if (cap > 0x7FFFFF00ull) return fail(PGPU_ERR_CAPACITY, "lattice needs more than 2^31 slots");
-
-        int rc;
-        if ((rc = E.key0.ensure(cap * 16)) || (rc = E.keyn.ensure((kw - 1) * cap * 16)) ||
-            (rc = E.tvals.ensure(cap * vdp * accb)) || (rc = E.ft.ensure(cap * 4)) ||
-            (rc = E.slot2vtx.ensure(cap * 4)) || (rc = E.bitmap.ensure((size_t)nwords * 4)) ||
-            (rc = E.offs.ensure((size_t)nwords * 4)) ||
-            (rc = E.partials.ensure((size_t)scan_parts(nwords) * 4 + 16)) ||
-            (rc = E.vkey0.ensure(cap * 16)) || (rc = E.vkeyn.ensure((kw - 1) * cap * 16)) ||
-            (rc = E.vv0.ensure(cap * vdp * payb)) || (rc = E.vv1.ensure(cap * vdp * payb)) ||
-            (rc = E.nbr.ensure((size_t)(d + 1) * cap * 8)) || (rc = E.dstat.ensure(64)) ||
-            (homog && (rc = E.vf32.ensure(cap * vdp * 4))) ||
-            (rc = E.vtx2slot.ensure(cap * 4)) || (rc = E.sval.ensure(cap * vdp * accb)) ||
-            (J.replay && (rc = E.rec.ensure((size_t)entries * 4))))
-            return rc;
-
-        unsigned* dstatus = (unsigned*)E.dstat.p;
-        uint32_t* dM = (uint32_t*)E.dstat.p + 1;
-        CUDA_TRY(cudaMemsetAsync(E.key0.p, 0xFF, cap * 16, st));
-        CUDA_TRY(cudaMemsetAsync(E.tvals.p, 0, cap * vdp * accb, st));
-        CUDA_TRY(cudaMemsetAsync(E.ft.p, 0xFF, cap * 4, st));
-        CUDA_TRY(cudaMemsetAsync(E.bitmap.p, 0, (size_t)nwords * 4, st));
-        CUDA_TRY(cudaMemsetAsync(E.dstat.p, 0, 64, st));
-        CUDA_TRY(cudaEventRecord(E.ev[0], st));
-
-        TableView tv{(uint4*)E.key0.p, (uint4*)E.keyn.p, (uint32_t)cap};
-        SplatArgs sa;
-        sa.src = J.splat;
-        sa.n = J.n;
-        sa.lc = lc;
-        sa.table = tv;
-        sa.vals = E.tvals.p;
-        sa.ft = (uint32_t*)E.ft.p;
-        sa.rec_slot = J.replay ? (uint32_t*)E.rec.p : nullptr;
-        sa.status = dstatus;
-        if (!ops->splat(sa, vdp, J.payload, st)) return fail(PGPU_ERR_UNSUPPORTED, "splat variant");
-        CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaEventRecord(E.ev[1], st));
-
-        launch_mark((const uint32_t*)E.ft.p, (uint32_t)cap, (uint32_t*)E.bitmap.p, E.sms, st);
-        launch_scan((const uint32_t*)E.bitmap.p, nwords, (uint32_t*)E.partials.p,
-                    (uint32_t*)E.offs.p, dM, st);
-        CompactArgs ca;
-        ca.table = tv;
-        ca.ft = (const uint32_t*)E.ft.p;
-        ca.bitmap = (uint32_t*)E.bitmap.p;
-        ca.nwords = nwords;
-        ca.offs = (const uint32_t*)E.offs.p;
-        ca.slot2vtx = (uint32_t*)E.slot2vtx.p;
-        ca.vtx2slot = (uint32_t*)E.vtx2slot.p;
-        ca.vkey0 = (uint4*)E.vkey0.p;
-        ca.vkeyn = (uint4*)E.vkeyn.p;
-        ca.vcap = (uint32_t)cap;
-        ca.tvals = E.tvals.p;
-        ca.vvals = homog ? E.vf32.p : E.vv0.p;
-        ca.wc = vd - 1;
-        if (!launch_assign(ca, kw, vdp, J.payload, homog, E.sms, st))
-            return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
-        CUDA_TRY(cudaGetLastError());
-        if (J.dump_splat)
-            CUDA_TRY(cudaMemcpyAsync(J.dump_splat, E.vv0.p, std::min<size_t>(cap * vdp * payb, J.dump_bytes),
-                                     cudaMemcpyDeviceToDevice, st));
-        CUDA_TRY(cudaEventRecord(E.ev[2], st));
-
-        NbrArgs na;
-        na.table = tv;
-        na.slot2vtx = (const uint32_t*)E.slot2vtx.p;
-        na.vkey0 = (const uint4*)E.vkey0.p;
-        na.vkeyn = (const uint4*)E.vkeyn.p;
-        na.vcap = (uint32_t)cap;
-        na.nverts = dM;
-        na.nbr = (int2*)E.nbr.p;
-        ops->neighbours(na, (uint32_t)cap, E.sms, st);
-        CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaEventRecord(E.ev[3], st));
-
-        BlurPlan bp;
-        bp.d = d;
-        bp.vdp = vdp;
-        bp.payload = J.payload;
-        bp.homog = homog;
-        bp.src_f32 = homog;
-        bp.nbr = (const int2*)E.nbr.p;
-        bp.nbr_stride = cap;
-        bp.nverts = dM;
-        bp.vmax = (uint32_t)cap;
-        bp.src = homog ? E.vf32.p : E.vv0.p;
-        bp.bufs[0] = E.vv1.p;
-        bp.bufs[1] = E.vv0.p;
-        bp.sval = E.sval.p;
-        bp.vtx2slot = (const uint32_t*)E.vtx2slot.p;
-        bp.wc = vd - 1;
-        bp.sms = E.sms;
-        if (blur_all_axes(bp, st)) return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
-        CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaEventRecord(E.ev[4], st));
-
-        SliceArgs sl;
-        sl.src = J.replay ? J.splat : J.slice;
-        sl.n = J.replay ? J.n : J.n_slice;
-        sl.lc = lc;
-        sl.table = tv;
-        sl.slot2vtx = (const uint32_t*)E.slot2vtx.p;
-        sl.rec_slot = J.replay ? (const uint32_t*)E.rec.p : nullptr;
-        sl.svals = E.sval.p;
-        sl.vd = vd;
-        sl.out = J.out;
-        sl.rec_vtx = J.rec_vtx;
-        sl.rec_w = J.rec_w;
-        sl.status = dstatus;
-        if (!ops->slice(sl, vdp, J.payload, homog, st)) return fail(PGPU_ERR_UNSUPPORTED, "slice variant");
-        CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaEventRecord(E.ev[5], st));
-        CUDA_TRY(cudaMemcpyAsync(E.hstat, E.dstat.p, 16, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaStreamSynchronize(st));
-
-        const unsigned status = E.hstat[0];
-        const uint32_t M = E.hstat[1];
-        if (status & kStatusKeyRange)
-            return fail(PGPU_ERR_ARGUMENT,
-                        "positions leave the lattice's int16 key range (the reference's keys "
-                        "wrap there and its rank indices leave [0, d]); scale them down");
-        if (status & (kStatusProbeLimit | kStatusSpinLimit)) {
-            ratio = std::max(ratio * 2.5, (double)M / std::max<uint32_t>(J.n, 1));
-            continue;
-        }
-        if (J.n) E.ratio[d] = (double)M / (double)J.n;
-        E.last_cap = cap;
-        pgpu_stats s;
-        memset(&s, 0, sizeof(s));
-        s.points = J.n;
-        s.vertices = M;
-        s.capacity = (long long)cap;
-        s.d = d;
-        s.vd = vd;
-        s.payload = J.payload;
-        s.retries = attempt;
-        cudaEventElapsedTime(&s.ms_splat, E.ev[0], E.ev[1]);
-        cudaEventElapsedTime(&s.ms_compact, E.ev[1], E.ev[2]);
-        cudaEventElapsedTime(&s.ms_neighbours, E.ev[2], E.ev[3]);
-        cudaEventElapsedTime(&s.ms_blur, E.ev[3], E.ev[4]);
-        cudaEventElapsedTime(&s.ms_slice, E.ev[4], E.ev[5]);
-        cudaEventElapsedTime(&s.ms_total, E.ev[0], E.ev[5]);
-        set_stats(s);
-        if (J.vertices_out) *J.vertices_out = M;
-        return PGPU_OK;
-    }
-    return fail(PGPU_ERR_CAPACITY, "hash table overfull after retries (d=%d, n=%u)", d, J.n);
+    BatchJob B;
+    B.d = J.d;
+    B.vd = J.vd;
+    B.payload = J.payload;
+    B.load = J.load;
+    B.homog = J.homog;
+    B.replay = J.replay;
+    BatchItem it;
+    it.splat = J.splat;
+    it.n = J.n;
+    it.slice = J.slice;
+    it.n_slice = J.n_slice;
+    it.out = J.out;
+    B.items.push_back(it);
+    B.rec_vtx = J.rec_vtx;
+    B.rec_w = J.rec_w;
+    B.dump_splat = J.dump_splat;
+    B.dump_bytes = J.dump_bytes;
+    std::vector<uint32_t> counts;
+    B.vertices_out = &counts;
+    const int rc = run_batch(E, B, st);
+    if (rc == PGPU_OK && J.vertices_out) *J.vertices_out = counts.empty() ? 0 : counts[0];
+    return rc;
 }
 
 // ---------------------------------------------------------------------------------
@@ -649,6 +494,82 @@ int pgpu_joint_bilateral(pgpu_image* im, const pgpu_image* ref, float filter_wid
 int pgpu_bilateral(pgpu_image* im, float filter_width, float filter_height, float filter_frames,
                    float color_sigma, const pgpu_options* opt) {
     return pgpu_joint_bilateral(im, im, filter_width, filter_height, filter_frames, color_sigma, opt);
+}
+
+int pgpu_bilateral_batch(pgpu_image* ims, int count, const float* filter_width,
+                         const float* color_sigma, const pgpu_options* opt_in) {
+    const pgpu_options opt = opts_or_default(opt_in);
+    if (count < 0 || (count > 0 && (!ims || !filter_width || !color_sigma)))
+        return fail(PGPU_ERR_ARGUMENT, "invalid batch arguments");
+    if (count == 0) return PGPU_OK;
+    const int C = ims[0].channels;
+    if (C + 1 > 8) return fail(PGPU_ERR_UNSUPPORTED, "%d image channels (supported: 1..7)", C);
+    for (int i = 0; i < count; ++i) {
+        const pgpu_image& v = ims[i];
+        const float fw = filter_width[i];
+        if (!view_ok(&v) || v.channels != C || v.frames != 1)
+            return fail(PGPU_ERR_ARGUMENT, "batch image %d: single-frame images with %d channels expected", i, C);
+        // every image must have both pixel axes as positions (d = C + 2), as
+        // JointBilateral::apply makes them for fw < 10 x the size (src/GaussTransform.cpp:541-542)
+        if (v.width < 2 || v.height < 2 || !(fw > 0) || !(fw < 10 * v.width) || !(fw < 10 * v.height) ||
+            !(color_sigma[i] > 0))
+            return fail(PGPU_ERR_UNSUPPORTED,
+                        "batch image %d: needs width, height > 1 and 0 < filter width < 10 x its "
+                        "width and height (filter it with pgpu_bilateral)", i);
+    }
+    ApiScope S(&opt);
+    if (S.rc) return S.rc;
+    Engine& E = *S.E;
+    std::vector<pgpu_image> dv(ims, ims + count);
+    int rc;
+    if (opt.memory != PGPU_MEM_DEVICE) {   // one staging buffer for the whole batch
+        size_t total = 0;
+        for (int i = 0; i < count; ++i) total += (size_t)ims[i].width * ims[i].height * C;
+        if ((rc = E.img_a.ensure(total * sizeof(float)))) return rc;
+        size_t off = 0;
+        for (int i = 0; i < count; ++i) {
+            dv[i] = dense_like(ims[i], (float*)E.img_a.p + off, C);
+            off += (size_t)ims[i].width * ims[i].height * C;
+            if ((rc = copy_view(ims[i], dv[i], C, cudaMemcpyHostToDevice, S.st))) return rc;
+        }
+    }
+    BatchJob B;
+    B.d = C + 2;
+    B.vd = C + 1;
+    B.payload = opt.payload;
+    B.load = opt.load_factor;
+    B.homog = true;
+    B.replay = true;
+    B.use_graph = (opt.flags & PGPU_FLAG_GRAPH) != 0;
+    B.items.resize(count);
+    volatile float one = 1.0f;
+    for (int i = 0; i < count; ++i) {
+        BatchItem& it = B.items[i];
+        PointSource& s = it.splat;
+        memset(&s, 0, sizeof(s));
+        s.width = dv[i].width;
+        s.height = dv[i].height;
+        s.frames = 1;
+        s.pos = planar(dv[i]);
+        s.pos_channels = C;
+        const float inv_r = one / color_sigma[i];
+        for (int c = 0; c < C; ++c) s.pos_scale[c] = inv_r;
+        s.coord_mask = 3;
+        s.coord_scale[0] = one / filter_width[i];
+        s.coord_scale[1] = one / filter_width[i];
+        s.val = planar(dv[i]);
+        s.val_channels = C;
+        s.homogeneous = 1;
+        it.n = (uint32_t)((size_t)dv[i].width * dv[i].height);
+        it.out = outview(dv[i], C, 1);
+    }
+    if ((rc = run_batch(E, B, S.st))) return rc;
+    if (opt.memory != PGPU_MEM_DEVICE) {
+        for (int i = 0; i < count; ++i)
+            if ((rc = copy_view(dv[i], ims[i], C, cudaMemcpyDeviceToHost, S.st))) return rc;
+        CUDA_TRY(cudaStreamSynchronize(S.st));
+    }
+    return PGPU_OK;
 }
 
 int pgpu_lattice_dump(int d, int vd, int n, const float* pos, const float* val, int payload,

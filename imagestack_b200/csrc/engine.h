@@ -4,8 +4,11 @@
 
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
+#include <vector>
 
 #include "../../include/permgpu.h"
 #include "lattice_ops.h"
@@ -51,17 +54,53 @@ struct Engine {
     DevBuf sval;       // filtered rows in slot space, arithmetic type, read by the slice
     DevBuf rec;        // slot of every (point, remainder), [r][n], recorded by the splat
     DevBuf dstat;
+    // batch metadata: statuses, counts, segment tables (device copy of hmeta)
+    DevBuf meta;
+    unsigned char* hmeta = nullptr;   // pinned host mirror
+    size_t hmeta_bytes = 0;
     // staging images for host-memory calls
     DevBuf img_a, img_b, img_c, img_d;
     unsigned* hstat = nullptr;
     cudaEvent_t ev[8] = {};
-    std::map<int, double> ratio;   // learned vertices per point, by d
+    std::map<int, double> ratio;                  // vertices per point of recent lattices, by d
+    std::map<std::string, double> ratio_by_sig;   // ... by image shape and scales
+    std::map<std::string, cudaGraphExec_t> graphs;  // captured batch pipelines, by batch shape
     size_t last_cap = 0;
+    uint64_t buffers_epoch = 0;   // bumped whenever a buffer moves (invalidates graphs)
     int init(int dev);
+    int ensure_hmeta(size_t bytes);
+    void drop_graphs();
 };
 
 int get_engine(int dev, Engine** out);
 int device_count_sm100();
+
+// One image of a batch.
+struct BatchItem {
+    PointSource splat;     // its points
+    uint32_t n = 0;
+    PointSource slice;     // slice positions when the job does not replay
+    uint32_t n_slice = 0;
+    OutView out;
+};
+
+// Lattices that share d, value channels and payload, run by the same launches.
+struct BatchJob {
+    int d = 0, vd = 0, payload = 0;
+    float load = 0.5f;
+    bool homog = false;    // the last value channel is the homogeneous weight
+    bool replay = true;    // slice at the splat points
+    bool use_graph = false;   // capture / replay the launch sequence as a CUDA graph
+    std::vector<BatchItem> items;
+    // parity dumps (single-item jobs)
+    int* rec_vtx = nullptr;
+    float* rec_w = nullptr;
+    void* dump_splat = nullptr;
+    size_t dump_bytes = 0;
+    // results
+    std::vector<uint32_t>* vertices_out = nullptr;   // per item
+};
+int run_batch(Engine& E, const BatchJob& B, cudaStream_t st);
 
 struct LatticeJob {
     int d = 0, vd = 0, payload = 0;

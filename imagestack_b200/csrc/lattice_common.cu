@@ -89,6 +89,32 @@ scan_down_kernel(const uint32_t* __restrict__ bitmap, uint32_t nwords,
     }
 }
 
+// Vertices of each segment of a batch: first touches are numbered segment after segment,
+// so segment k owns the first-touch bits in [entry[k], entry[k+1]).
+__device__ __forceinline__ uint32_t bits_before(const uint32_t* bitmap, const uint32_t* offs,
+                                                uint32_t nwords, uint32_t total, uint32_t e) {
+    const uint32_t w = e >> 5;
+    if (w >= nwords) return total;
+    return offs[w] + __popc(bitmap[w] & ((1u << (e & 31u)) - 1u));
+}
+
+__global__ void segment_counts_kernel(const uint32_t* bitmap, const uint32_t* offs, uint32_t nwords,
+                                      const uint32_t* total, const uint32_t* entry, int nseg,
+                                      uint32_t* counts) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nseg) return;
+    const uint32_t t = *total;
+    counts[k] = bits_before(bitmap, offs, nwords, t, entry[k + 1]) -
+                bits_before(bitmap, offs, nwords, t, entry[k]);
+}
+
+void launch_segment_counts(const uint32_t* bitmap, const uint32_t* offs, uint32_t nwords,
+                           const uint32_t* total, const uint32_t* entry, int nseg, uint32_t* counts,
+                           cudaStream_t st) {
+    segment_counts_kernel<<<(nseg + 127) / 128, 128, 0, st>>>(bitmap, offs, nwords, total, entry,
+                                                              nseg, counts);
+}
+
 // ---------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------

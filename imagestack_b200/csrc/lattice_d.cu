@@ -22,8 +22,7 @@ int grid_cap(uint64_t work, int threads, int sms) {
 
 template <int VDP, typename Acc>
 void splat_t(const SplatArgs& a, cudaStream_t st) {
-    const uint32_t blocks = (a.n + kSplatThreads - 1) / kSplatThreads;
-    if (blocks) splat_kernel<D, VDP, Acc><<<blocks, kSplatThreads, 0, st>>>(a);
+    if (a.blocks) splat_kernel<D, VDP, Acc><<<a.blocks, kSplatThreads, 0, st>>>(a);
 }
 
 bool splat(const SplatArgs& a, int vdp, int payload, cudaStream_t st) {
@@ -42,8 +41,7 @@ void neighbours(const NbrArgs& a, uint32_t vmax, int sms, cudaStream_t st) {
 
 template <int VDP, typename A, bool HOMOG>
 void slice_t(const SliceArgs& a, cudaStream_t st) {
-    const uint32_t blocks = (a.n + kSliceThreads - 1) / kSliceThreads;
-    if (blocks) slice_kernel<D, VDP, A, HOMOG><<<blocks, kSliceThreads, 0, st>>>(a);
+    if (a.blocks) slice_kernel<D, VDP, A, HOMOG><<<a.blocks, kSliceThreads, 0, st>>>(a);
 }
 
 // the slice reads the last blur pass's rows: FP64 for the FP64 lattice, FP32 otherwise;

@@ -133,9 +133,10 @@ __device__ __forceinline__ uint32_t key_hash(const Key<KW>& k) {
 // (src/Permutohedral.h:69-75).
 // ---------------------------------------------------------------------------------
 struct TableView {
-    uint4* key0;
-    uint4* keyn;
-    uint32_t cap;
+    uint4* key0;       // word 0 of slot 0 of this table (a segment of a batch's slot array)
+    uint4* keyn;       // word 1 of slot 0; word w at keyn[(w-1)*stride + s]
+    uint32_t cap;      // slots of this table
+    uint32_t stride;   // slots of the whole array
 };
 
 __device__ __forceinline__ uint32_t home_slot(uint32_t h, uint32_t cap) { return __umulhi(h, cap); }
@@ -158,7 +159,7 @@ __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home,
             if (is_empty_word(w)) {
                 if (KW > 1) {
 #pragma unroll
-                    for (int i = 1; i < KW; ++i) __stcg(&t.keyn[(size_t)(i - 1) * t.cap + s], k.w[i]);
+                    for (int i = 1; i < KW; ++i) __stcg(&t.keyn[(size_t)(i - 1) * t.stride + s], k.w[i]);
                     __threadfence();
                     atomicExch(&t.key0[s], k.w[0]);
                 }
@@ -181,7 +182,7 @@ __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home,
             bool same = true;
 #pragma unroll
             for (int i = 1; i < KW; ++i)
-                same = same && words_equal(__ldcg(&t.keyn[(size_t)(i - 1) * t.cap + s]), k.w[i]);
+                same = same && words_equal(__ldcg(&t.keyn[(size_t)(i - 1) * t.stride + s]), k.w[i]);
             if (same) return (int)s;
         }
         s = (s + 1 == t.cap) ? 0u : s + 1;
@@ -203,7 +204,7 @@ __device__ __forceinline__ int table_find(const TableView& t, const Key<KW>& k, 
             bool same = true;
 #pragma unroll
             for (int i = 1; i < KW; ++i)
-                same = same && words_equal(__ldg(&t.keyn[(size_t)(i - 1) * t.cap + s]), k.w[i]);
+                same = same && words_equal(__ldg(&t.keyn[(size_t)(i - 1) * t.stride + s]), k.w[i]);
             if (same) return (int)s;
         }
         s = (s + 1 == t.cap) ? 0u : s + 1;

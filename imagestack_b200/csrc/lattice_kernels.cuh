@@ -54,15 +54,65 @@ struct OutView {
     int normalize;    // 1: out[c] = acc[c] / acc[vd-1] (JointBilateral), 0: out[c] = acc[c]
 };
 
+// One lattice of a batch — one image; the single-image entry points run a batch of one.
+// Each lattice owns a contiguous range of the shared hash-slot array and of the point
+// numbering; its points are numbered after the previous lattice's, so first-touch order,
+// and with it the vertex numbering, stays per-lattice insertion order.
+struct Segment {
+    PointSource src;       // its points
+    OutView out;           // where its slice goes
+    uint32_t n;            // points
+    uint32_t point_base;   // first point in the batch numbering
+    uint32_t block_base;   // first block of the segment in splat / slice launches
+    uint32_t slot_base;    // first slot in the shared hash-slot array
+    uint32_t cap;          // slots
+    uint32_t pad_;
+};
+
+// Segment of block b: the last one whose block_base <= b (segments are in block order).
+__device__ __forceinline__ int segment_of_block(const Segment* segs, int nseg, uint32_t b) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&segs[mid].block_base) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Segment of slot s: the last k with slot_base[k] <= s (slot_base has nseg + 1 entries).
+__device__ __forceinline__ int segment_of_slot(const uint32_t* slot_base, int nseg, uint32_t s) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(slot_base + mid) <= s) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// the block's segment, copied into shared memory by the whole block (ends with a barrier)
+__device__ __forceinline__ void load_segment(const Segment* g, Segment& s) {
+    static_assert(sizeof(Segment) % 4 == 0, "Segment is copied as 32-bit words");
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&s);
+    for (int t = threadIdx.x; t < (int)(sizeof(Segment) / 4); t += blockDim.x) dst[t] = __ldg(src + t);
+    __syncthreads();
+}
+
 struct SplatArgs {
-    PointSource src;
-    uint32_t n;
+    const Segment* segs;
+    int nseg;
+    uint32_t n_total;      // points of the batch
     LatticeConsts lc;
-    TableView table;
-    void* vals;        // cap * VDP accumulators (float or double), zeroed
-    uint32_t* ft;      // cap first-touch entries, all ones
-    uint32_t* rec_slot;   // optional [r][n] slot of every (point, remainder), for the slice
-    unsigned* status;
+    uint4* key0;           // the shared hash-slot array (cap_total slots)
+    uint4* keyn;
+    uint32_t cap_total;
+    void* vals;            // cap_total * VDP accumulators (float or double), zeroed
+    uint32_t* ft;          // cap_total first-touch entries, all ones
+    uint32_t* rec_slot;    // optional [r][n_total] slot of every (point, remainder)
+    unsigned* seg_status;  // one status word per segment
+    uint32_t blocks;       // splat blocks of the batch
 };
 
 struct CompactArgs {
@@ -82,7 +132,12 @@ struct CompactArgs {
 };
 
 struct NbrArgs {
-    TableView table;
+    uint4* key0;           // the shared hash-slot array
+    uint4* keyn;
+    uint32_t cap_total;
+    const uint32_t* seg_slot_base;   // nseg + 1 slot boundaries
+    int nseg;
+    const uint32_t* vtx2slot;
     const uint32_t* slot2vtx;
     const uint4* vkey0;
     const uint4* vkeyn;
@@ -103,19 +158,24 @@ struct BlurArgs {
     int wc;                     // homogeneous weight channel (homogeneous rows only)
 };
 
+// Slice segments are the splat's for the replay slice; for a slice at other positions
+// they carry those positions, with the same slot ranges.
 struct SliceArgs {
-    PointSource src;
-    uint32_t n;
+    const Segment* segs;
+    int nseg;
+    uint32_t n_total;           // points of the batch (the record stride)
     LatticeConsts lc;
-    TableView table;
+    uint4* key0;                // the shared hash-slot array
+    uint4* keyn;
+    uint32_t cap_total;
     const uint32_t* slot2vtx;   // parity dumps only
-    const uint32_t* rec_slot;   // slots recorded by the splat, [r][n]; null: look keys up
+    const uint32_t* rec_slot;   // slots recorded by the splat, [r][n_total]; null: look up
     const void* svals;          // filtered rows in slot space (float, or double)
     int vd;
-    OutView out;
-    int* rec_vtx;          // optional n*(d+1) vertex indices (parity dumps)
-    float* rec_w;          // optional n*(d+1) weights
-    unsigned* status;
+    int* rec_vtx;               // optional (point, remainder) vertex indices (dumps)
+    float* rec_w;               // optional weights
+    unsigned* seg_status;
+    uint32_t blocks;
 };
 
 // ---------------------------------------------------------------------------------
@@ -229,18 +289,25 @@ template <int D, int VDP, typename Acc>
 __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kernel(SplatArgs a) {
     constexpr int KW = key_words(D);
     __shared__ Acc stage[kSplatThreads / 32][32][VDP];
+    __shared__ Segment sg;
+    const int kseg = segment_of_block(a.segs, a.nseg, blockIdx.x);
+    load_segment(a.segs + kseg, sg);
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t i = blockIdx.x * (uint32_t)kSplatThreads + threadIdx.x;
-    const bool valid = i < a.n;
+    const uint32_t i = (blockIdx.x - sg.block_base) * (uint32_t)kSplatThreads + threadIdx.x;
+    const bool valid = i < sg.n;
     const unsigned active = __ballot_sync(0xFFFFFFFFu, valid);
     if (!valid) return;
 
+    unsigned* status = a.seg_status + kseg;
+    const TableView table{a.key0 + sg.slot_base, a.keyn + sg.slot_base, sg.cap, a.cap_total};
     float p[D], v[VDP];
-    load_point<D, VDP>(a.src, i, p, v);
+    load_point<D, VDP>(sg.src, i, p, v);
     Simplex<D> sx;
-    compute_simplex<D>(p, a.lc, sx, a.status);
-    const uint32_t e0 = i * (uint32_t)(D + 1);
-    Acc* vals = reinterpret_cast<Acc*>(a.vals);
+    compute_simplex<D>(p, a.lc, sx, status);
+    const uint32_t gi = sg.point_base + i;   // point number in the batch
+    const uint32_t e0 = gi * (uint32_t)(D + 1);
+    Acc* vals = reinterpret_cast<Acc*>(a.vals) + (size_t)sg.slot_base * VDP;
+    uint32_t* ft = a.ft + sg.slot_base;
 
     // Phase 1: group the lanes that share each vertex key (exact match on all key words);
     // each group's leader starts loading its home slot.  For d <= 8 the loads of all d+1
@@ -262,9 +329,9 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
             pr &= __match_any_sync(active, ((unsigned long long)key.w[w].w << 32) | key.w[w].z);
         }
         peers[r] = pr;
-        home[r] = home_slot(key_hash<KW>(key), a.table.cap);
+        home[r] = home_slot(key_hash<KW>(key), table.cap);
         first[r] = make_uint4(0u, 0u, 0u, 0u);
-        if (kAhead && lane == (unsigned)(__ffs(pr) - 1)) first[r] = __ldcg(&a.table.key0[home[r]]);
+        if (kAhead && lane == (unsigned)(__ffs(pr) - 1)) first[r] = __ldcg(&table.key0[home[r]]);
     }
 
     // Phase 2: per remainder, the group's weighted values are summed by its leader, which
@@ -315,15 +382,16 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
             vertex_coords<D>(sx, r, kc);
             Key<KW> key;
             pack_key<D>(kc, key);
-            const uint4 w0 = kAhead ? first[r] : __ldcg(&a.table.key0[home[r]]);
-            s = table_insert<KW>(a.table, key, home[r], w0, a.status);
+            const uint4 w0 = kAhead ? first[r] : __ldcg(&table.key0[home[r]]);
+            s = table_insert<KW>(table, key, home[r], w0, status);
             if (s >= 0) {
                 atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
-                atomicMin(&a.ft[s], e0 + (uint32_t)r);   // the leader's entry is the group's smallest
+                atomicMin(&ft[s], e0 + (uint32_t)r);   // the leader's entry is the group's smallest
             }
         }
         s = __shfl_sync(active, s, leader);
-        if (a.rec_slot) a.rec_slot[(size_t)r * a.n + i] = (uint32_t)s;
+        if (a.rec_slot)
+            a.rec_slot[(size_t)r * a.n_total + gi] = s >= 0 ? sg.slot_base + (uint32_t)s : 0xFFFFFFFFu;
     }
 }
 
@@ -361,7 +429,7 @@ __global__ void assign_kernel(CompactArgs a) {
             a.vkey0[vtx] = a.table.key0[s];
 #pragma unroll
             for (int k = 1; k < KW; ++k)
-                a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.cap + s];
+                a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.stride + s];
             Acc wt = tvals[(size_t)s * VDP];
 #pragma unroll
             for (int k = 0; k < VDP; ++k) if (k == a.wc) wt = tvals[(size_t)s * VDP + k];
@@ -385,7 +453,7 @@ __global__ void assign_kernel(CompactArgs a) {
         a.vkey0[vtx] = a.table.key0[s];
 #pragma unroll
         for (int k = 1; k < KW; ++k)
-            a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.cap + s];
+            a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.stride + s];
 #pragma unroll
         for (int k = 0; k < VDP; ++k)
             Payload<P>::store(vvals + (size_t)vtx * VDP + k, tvals[(size_t)s * VDP + k]);
@@ -402,6 +470,12 @@ __global__ void neighbours_kernel(NbrArgs a) {
     const uint32_t m = *a.nverts;
     for (uint32_t vtx = blockIdx.x * blockDim.x + threadIdx.x; vtx < m;
          vtx += gridDim.x * blockDim.x) {
+        // neighbours are looked up in the vertex's own lattice only
+        const uint32_t slot = __ldg(a.vtx2slot + vtx);
+        const int kseg = a.nseg > 1 ? segment_of_slot(a.seg_slot_base, a.nseg, slot) : 0;
+        const uint32_t base = __ldg(a.seg_slot_base + kseg);
+        const TableView table{a.key0 + base, a.keyn + base, __ldg(a.seg_slot_base + kseg + 1) - base,
+                              a.cap_total};
         Key<KW> key;
         key.w[0] = a.vkey0[vtx];
 #pragma unroll
@@ -419,10 +493,11 @@ __global__ void neighbours_kernel(NbrArgs a) {
             Key<KW> k1, k2;
             pack_key<D>(n1, k1);
             pack_key<D>(n2, k2);
-            const int s1 = table_find<KW>(a.table, k1, key_hash<KW>(k1));
-            const int s2 = table_find<KW>(a.table, k2, key_hash<KW>(k2));
+            const int s1 = table_find<KW>(table, k1, key_hash<KW>(k1));
+            const int s2 = table_find<KW>(table, k2, key_hash<KW>(k2));
             a.nbr[(size_t)j * a.vcap + vtx] =
-                make_int2(s1 >= 0 ? (int)a.slot2vtx[s1] : -1, s2 >= 0 ? (int)a.slot2vtx[s2] : -1);
+                make_int2(s1 >= 0 ? (int)__ldg(a.slot2vtx + base + s1) : -1,
+                          s2 >= 0 ? (int)__ldg(a.slot2vtx + base + s2) : -1);
         }
     }
 }
@@ -533,36 +608,42 @@ constexpr int kSliceThreads = 256;
 template <int D, int VDP, typename A, bool HOMOG>
 __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
     constexpr int KW = key_words(D);
-    const uint32_t i = blockIdx.x * (uint32_t)kSliceThreads + threadIdx.x;
-    if (i >= a.n) return;
+    __shared__ Segment sg;
+    const int kseg = segment_of_block(a.segs, a.nseg, blockIdx.x);
+    load_segment(a.segs + kseg, sg);
+    const uint32_t i = (blockIdx.x - sg.block_base) * (uint32_t)kSliceThreads + threadIdx.x;
+    if (i >= sg.n) return;
+    unsigned* status = a.seg_status + kseg;
     // A splat that overflowed the table is rerun by the host with more slots; its
     // output may be the caller's input image (in-place filtering), so write nothing.
-    if (__ldcg(a.status) & (kStatusProbeLimit | kStatusSpinLimit | kStatusKeyRange)) return;
+    if (__ldcg(status) & (kStatusProbeLimit | kStatusSpinLimit | kStatusKeyRange)) return;
+    const uint32_t gi = sg.point_base + i;
     float p[D];
-    load_position<D>(a.src, i, p);
+    load_position<D>(sg.src, i, p);
     Simplex<D> sx;
-    compute_simplex<D>(p, a.lc, sx, a.status);
+    compute_simplex<D>(p, a.lc, sx, status);
     const A* sv = reinterpret_cast<const A*>(a.svals);
     A acc[VDP];
 #pragma unroll
     for (int k = 0; k < VDP; ++k) acc[k] = (A)0;
 #pragma unroll
     for (int r = 0; r <= D; ++r) {
-        int s;
+        int s;   // slot in the shared array
         if (a.rec_slot) {
-            s = (int)__ldg(a.rec_slot + (size_t)r * a.n + i);
+            s = (int)__ldg(a.rec_slot + (size_t)r * a.n_total + gi);
         } else {
             int kc[D];
             vertex_coords<D>(sx, r, kc);
             Key<KW> key;
             pack_key<D>(kc, key);
-            const uint32_t h = key_hash<KW>(key);
-            s = table_find<KW>(a.table, key, h);
+            const TableView table{a.key0 + sg.slot_base, a.keyn + sg.slot_base, sg.cap, a.cap_total};
+            const int ls = table_find<KW>(table, key, key_hash<KW>(key));
+            s = ls >= 0 ? (int)sg.slot_base + ls : -1;
         }
         const float w = sx.bary[r];
         if (a.rec_vtx) {
-            a.rec_vtx[(size_t)i * (D + 1) + r] = s >= 0 ? (int)__ldg(a.slot2vtx + s) : -1;
-            a.rec_w[(size_t)i * (D + 1) + r] = w;
+            a.rec_vtx[(size_t)gi * (D + 1) + r] = s >= 0 ? (int)__ldg(a.slot2vtx + s) : -1;
+            a.rec_w[(size_t)gi * (D + 1) + r] = w;
         }
         if (s >= 0) {
             A row[VDP];
@@ -583,14 +664,15 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
         }
     }
     // write
-    const uint32_t wdt = (uint32_t)a.src.width, hgt = (uint32_t)a.src.height;
+    const uint32_t wdt = (uint32_t)sg.src.width, hgt = (uint32_t)sg.src.height;
     const uint32_t x = i % wdt, q = i / wdt, y = q % hgt, t = q / hgt;
-    float* o = a.out.base + (long long)t * a.out.tstride + (long long)y * a.out.ystride + x;
+    const OutView& ov = sg.out;
+    float* o = ov.base + (long long)t * ov.tstride + (long long)y * ov.ystride + x;
 #pragma unroll
     for (int k = 0; k < VDP; ++k) {
-        if (k < a.out.channels) {
+        if (k < ov.channels) {
             float r;
-            if (a.out.normalize) {
+            if (ov.normalize) {
                 A wsum = acc[0];
 #pragma unroll
                 for (int j = 0; j < VDP; ++j) if (j == a.vd - 1) wsum = acc[j];
@@ -598,7 +680,7 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
             } else {
                 r = (float)acc[k];
             }
-            o[(long long)k * a.out.cstride] = r;
+            o[(long long)k * ov.cstride] = r;
         }
     }
 }

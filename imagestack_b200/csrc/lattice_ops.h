@@ -31,6 +31,10 @@ PGPU_DECLARE_DIM(13) PGPU_DECLARE_DIM(14) PGPU_DECLARE_DIM(15) PGPU_DECLARE_DIM(
 const DimOps* dim_ops(int d);
 
 void launch_mark(const uint32_t* ft, uint32_t cap, uint32_t* bitmap, int sms, cudaStream_t st);
+// per-segment vertex counts from the first-touch bitmap and its prefix popcount
+void launch_segment_counts(const uint32_t* bitmap, const uint32_t* offs, uint32_t nwords,
+                           const uint32_t* total, const uint32_t* entry, int nseg, uint32_t* counts,
+                           cudaStream_t st);
 uint32_t scan_parts(uint32_t nwords);
 void launch_scan(const uint32_t* bitmap, uint32_t nwords, uint32_t* partials, uint32_t* offs,
                  uint32_t* total, cudaStream_t st);

@@ -34,8 +34,10 @@ constexpr size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 constexpr size_t kEntries = (size_t)kNoAllocMaxPixels * (kNoAllocMaxD + 1);
 constexpr size_t kWords = (kEntries + 31) / 32;
 constexpr size_t kParts = (kWords + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
-constexpr size_t kOffStatus = 0;
-constexpr size_t kOffKey0 = align_up(kOffStatus + 64);
+constexpr size_t kOffStatus = 0;                                      // status, vertex count
+constexpr size_t kOffSeg = align_up(kOffStatus + 64);                 // the image's descriptor
+constexpr size_t kOffSlotBase = align_up(kOffSeg + sizeof(Segment));  // its slot range
+constexpr size_t kOffKey0 = align_up(kOffSlotBase + 16);
 constexpr size_t kOffTvals = align_up(kOffKey0 + (size_t)kNoAllocSlots * 16);
 constexpr size_t kOffFt = align_up(kOffTvals + (size_t)kNoAllocSlots * kNoAllocVdp * 4);
 constexpr size_t kOffSlot2Vtx = align_up(kOffFt + (size_t)kNoAllocSlots * 4);
@@ -153,17 +155,39 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
 
     const DimOps* ops = dim_ops(d);
     const LatticeConsts lc = make_consts(d);
-    TableView tv{(uint4*)(base + kOffKey0), (uint4*)(base + kOffKey0), cap};
+
+    // the image is a batch of one: its descriptor and slot range go to the array too
+    Segment seg;
+    memset(&seg, 0, sizeof(seg));
+    seg.src = src;
+    seg.out.base = d_out;
+    seg.out.ystride = width;
+    seg.out.tstride = plane;
+    seg.out.cstride = plane;
+    seg.out.channels = channels;
+    seg.out.normalize = 1;
+    seg.n = n;
+    seg.cap = cap;
+    const uint32_t slot_bounds[2] = {0u, cap};
+    CUDA_TRY(cudaMemcpyAsync(base + kOffSeg, &seg, sizeof(seg), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(base + kOffSlotBase, slot_bounds, sizeof(slot_bounds),
+                             cudaMemcpyHostToDevice, st));
+    const Segment* dseg = (const Segment*)(base + kOffSeg);
+    uint4* key0 = (uint4*)(base + kOffKey0);
 
     SplatArgs sa;
-    sa.src = src;
-    sa.n = n;
+    sa.segs = dseg;
+    sa.nseg = 1;
+    sa.n_total = n;
     sa.lc = lc;
-    sa.table = tv;
+    sa.key0 = key0;
+    sa.keyn = key0;
+    sa.cap_total = cap;
     sa.vals = base + kOffTvals;
     sa.ft = (uint32_t*)(base + kOffFt);
     sa.rec_slot = (uint32_t*)(base + kOffRec);
-    sa.status = dstatus;
+    sa.seg_status = dstatus;
+    sa.blocks = (n + kSplatThreads - 1) / kSplatThreads;
     if (!ops->splat(sa, vdp, kPayloadF32, st)) return fail(PGPU_ERR_UNSUPPORTED, "splat variant");
     CUDA_TRY(cudaGetLastError());
 
@@ -172,7 +196,7 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
                 (uint32_t*)(base + kOffOffs), dM, st);
     CompactArgs ca;
     memset(&ca, 0, sizeof(ca));
-    ca.table = tv;
+    ca.table = TableView{key0, key0, cap, cap};
     ca.ft = (const uint32_t*)(base + kOffFt);
     ca.bitmap = (uint32_t*)(base + kOffBitmap);
     ca.nwords = nwords;
@@ -189,7 +213,12 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
         return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
 
     NbrArgs na;
-    na.table = tv;
+    na.key0 = key0;
+    na.keyn = key0;
+    na.cap_total = cap;
+    na.seg_slot_base = (const uint32_t*)(base + kOffSlotBase);
+    na.nseg = 1;
+    na.vtx2slot = (const uint32_t*)(base + kOffVtx2Slot);
     na.slot2vtx = (const uint32_t*)(base + kOffSlot2Vtx);
     na.vkey0 = (const uint4*)(base + kOffVkey0);
     na.vkeyn = (const uint4*)(base + kOffVkey0);
@@ -219,21 +248,19 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
 
     SliceArgs sl;
     memset(&sl, 0, sizeof(sl));
-    sl.src = src;
-    sl.n = n;
+    sl.segs = dseg;
+    sl.nseg = 1;
+    sl.n_total = n;
     sl.lc = lc;
-    sl.table = tv;
+    sl.key0 = key0;
+    sl.keyn = key0;
+    sl.cap_total = cap;
     sl.slot2vtx = (const uint32_t*)(base + kOffSlot2Vtx);
     sl.rec_slot = (const uint32_t*)(base + kOffRec);
     sl.svals = base + kOffSval;
     sl.vd = vd;
-    sl.out.base = d_out;
-    sl.out.ystride = width;
-    sl.out.tstride = plane;
-    sl.out.cstride = plane;
-    sl.out.channels = channels;
-    sl.out.normalize = 1;
-    sl.status = dstatus;
+    sl.seg_status = dstatus;
+    sl.blocks = (n + kSliceThreads - 1) / kSliceThreads;
     if (!ops->slice(sl, vdp, kPayloadF32, false, st)) return fail(PGPU_ERR_UNSUPPORTED, "slice variant");
     CUDA_TRY(cudaGetLastError());
 

@@ -103,6 +103,18 @@ int pgpu_joint_bilateral(pgpu_image *im, const pgpu_image *ref, float filter_wid
 int pgpu_bilateral(pgpu_image *im, float filter_width, float filter_height,
                    float filter_frames, float color_sigma, const pgpu_options *opt);
 
+/* Many bilateral filters in one set of launches (no counterpart in the reference, which
+ * filters one image per call; each image's result equals Bilateral::apply on it,
+ * src/GaussTransform.cpp:730-734).  ims[i] is filtered in place with its own
+ * filter_width[i] (= filter height) and color_sigma[i]; images may differ in size but
+ * must share the channel count (1..7) and be single frames larger than 1x1 with
+ * 0 < filter width < 10 x their width and height.  Every image keeps its own lattice
+ * (its own hash-table range).  opt->flags & PGPU_FLAG_GRAPH captures the launch sequence
+ * as a CUDA graph and replays it for later batches of the same shape. */
+#define PGPU_FLAG_GRAPH 1
+int pgpu_bilateral_batch(pgpu_image *ims, int count, const float *filter_width,
+                         const float *color_sigma, const pgpu_options *opt);
+
 /* Statistics of the last successful lattice run on this thread. */
 int pgpu_last_stats(pgpu_stats *out);
 

@@ -1,0 +1,94 @@
+"""Batched bilateral filtering: many uneven images per launch, each with its own lattice
+(its own hash-table range) and sigmas; every result must equal the single-image path."""
+import numpy as np
+import pytest
+
+import imagestack_b200 as ib
+from imagestack_b200 import synth
+
+RTOL_FP32 = 1e-5
+
+
+def rel_err(a, b, floor_frac=1e-6):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    floor = max(np.abs(b).max() * floor_frac, 1e-30)
+    return float((np.abs(a - b) / np.maximum(np.abs(b), floor)).max())
+
+
+def uneven_batch(count, seed, lo=64, hi=320, channels=3):
+    specs = synth.batch_specs(count, lo, hi, seed=seed)
+    imgs = [synth.image(w, h, channels, rects=6, seed=s) for (w, h, ss, sr, s) in specs]
+    return imgs, [s[2] for s in specs], [s[3] for s in specs]
+
+
+def test_batch_argument_checks_need_no_gpu():
+    a = np.zeros((3, 20, 20), np.float32)
+    b = np.zeros((1, 20, 20), np.float32)
+    with pytest.raises(ib.PgpuError) as e:     # channel counts differ
+        ib.bilateral_batch([a, b], [4.0, 4.0], [0.1, 0.1])
+    assert e.value.code == ib.ERR_ARGUMENT
+    with pytest.raises(ib.PgpuError) as e:     # sigma too large for a 20 px side
+        ib.bilateral_batch([a], [400.0], [0.1])
+    assert e.value.code == ib.ERR_UNSUPPORTED
+    with pytest.raises(ib.PgpuError):
+        ib.bilateral_batch([a], [4.0, 5.0], [0.1])
+
+
+@pytest.mark.gpu
+def test_batch_matches_single_image_path(gpu):
+    imgs, ss, sr = uneven_batch(24, seed=3)
+    expect = []
+    for im, s, r in zip(imgs, ss, sr):
+        e = im.copy()
+        gpu.Bilateral.apply(e, s, s, 0.0, r)
+        expect.append(e)
+    work = [im.copy() for im in imgs]
+    gpu.bilateral_batch(work, ss, sr)
+    st = gpu.last_stats()
+    assert st["points"] == sum(im.shape[1] * im.shape[2] for im in imgs)
+    for w, e in zip(work, expect):
+        assert rel_err(w, e) <= RTOL_FP32
+
+
+@pytest.mark.gpu
+def test_batch_on_device_with_graph_replay(gpu):
+    import torch
+    imgs, ss, sr = uneven_batch(16, seed=4)
+    expect = [im.copy() for im in imgs]
+    gpu.bilateral_batch(expect, ss, sr)
+    for rep in range(3):   # capture once, replay twice
+        dev = [torch.from_numpy(im.copy()).cuda() for im in imgs]
+        gpu.bilateral_batch(dev, ss, sr, graph=True)
+        torch.cuda.synchronize()
+        for d, e in zip(dev, expect):
+            assert rel_err(d.cpu().numpy(), e) <= RTOL_FP32
+
+
+@pytest.mark.gpu
+def test_batch_fp16_payload_error_vs_fp64(gpu):
+    imgs, ss, sr = uneven_batch(12, seed=5, lo=128, hi=512)
+    ref = [im.copy() for im in imgs]
+    gpu.bilateral_batch(ref, ss, sr, payload="fp64")
+    out = [im.copy() for im in imgs]
+    gpu.bilateral_batch(out, ss, sr, payload="fp16")
+    err = max(rel_err(o, r, floor_frac=1e-2) for o, r in zip(out, ref))
+    print("batched fp16 max relative error vs FP64 lattice:", err)
+    assert err <= 1e-3
+
+
+@pytest.mark.gpu
+def test_batch_retries_only_what_overflows(gpu):
+    """A flat image teaches a small vertex ratio; a noisy one in the same batch then
+    overflows its range and is rerun; both results stay exact."""
+    flat = np.full((3, 96, 96), 0.25, np.float32)
+    gpu.bilateral_batch([flat.copy()], [16.0], [0.5])
+    rng = np.random.default_rng(9)
+    noisy = rng.random((3, 80, 80), dtype=np.float32)
+    work = [flat.copy(), noisy.copy()]
+    gpu.bilateral_batch(work, [16.0, 1.0], [0.5, 0.02])
+    e0, e1 = flat.copy(), noisy.copy()
+    gpu.Bilateral.apply(e0, 16.0, 16.0, 0.0, 0.5)
+    gpu.Bilateral.apply(e1, 1.0, 1.0, 0.0, 0.02)
+    assert rel_err(work[0], e0) <= RTOL_FP32
+    assert rel_err(work[1], e1) <= RTOL_FP32
