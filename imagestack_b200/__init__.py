@@ -251,6 +251,99 @@ def bilateral_batch(images, filter_widths, color_sigmas, payload: str = "fp32",
     return images
 
 
+REQ_BILATERAL, REQ_JOINT_BILATERAL, REQ_GAUSS_TRANSFORM = 0, 1, 2
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("workers", C.c_int), ("max_batch", C.c_int),
+                ("payload", C.c_int), ("load_factor", C.c_float), ("memory_budget", C.c_longlong)]
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_int), ("in_", Image), ("ref", Image), ("out", Image),
+                ("filter_width", C.c_float), ("color_sigma", C.c_float),
+                ("sigmas", C.POINTER(C.c_float)), ("n_sigmas", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_longlong) for k in ("submitted", "completed", "failed", "rejected", "queued",
+                                             "in_flight", "batches", "pixels", "peak_bytes")] + \
+               [(k, C.c_double) for k in ("seconds", "p50_ms", "p99_ms", "mean_ms", "max_ms",
+                                          "mpix_per_s", "req_per_s")]
+
+
+class Server:
+    """Continuous-batching request server (pgpu_server_*): host images in, results written
+    to each request's output array.  Requests of different sizes and kinds are batched as
+    they arrive and run on several device streams at once."""
+
+    def __init__(self, workers: int = 4, max_batch: int = 64, payload: str = "fp32",
+                 memory_budget: int = 40 << 30, device: int = 0, load_factor: float = 0.5):
+        L = lib()
+        L.pgpu_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]
+        L.pgpu_server_submit.argtypes = [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_longlong)]
+        L.pgpu_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_int]
+        L.pgpu_server_drain.argtypes = [C.c_void_p, C.c_int]
+        L.pgpu_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+        L.pgpu_server_reset_stats.argtypes = [C.c_void_p]
+        L.pgpu_server_destroy.argtypes = [C.c_void_p]
+        cfg = ServerConfig(device, workers, max_batch, PAYLOADS[payload], load_factor, memory_budget)
+        h = C.c_void_p()
+        _check(L.pgpu_server_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, kind: int, image, out, ref=None, filter_width: float = 0.0,
+               color_sigma: float = 0.0, sigmas=None) -> int:
+        """Queue a request; the arrays must stay alive until wait() returns for it."""
+        r = Request()
+        r.kind = kind
+        r.in_ = _view(image, "image")[0]
+        r.out = _view(out, "out")[0]
+        if ref is not None:
+            r.ref = _view(ref, "ref")[0]
+        r.filter_width = filter_width
+        r.color_sigma = color_sigma
+        sig = None
+        if sigmas is not None:
+            sig = (C.c_float * len(sigmas))(*[float(s) for s in sigmas])
+            r.sigmas = C.cast(sig, C.POINTER(C.c_float))
+            r.n_sigmas = len(sigmas)
+        t = C.c_longlong()
+        _check(lib().pgpu_server_submit(self._h, C.byref(r), C.byref(t)))
+        self._keep[t.value] = (image, out, ref, sig)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 600000):
+        rc = lib().pgpu_server_wait(self._h, ticket, timeout_ms)
+        if rc != ERR_TIMEOUT:
+            self._keep.pop(ticket, None)
+        _check(rc)
+
+    def drain(self, timeout_ms: int = 600000):
+        _check(lib().pgpu_server_drain(self._h, timeout_ms))
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(lib().pgpu_server_get_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def reset_stats(self):
+        _check(lib().pgpu_server_reset_stats(self._h))
+
+    def close(self):
+        if self._h:
+            lib().pgpu_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 def lattice_dump(pos: np.ndarray, val: np.ndarray, payload: str = "fp32") -> dict:
     """Everything one lattice computes for n interleaved points (pos scaled by 1/sigma):
     keys (M, d) in vertex order, replay vertex index and weight (n, d+1), vertex values

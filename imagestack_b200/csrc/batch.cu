@@ -36,6 +36,25 @@ void Engine::drop_graphs() {
     graphs.clear();
 }
 
+void Engine::shutdown() {
+    if (device >= 0) cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    drop_graphs();
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    if (hstat) cudaFreeHost(hstat);
+    hstat = nullptr;
+    if (hmeta) cudaFreeHost(hmeta);
+    hmeta = nullptr;
+    hmeta_bytes = 0;
+    for (DevBuf* b : {&key0, &keyn, &tvals, &ft, &slot2vtx, &bitmap, &offs, &partials, &vkey0, &vkeyn,
+                      &vv0, &vv1, &nbr, &vf32, &vtx2slot, &sval, &rec, &dstat, &meta, &img_a, &img_b,
+                      &img_c, &img_d})
+        b->release();
+}
+
 namespace {
 
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }

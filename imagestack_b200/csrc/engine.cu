@@ -195,8 +195,8 @@ pgpu_image dense_like(const pgpu_image& v, float* base, int channels) {
     return d;
 }
 
-static int copy_view(const pgpu_image& src, const pgpu_image& dst, int channels, cudaMemcpyKind kind,
-                     cudaStream_t st) {
+int copy_view(const pgpu_image& src, const pgpu_image& dst, int channels, cudaMemcpyKind kind,
+              cudaStream_t st) {
     if (is_dense(src) && is_dense(dst)) {
         CUDA_TRY(cudaMemcpyAsync(dst.base, src.base,
                                  sizeof(float) * (size_t)src.width * src.height * src.frames * channels,

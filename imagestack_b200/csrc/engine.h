@@ -70,7 +70,18 @@ struct Engine {
     int init(int dev);
     int ensure_hmeta(size_t bytes);
     void drop_graphs();
+    void shutdown();   // release stream, events, pinned buffers and graphs
 };
+
+// image views and their staging (engine.cu)
+bool view_ok(const pgpu_image* v);
+bool same_view(const pgpu_image& a, const pgpu_image& b);
+bool is_dense(const pgpu_image& v);
+pgpu_image dense_like(const pgpu_image& v, float* base, int channels);
+int copy_view(const pgpu_image& src, const pgpu_image& dst, int channels, cudaMemcpyKind kind,
+              cudaStream_t st);
+PlanarView planar(const pgpu_image& v);
+OutView outview(const pgpu_image& v, int channels, int normalize);
 
 int get_engine(int dev, Engine** out);
 int device_count_sm100();

@@ -115,6 +115,58 @@ int pgpu_bilateral(pgpu_image *im, float filter_width, float filter_height,
 int pgpu_bilateral_batch(pgpu_image *ims, int count, const float *filter_width,
                          const float *color_sigma, const pgpu_options *opt);
 
+/* ---- Request server (no counterpart in the reference, which runs one operation at a
+ * time on the CPU).  A pool of worker threads, each with its own CUDA stream and lattice
+ * workspace, takes queued requests in batches: compatible requests (same position
+ * dimensions, value channels and kind) that fit the memory budget go into one batched
+ * launch sequence; requests arriving while batches run are admitted as workers and
+ * memory free up, and batches on different workers overlap on the device.  Images are
+ * in host memory; each result goes to the request's `out`. ---- */
+#define PGPU_REQ_BILATERAL 0        /* in: image; filtered into out (may be in) */
+#define PGPU_REQ_JOINT_BILATERAL 1  /* in: image, ref: edge image; result into out */
+#define PGPU_REQ_GAUSS_TRANSFORM 2  /* in: values, ref: positions, sigmas; un-normalised out */
+
+typedef struct pgpu_server_config {
+    int device;
+    int workers;                 /* worker threads (streams); 0: 4 */
+    int max_batch;               /* requests per batch; 0: 64 */
+    int payload;                 /* PGPU_PAYLOAD_* of every lattice */
+    float load_factor;           /* hash-table load; 0: 0.5 */
+    long long memory_budget;     /* device bytes for images and lattices in flight; 0: 40 GiB */
+} pgpu_server_config;
+
+typedef struct pgpu_request {
+    int kind;                    /* PGPU_REQ_* */
+    pgpu_image in, ref, out;     /* host memory, single frames */
+    float filter_width;          /* bilateral kinds: spatial sigma (width = height) */
+    float color_sigma;
+    const float *sigmas;         /* Gauss transform: one sigma per position channel */
+    int n_sigmas;
+} pgpu_request;
+
+typedef struct pgpu_server_stats {
+    long long submitted, completed, failed, rejected, queued, in_flight, batches;
+    long long pixels;            /* points of completed requests */
+    long long peak_bytes;        /* largest admitted footprint in flight */
+    double seconds;              /* since the first submission */
+    double p50_ms, p99_ms, mean_ms, max_ms;   /* submit -> done latency */
+    double mpix_per_s, req_per_s;
+} pgpu_server_stats;
+
+int pgpu_server_create(const pgpu_server_config *cfg, void **server);
+/* Queue a request (its images must stay valid until it completes); *ticket identifies it.
+ * A request whose footprint alone exceeds the budget is refused with PGPU_ERR_ADMISSION. */
+int pgpu_server_submit(void *server, const pgpu_request *req, long long *ticket);
+/* Wait up to timeout_ms for a request; returns its status, or PGPU_ERR_TIMEOUT. */
+int pgpu_server_wait(void *server, long long ticket, int timeout_ms);
+/* Wait up to timeout_ms until nothing is queued or running. */
+int pgpu_server_drain(void *server, int timeout_ms);
+int pgpu_server_get_stats(void *server, pgpu_server_stats *out);
+/* Forget the latency record (start a new measurement window). */
+int pgpu_server_reset_stats(void *server);
+/* Stop the workers (after finishing what runs) and free everything. */
+void pgpu_server_destroy(void *server);
+
 /* Statistics of the last successful lattice run on this thread. */
 int pgpu_last_stats(pgpu_stats *out);
 
