@@ -1,10 +1,15 @@
-"""Benchmark: bilateral filtering throughput of the B200 permutohedral lattice.
+"""Benchmark: bilateral filtering throughput and latency of the B200 permutohedral lattice.
 
-Workload (one "step"): the 3840x2160 RGB bilateral, d=5 positions (r/0.1, g/0.1, b/0.1,
-x/16, y/16), values RGB + homogeneous 1, on a seeded synthetic frame (gradients, 64
-rectangles, Gaussian noise sigma 0.05).  `value` is Mpix/s of the whole job with the frame
-already resident in HBM; `e2e` is the same metric through the C ABI with pinned host
-buffers, host->device and device->host copies inside the timed region.
+Headline workload (one "step"): a batch of four 3840x2160 RGB frames through the batched
+lattice with FP16 payload (FP32 accumulation), d=5 positions (r/0.1, g/0.1, b/0.1, x/16,
+y/16), values RGB + homogeneous 1, on seeded synthetic frames (gradients, 64 rectangles,
+Gaussian noise sigma 0.05).  `value` is Mpix/s with the frames already resident in HBM;
+`e2e` is the same step through the C ABI with pinned host frames, host->device and
+device->host copies inside the timed region.  Beside it, the same line reports the plain
+GPU lattice (one FP32 frame per call), the mixed-size batch (256 images, sides
+log-uniform 128..1024, per-image sigmas), a served request stream (Poisson arrivals
+ramped 50 -> 2000 req/s, bilateral RGB and grey joint-bilateral requests, sides 64..2048)
+with p50/p99 latency, and the FP16 error against the FP64 lattice.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -19,16 +24,24 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 W, H, SIGMA_S, SIGMA_R, RECTS, SEED = 3840, 2160, 16.0, 0.1, 64, 2
+FRAMES_PER_STEP = 4
 METRIC = "bilateral Mpix/s (d=5 4K, batched) vs plain GPU; p50/p99 latency @ err<=1e-3"
-WORKLOAD = "bilateral RGB 3840x2160, d=5 (sigma_s 16, sigma_r 0.1)"
+WORKLOAD = ("bilateral RGB 3840x2160 x%d frames per batch, d=5 (sigma_s 16, sigma_r 0.1), "
+            "FP16 payload / FP32 accumulation" % FRAMES_PER_STEP)
 L2_BYTES = 126 * 1024 * 1024
-KERNELS_PER_LATTICE = 8   # splat, mark, 3 scan phases, assign, neighbours, slice (+ d+1 blurs)
+KERNELS_PER_LATTICE = 9   # splat, mark, 3 scan phases, counts, assign, neighbours, slice
+D = 5
+
+
+def blur_launches(d):
+    return (d + 2) // 2   # axes are blurred in fused pairs
 
 
 def peaks():
@@ -57,53 +70,48 @@ def ncu_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """SM clock and throttle reasons sampled through NVML while the timed region runs."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+             "sw_power_cap": 0x4}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for n, bit in self.NAMES.items():
+                    if r & bit:
+                        self.reasons.add(n)
+                time.sleep(0.005)
+        except Exception:
+            pass
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "50"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except Exception:
-            self.proc = None
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
         return self
 
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-                self.lines = [l for l in out.splitlines() if l.strip()]
-            except Exception:
-                self.proc.kill()
+        self._stop.set()
+        self._t.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
-            p = [x.strip() for x in l.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, p[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
 
 
 def dist_init():
@@ -111,6 +119,14 @@ def dist_init():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def rel_err(a, b, floor_frac=1e-2):
+    import numpy as np
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    floor = max(np.abs(b).max() * floor_frac, 1e-30)
+    return float((np.abs(a - b) / np.maximum(np.abs(b), floor)).max())
 
 
 # --------------------------------------------------------------------------------------
@@ -141,7 +157,7 @@ def _cpu_worker(args):
 
 
 def cpu_baseline_single():
-    """Reference Bilateral::apply on the full frame, one thread, in a fresh process."""
+    """Reference Bilateral::apply on one full frame, one thread, in a fresh process."""
     code = ("import sys,json; sys.path.insert(0,%r); import bench; "
             "print(json.dumps(bench._cpu_worker((%d,%d,%d))))" % (ROOT, W, H, SEED))
     env = dict(os.environ, OMP_NUM_THREADS="1")
@@ -197,7 +213,142 @@ def run_reference_arm(args):
 # our arm
 # --------------------------------------------------------------------------------------
 
+def timed_steps(stream, steps, fn, prepare):
+    """Per-step CUDA events on `stream`, `prepare` (restore inputs, flush L2) outside."""
+    import torch
+    events, stats = [], []
+    for _ in range(steps):
+        prepare()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        events.append((e0, e1))
+        stats.append(fn.stats() if hasattr(fn, "stats") else None)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in events), stats
+
+
+def mixed_batch(ib, synth, torch, dev, steps):
+    """256 uneven RGB images, per-image sigmas, one batched launch
+    sequence (FP16 payload, CUDA graph) against the plain per-image FP32 path."""
+    specs = synth.batch_specs(256, 128, 1024, seed=SEED)
+    imgs = [torch.from_numpy(synth.image(w, h, 3, rects=16, seed=s)).to(dev)
+            for (w, h, ss, sr, s) in specs]
+    ss = [s[2] for s in specs]
+    sr = [s[3] for s in specs]
+    px = sum(im.shape[1] * im.shape[2] for im in imgs)
+    work = [torch.empty_like(im) for im in imgs]
+    stream = torch.cuda.current_stream(dev)
+
+    def restore():
+        for wk, im in zip(work, imgs):
+            wk.copy_(im)
+
+    def batched():
+        ib.bilateral_batch(work, ss, sr, payload="fp16", graph=True)
+
+    def plain():
+        for wk, s, r in zip(work, ss, sr):
+            ib.Bilateral.apply(wk, s, s, 0.0, r)
+
+    for _ in range(2):
+        restore()
+        batched()
+        restore()
+        plain()
+    torch.cuda.synchronize()
+    tb, _ = timed_steps(stream, steps, batched, restore)
+    tp, _ = timed_steps(stream, max(1, steps // 2), plain, restore)
+    # error of the batched FP16 results against the FP64 lattice on a sample of images
+    restore()
+    batched()
+    torch.cuda.synchronize()
+    err = 0.0
+    for k in range(0, 256, 32):
+        ref = imgs[k].clone()
+        ib.Bilateral.apply(ref, ss[k], ss[k], 0.0, sr[k], payload="fp64")
+        torch.cuda.synchronize()
+        err = max(err, rel_err(work[k].cpu().numpy(), ref.cpu().numpy()))
+    return {"images": 256, "pixels": px,
+            "batched_fp16_graph_mpix_s": round(px * steps / (tb / 1e3) / 1e6, 2),
+            "plain_fp32_per_image_mpix_s": round(px * max(1, steps // 2) / (tp / 1e3) / 1e6, 2),
+            "max_rel_err_fp16_vs_fp64": err}
+
+
+def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0):
+    """BASELINE config 5: Poisson arrivals ramped rate0 -> rate1 req/s over `seconds`;
+    half bilateral RGB (d=5), half joint bilateral of a grey image on a grey guide (d=3);
+    sides log-uniform 64..2048, sigmas as the mixed batch; FP16 payload, 40 GB budget.
+    Requests reuse a pool of pinned host images; each has its own pinned output."""
+    import numpy as np
+    rng = np.random.default_rng(SEED)
+    P = 24
+    sides = synth.log_uniform_int(SEED, 31, 2 * P, 64, 2048)
+    pool = []
+    for k in range(P):
+        w, h = int(sides[2 * k]), int(sides[2 * k + 1])
+        rgb = synth.image(w, h, 3, rects=8, seed=700 + k)
+        kind = k % 2
+        if kind == 0:
+            img = torch.from_numpy(rgb).pin_memory()
+            ref = None
+        else:
+            img = torch.from_numpy(synth.luminance(rgb)).pin_memory()
+            ref = torch.from_numpy(synth.luminance(synth.image(w, h, 3, rects=8, seed=900 + k))).pin_memory()
+        outs = [torch.empty_like(img).pin_memory() for _ in range(4)]
+        pool.append(dict(kind=ib.REQ_BILATERAL if kind == 0 else ib.REQ_JOINT_BILATERAL,
+                         img=img, ref=ref, outs=outs, busy=[None] * 4,
+                         ss=float(4 + 28 * rng.random()), sr=float(0.05 + 0.25 * rng.random())))
+    srv = ib.Server(workers=4, max_batch=32, payload="fp16", memory_budget=40 << 30)
+    # warm each worker's workspace on the pool
+    tickets = []
+    for q in pool:
+        t = srv.submit(q["kind"], q["img"].numpy(), q["outs"][0].numpy(),
+                       ref=None if q["ref"] is None else q["ref"].numpy(),
+                       filter_width=q["ss"], color_sigma=q["sr"])
+        tickets.append(t)
+    for t in tickets:
+        srv.wait(t)
+    srv.reset_stats()
+    pending = []
+    lock = threading.Lock()
+    t_start = time.perf_counter()
+    t = 0.0
+    j = 0
+    while t < seconds:
+        rate = rate0 + (rate1 - rate0) * t / seconds
+        t += rng.exponential(1.0 / rate)
+        delay = t_start + t - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        q = pool[j % P]
+        slot = (j // P) % 4
+        if q["busy"][slot] is not None:      # the output slot is still owned by an older request
+            srv.wait(q["busy"][slot])
+        tk = srv.submit(q["kind"], q["img"].numpy(), q["outs"][slot].numpy(),
+                        ref=None if q["ref"] is None else q["ref"].numpy(),
+                        filter_width=q["ss"], color_sigma=q["sr"])
+        q["busy"][slot] = tk
+        pending.append(tk)
+        j += 1
+    for q in pool:
+        for s, tk in enumerate(q["busy"]):
+            if tk is not None:
+                srv.wait(tk)
+    st = srv.stats()
+    srv.close()
+    return {"requests": int(st["completed"]), "failed": int(st["failed"]),
+            "window_s": round(seconds, 2), "rate_req_s": [rate0, rate1],
+            "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+            "max_ms": round(st["max_ms"], 3), "throughput_mpix_s": round(st["mpix_per_s"], 2),
+            "throughput_req_s": round(st["req_per_s"], 1), "batches": int(st["batches"]),
+            "payload": "fp16", "workers": 4, "memory_budget_gib": 40}
+
+
 def run_ours(args):
+    import numpy as np
     import torch
 
     import imagestack_b200 as ib
@@ -213,52 +364,59 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    img = synth.image(W, H, 3, rects=RECTS, seed=SEED + rank)
-    pristine = torch.from_numpy(img).to(dev)
-    work = torch.empty_like(pristine)
+    frames = [synth.image(W, H, 3, rects=RECTS, seed=SEED + 17 * rank + k)
+              for k in range(FRAMES_PER_STEP)]
+    pristine = [torch.from_numpy(f).to(dev) for f in frames]
+    work = [torch.empty_like(p) for p in pristine]
     flush = torch.empty(4 * L2_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    payload = args.payload
+    ss = [SIGMA_S] * FRAMES_PER_STEP
+    sr = [SIGMA_R] * FRAMES_PER_STEP
 
-    def step():
-        work.copy_(pristine)   # the filter is in place: restore the frame
-        flush.fill_(1.0)       # evict L2 between steps; both outside the timed window
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        ib.Bilateral.apply(work, SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload=payload)
-        ev1.record(stream)
-        return ev0, ev1
+    def prepare():
+        for wk, p in zip(work, pristine):
+            wk.copy_(p)      # the filter is in place: restore the frames
+        flush.fill_(1.0)     # evict L2 between steps; both outside the timed window
+
+    def headline():
+        ib.bilateral_batch(work, ss, sr, payload=args.payload)
+    headline.stats = ib.last_stats
+
+    def plain():
+        ib.Bilateral.apply(work[0], SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload="fp32")
+    plain.stats = ib.last_stats
 
     for _ in range(args.warmup):
-        step()
+        prepare()
+        headline()
+        prepare()
+        plain()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    events, stage = [], []
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            events.append(step())
-            stage.append(ib.last_stats())
-        torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in events]
-    total_ms = sum(step_ms)
+        total_ms, stage = timed_steps(stream, args.steps, headline, prepare)
+    plain_ms, plain_stage = timed_steps(stream, args.steps, plain, prepare)
     if dist:
         t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
-    value = world * W * H * args.steps / (total_ms / 1e3) / 1e6
+    px_step = W * H * FRAMES_PER_STEP
+    value = world * px_step * args.steps / (total_ms / 1e3) / 1e6
+    plain_mpix = W * H * args.steps / (plain_ms / 1e3) / 1e6
 
-    # end to end through the C ABI: pinned host frame in, filtered frame back out
-    host = torch.from_numpy(img.copy()).pin_memory()
-    host_np = host.numpy()
+    # end to end through the C ABI: pinned host frames in, filtered frames back out
+    host = [torch.from_numpy(f.copy()).pin_memory() for f in frames]
+    host_np = [h.numpy() for h in host]
+    e2e_steps = min(args.steps, 10)
     e2e_times = []
-    for i in range(args.warmup + args.steps):
-        host_np[...] = img
+    for i in range(args.warmup + e2e_steps):
+        for hn, f in zip(host_np, frames):
+            hn[...] = f
         t0 = time.perf_counter()
-        ib.Bilateral.apply(host_np, SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload=payload)
+        ib.bilateral_batch(host_np, ss, sr, payload=args.payload)
         el = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(el)
@@ -267,45 +425,64 @@ def run_ours(args):
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = world * W * H * args.steps / e2e_s / 1e6
+    e2e = world * px_step * e2e_steps / e2e_s / 1e6
 
     if rank == 0:
         hbm, peak_kind = peaks()
-        st = stage[-1]
-        M = st["vertices"]
         n = W * H
-        d, vd = 5, 4
+        M = stage[-1]["vertices"]
         splat_ms = statistics.mean(s["ms_splat"] for s in stage)
         stages = {k: round(statistics.mean(s[k] for s in stage), 4)
                   for k in ("ms_splat", "ms_compact", "ms_neighbours", "ms_blur", "ms_slice",
                             "ms_total")}
-        # algorithmic bytes of one splat launch: the RGB frame read once (positions and
+        plain_stages = {k: round(statistics.mean(s[k] for s in plain_stage), 4)
+                        for k in ("ms_splat", "ms_compact", "ms_neighbours", "ms_blur",
+                                  "ms_slice", "ms_total")}
+        # algorithmic bytes of one splat launch: every frame's RGB read once (positions and
         # values come from the same channels) + one key and one FP32 accumulator row per
         # vertex
-        splat_bytes = n * 3 * 4 + M * (2 * d + vd * 4)
+        vd = 4
+        splat_bytes = FRAMES_PER_STEP * n * 3 * 4 + M * (2 * D + vd * 4)
         achieved = splat_bytes / (splat_ms / 1e3) / 1e9
         traffic = ncu_traffic().get("splat_dram_bytes")
+        # FP16 error on the 4K frame against the FP64 lattice
+        a = pristine[0].clone()
+        ib.Bilateral.apply(a, SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload=args.payload)
+        b = pristine[0].clone()
+        ib.Bilateral.apply(b, SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload="fp64")
+        torch.cuda.synchronize()
+        err4k = rel_err(a.cpu().numpy(), b.cpu().numpy())
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"fp32": "f32", "fp16": "f16-payload/f32-accum",
-                      "bf16": "bf16-payload/f32-accum", "fp64": "f64"}[payload],
+                      "bf16": "bf16-payload/f32-accum", "fp64": "f64"}[args.payload],
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "frame": [W, H], "seed": SEED,
-                       "payload": payload, "path": "plain (one frame per call)",
+            "config": {"workload": WORKLOAD, "frame": [W, H], "frames_per_step": FRAMES_PER_STEP,
+                       "seed": SEED, "payload": args.payload, "path": "batched",
                        "l2": "flushed between steps (512 MiB write), outside the timed window",
                        "parallelism": "replicas x%d" % world},
+            "plain_gpu": {"mpix_s": round(plain_mpix, 2), "payload": "fp32",
+                          "path": "one frame per call", "stages_ms": plain_stages},
+            "max_rel_err_vs_fp64": {"4k_frame": err4k, "tolerance": 1e-3,
+                                    "denominator": "max(|fp64|, 1e-2 x max|fp64|)"},
             "roofline": {"kernel": "splat", "bound": "hbm", "achieved": round(achieved, 2),
                          "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4),
-                         "traffic": traffic, "algorithmic_bytes": splat_bytes},
+                         "frac": round(achieved / hbm, 4), "traffic": traffic,
+                         "algorithmic_bytes": splat_bytes,
+                         "note": "latency bound on L2 probes and atomics; see profiles/"},
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s",
-                    "h2d_bytes_per_step": n * 3 * 4, "d2h_bytes_per_step": n * 3 * 4},
-            "gpu_launches": args.steps * (KERNELS_PER_LATTICE + d + 1),
-            "stages_ms": stages, "vertices": M, "capacity": st["capacity"],
+                    "h2d_bytes_per_step": px_step * 3 * 4, "d2h_bytes_per_step": px_step * 3 * 4},
+            "gpu_launches": args.steps * (KERNELS_PER_LATTICE + blur_launches(D)),
+            "stages_ms": stages, "vertices": M, "capacity": stage[-1]["capacity"],
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.quick:
+            line["mixed_batch"] = mixed_batch(ib, synth, torch, dev, steps=6)
+            line["served"] = served_stream(ib, synth, torch)
+            line["p50_ms"] = line["served"]["p50_ms"]
+            line["p99_ms"] = line["served"]["p99_ms"]
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline_single()
@@ -320,11 +497,12 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--payload", default="fp32", choices=["fp32", "fp16", "bf16", "fp64"])
+    ap.add_argument("--payload", default="fp16", choices=["fp32", "fp16", "bf16", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="headline and plain path only")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

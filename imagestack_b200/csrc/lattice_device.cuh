@@ -233,9 +233,17 @@ struct Simplex {
     float bary[D + 1]; // barycentric weight of remainder r
 };
 
+// Per-thread shared-memory column for compute_simplex: element k at col[k * stride].
+struct SimplexScratch {
+    float* delta;            // d+1 floats: delta of the coordinate of rank k
+    unsigned char* coord;    // d+1 bytes: the coordinate of rank k
+    int stride;
+};
+
 template <int D>
 __device__ __forceinline__ void compute_simplex(const float (&p)[D], const LatticeConsts& lc,
-                                                Simplex<D>& sx, unsigned* range_flag) {
+                                                Simplex<D>& sx, unsigned* range_flag,
+                                                const SimplexScratch& scr) {
     float e[D + 1];
     // elevated[d] = -d*position[d-1]*scaleFactor[d-1]
     e[D] = __fmul_rn(__fmul_rn((float)(-D), p[D - 1]), lc.sf[D - 1]);
@@ -304,29 +312,64 @@ __device__ __forceinline__ void compute_simplex(const float (&p)[D], const Latti
     }
 
     // Barycentric weights (src/Permutohedral.h:351-356).  b[k] receives +delta of the
-    // coordinate ranked d-k and -delta of the one ranked d+1-k; in IEEE arithmetic
-    // both accumulation orders give delta_plus - delta_minus, so the weights are
-    // formed by selection (no dynamically indexed arrays) and stay bit-exact.
-    float delta[D + 1];
-#pragma unroll
-    for (int i = 0; i <= D; ++i) delta[i] = __fmul_rn(__fsub_rn(e[i], (float)sx.g[i]), scale);
-    float top = 0.0f, bottom = 0.0f;   // coordinates ranked d and 0
+    // coordinate ranked d-k and -delta of the one ranked d+1-k; in IEEE arithmetic both
+    // accumulation orders give delta_plus - delta_minus.  The ranks are a permutation of
+    // 0..d, so the deltas are scattered by rank into this thread's shared-memory column
+    // and read back in rank order (with the coordinate of each rank, for the key walk).
+    // Ranks outside [0, d] only arise with keys outside int16, which is flagged above.
 #pragma unroll
     for (int i = 0; i <= D; ++i) {
-        if (sx.rank[i] == D) top = delta[i];
-        if (sx.rank[i] == 0) bottom = delta[i];
-    }
-    // b[0] = delta(rank d) + (1 + b[d+1]),  b[d+1] = -delta(rank 0)
-    sx.bary[0] = __fadd_rn(top, __fadd_rn(1.0f, -bottom));
-#pragma unroll
-    for (int k = 1; k <= D; ++k) {
-        float plus = 0.0f, minus = 0.0f;
-#pragma unroll
-        for (int i = 0; i <= D; ++i) {
-            if (sx.rank[i] == D - k) plus = delta[i];
-            if (sx.rank[i] == D + 1 - k) minus = delta[i];
+        const float delta = __fmul_rn(__fsub_rn(e[i], (float)sx.g[i]), scale);
+        if ((unsigned)sx.rank[i] <= (unsigned)D) {
+            scr.delta[sx.rank[i] * scr.stride] = delta;
+            scr.coord[sx.rank[i] * scr.stride] = (unsigned char)i;
         }
-        sx.bary[k] = __fsub_rn(plus, minus);
+    }
+    float srt[D + 1];
+#pragma unroll
+    for (int k = 0; k <= D; ++k) srt[k] = scr.delta[k * scr.stride];
+    // b[0] = delta(rank d) + (1 + b[d+1]),  b[d+1] = -delta(rank 0)
+    sx.bary[0] = __fadd_rn(srt[D], __fadd_rn(1.0f, -srt[0]));
+#pragma unroll
+    for (int k = 1; k <= D; ++k) sx.bary[k] = __fsub_rn(srt[D - k], srt[D + 1 - k]);
+}
+
+// Key of remainder 0: the greedy point itself (canonical[0][j] = 0 for every j).
+template <int D>
+__device__ __forceinline__ void first_key(const Simplex<D>& sx, Key<key_words(D)>& k) {
+    int kc[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) kc[i] = sx.g[i];
+    pack_key<D>(kc, k);
+}
+
+// Key of remainder r+1 from that of r: with canonical[r][j] = r for j <= d-r, else r-(d+1)
+// (src/Permutohedral.h:247-254), every stored coordinate grows by one except the one
+// ranked d-r, which drops by d.  Stored lanes are int16 + 0x8000 mod 2^16, so the step is
+// a per-lane 16-bit add (__vadd2) that wraps exactly like the reference's short keys.
+// `coord` is the coordinate ranked d-r (d: the implied coordinate, no stored lane).
+template <int D>
+__device__ __forceinline__ void key_step(Key<key_words(D)>& k, int coord) {
+    constexpr int KW = key_words(D);
+#pragma unroll
+    for (int w = 0; w < KW; ++w) {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            uint32_t inc = 0;
+            bool any = false;   // known at compile time once the loops are unrolled
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const int lane = 2 * h + half;
+                const int c = w == 0 ? lane : 7 + (w - 1) * 8 + lane;   // coordinate in this lane
+                const bool stored = (w == 0 ? lane < 7 : true) && c < D;
+                if (stored) {
+                    const uint32_t step = coord == c ? (uint32_t)(uint16_t)(-D) : 1u;
+                    inc |= step << (16 * half);
+                    any = true;
+                }
+            }
+            if (any) word_u32(k.w[w], h) = __vadd2(word_u32(k.w[w], h), inc);
+        }
     }
 }
 

@@ -288,7 +288,13 @@ __host__ __device__ constexpr int splat_min_blocks(int d) { return d <= 6 ? 4 : 
 template <int D, int VDP, typename Acc>
 __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kernel(SplatArgs a) {
     constexpr int KW = key_words(D);
+    // the keys of every remainder stay in shared memory for the leaders' inserts when
+    // they fit beside the staging rows (one-word keys, rows of at most 16 bytes)
+    constexpr bool kKeysInSmem = KW == 1 && sizeof(Acc) * VDP <= 16;
     __shared__ Acc stage[kSplatThreads / 32][32][VDP];
+    __shared__ float s_delta[(D + 1) * kSplatThreads];
+    __shared__ unsigned char s_coord[(D + 1) * kSplatThreads];
+    __shared__ uint4 s_key[kKeysInSmem ? (D + 1) * kSplatThreads : 1];
     __shared__ Segment sg;
     const int kseg = segment_of_block(a.segs, a.nseg, blockIdx.x);
     load_segment(a.segs + kseg, sg);
@@ -303,7 +309,8 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
     float p[D], v[VDP];
     load_point<D, VDP>(sg.src, i, p, v);
     Simplex<D> sx;
-    compute_simplex<D>(p, a.lc, sx, status);
+    const SimplexScratch scr{s_delta + threadIdx.x, s_coord + threadIdx.x, kSplatThreads};
+    compute_simplex<D>(p, a.lc, sx, status, scr);
     const uint32_t gi = sg.point_base + i;   // point number in the batch
     const uint32_t e0 = gi * (uint32_t)(D + 1);
     Acc* vals = reinterpret_cast<Acc*>(a.vals) + (size_t)sg.slot_base * VDP;
@@ -316,12 +323,12 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
     unsigned peers[D + 1];
     uint32_t home[D + 1];
     uint4 first[D + 1];
+    Key<KW> key;
+    first_key<D>(sx, key);
 #pragma unroll
     for (int r = 0; r <= D; ++r) {
-        int kc[D];
-        vertex_coords<D>(sx, r, kc);
-        Key<KW> key;
-        pack_key<D>(kc, key);
+        if (r > 0) key_step<D>(key, scr.coord[(D - (r - 1)) * scr.stride]);
+        if (kKeysInSmem) s_key[r * kSplatThreads + threadIdx.x] = key.w[0];
         unsigned pr = active;
 #pragma unroll
         for (int w = 0; w < KW; ++w) {
@@ -378,12 +385,16 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
         }
         int s = -1;
         if (lane == leader) {
-            int kc[D];
-            vertex_coords<D>(sx, r, kc);
-            Key<KW> key;
-            pack_key<D>(kc, key);
+            Key<KW> kr;
+            if constexpr (kKeysInSmem) {
+                kr.w[0] = s_key[r * kSplatThreads + threadIdx.x];
+            } else {
+                int kc[D];
+                vertex_coords<D>(sx, r, kc);
+                pack_key<D>(kc, kr);
+            }
             const uint4 w0 = kAhead ? first[r] : __ldcg(&table.key0[home[r]]);
-            s = table_insert<KW>(table, key, home[r], w0, status);
+            s = table_insert<KW>(table, kr, home[r], w0, status);
             if (s >= 0) {
                 atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
                 atomicMin(&ft[s], e0 + (uint32_t)r);   // the leader's entry is the group's smallest
@@ -608,6 +619,8 @@ constexpr int kSliceThreads = 256;
 template <int D, int VDP, typename A, bool HOMOG>
 __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
     constexpr int KW = key_words(D);
+    __shared__ float s_delta[(D + 1) * kSliceThreads];
+    __shared__ unsigned char s_coord[(D + 1) * kSliceThreads];
     __shared__ Segment sg;
     const int kseg = segment_of_block(a.segs, a.nseg, blockIdx.x);
     load_segment(a.segs + kseg, sg);
@@ -621,21 +634,21 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
     float p[D];
     load_position<D>(sg.src, i, p);
     Simplex<D> sx;
-    compute_simplex<D>(p, a.lc, sx, status);
+    const SimplexScratch scr{s_delta + threadIdx.x, s_coord + threadIdx.x, kSliceThreads};
+    compute_simplex<D>(p, a.lc, sx, status, scr);
     const A* sv = reinterpret_cast<const A*>(a.svals);
     A acc[VDP];
 #pragma unroll
     for (int k = 0; k < VDP; ++k) acc[k] = (A)0;
+    Key<KW> key;
+    if (!a.rec_slot) first_key<D>(sx, key);
 #pragma unroll
     for (int r = 0; r <= D; ++r) {
         int s;   // slot in the shared array
         if (a.rec_slot) {
             s = (int)__ldg(a.rec_slot + (size_t)r * a.n_total + gi);
         } else {
-            int kc[D];
-            vertex_coords<D>(sx, r, kc);
-            Key<KW> key;
-            pack_key<D>(kc, key);
+            if (r > 0) key_step<D>(key, scr.coord[(D - (r - 1)) * scr.stride]);
             const TableView table{a.key0 + sg.slot_base, a.keyn + sg.slot_base, sg.cap, a.cap_total};
             const int ls = table_find<KW>(table, key, key_hash<KW>(key));
             s = ls >= 0 ? (int)sg.slot_base + ls : -1;
