@@ -288,17 +288,15 @@ __host__ __device__ constexpr int splat_min_blocks(int d) { return d <= 6 ? 4 : 
 template <int D, int VDP, typename Acc>
 __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kernel(SplatArgs a) {
     constexpr int KW = key_words(D);
-    // the keys of every remainder stay in shared memory for the leaders' inserts when
-    // they fit beside the staging rows (one-word keys, rows of at most 16 bytes)
-    constexpr bool kKeysInSmem = KW == 1 && sizeof(Acc) * VDP <= 16;
-    __shared__ Acc stage[kSplatThreads / 32][32][VDP];
+    // one-word keys of every remainder stay in shared memory for the leaders' inserts
+    constexpr bool kKeysInSmem = KW == 1;
     __shared__ float s_delta[(D + 1) * kSplatThreads];
     __shared__ unsigned char s_coord[(D + 1) * kSplatThreads];
     __shared__ uint4 s_key[kKeysInSmem ? (D + 1) * kSplatThreads : 1];
     __shared__ Segment sg;
     const int kseg = segment_of_block(a.segs, a.nseg, blockIdx.x);
     load_segment(a.segs + kseg, sg);
-    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned lane = threadIdx.x & 31u;
     const uint32_t i = (blockIdx.x - sg.block_base) * (uint32_t)kSplatThreads + threadIdx.x;
     const bool valid = i < sg.n;
     const unsigned active = __ballot_sync(0xFFFFFFFFu, valid);
@@ -316,8 +314,9 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
     Acc* vals = reinterpret_cast<Acc*>(a.vals) + (size_t)sg.slot_base * VDP;
     uint32_t* ft = a.ft + sg.slot_base;
 
-    // Phase 1: group the lanes that share each vertex key (exact match on all key words);
-    // each group's leader starts loading its home slot.  For d <= 8 the loads of all d+1
+    // Phase 1: group the lanes that share each vertex key: lanes with equal hashes,
+    // confirmed against the group leader's key (a hash collision inside the warp falls
+    // back to matching all key words); each group's leader starts loading its home slot.  For d <= 8 the loads of all d+1
     // remainders are in flight together before any is needed.
     constexpr bool kAhead = D <= PGPU_SPLAT_AHEAD_MAX_D;
     unsigned peers[D + 1];
@@ -329,21 +328,40 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
     for (int r = 0; r <= D; ++r) {
         if (r > 0) key_step<D>(key, scr.coord[(D - (r - 1)) * scr.stride]);
         if (kKeysInSmem) s_key[r * kSplatThreads + threadIdx.x] = key.w[0];
-        unsigned pr = active;
+        const uint32_t hk = key_hash<KW>(key);
+        unsigned pr = __match_any_sync(active, hk);
+        {
+            const unsigned ld = __ffs(pr) - 1;
+            bool same = true;
 #pragma unroll
-        for (int w = 0; w < KW; ++w) {
-            pr &= __match_any_sync(active, ((unsigned long long)key.w[w].y << 32) | key.w[w].x);
-            pr &= __match_any_sync(active, ((unsigned long long)key.w[w].w << 32) | key.w[w].z);
+            for (int w = 0; w < KW; ++w) {
+                same &= __shfl_sync(active, key.w[w].x, ld) == key.w[w].x;
+                same &= __shfl_sync(active, key.w[w].y, ld) == key.w[w].y;
+                same &= __shfl_sync(active, key.w[w].z, ld) == key.w[w].z;
+                same &= __shfl_sync(active, key.w[w].w, ld) == key.w[w].w;
+            }
+            if (!__all_sync(active, same)) {
+                pr = active;
+#pragma unroll
+                for (int w = 0; w < KW; ++w) {
+                    pr &= __match_any_sync(active, ((unsigned long long)key.w[w].y << 32) | key.w[w].x);
+                    pr &= __match_any_sync(active, ((unsigned long long)key.w[w].w << 32) | key.w[w].z);
+                }
+            }
         }
         peers[r] = pr;
-        home[r] = home_slot(key_hash<KW>(key), table.cap);
+        home[r] = home_slot(hk, table.cap);
         first[r] = make_uint4(0u, 0u, 0u, 0u);
         if (kAhead && lane == (unsigned)(__ffs(pr) - 1)) first[r] = __ldcg(&table.key0[home[r]]);
     }
 
-    // Phase 2: per remainder, the group's weighted values are summed by its leader, which
-    // finds or inserts the vertex and adds them with one vector atomic; the first touch
-    // is a fire-and-forget atomicMin.  Every lane records the slot for the slice.
+    // Phase 2: per remainder, the group's leader finds or inserts the vertex and records
+    // the first touch (a fire-and-forget atomicMin: the leader's entry is the group's
+    // smallest); every lane then adds its own weighted values with one vector atomic.
+    // Summing a group in registers first does not pay here: the lanes of a vertex are
+    // rarely a run (on the 4K d=5 bilateral every warp has a vertex split over several
+    // runs), and gathering them costs more instructions than the L2 atomics it saves.
+    // Every lane records the slot for the slice.
 #pragma unroll
     for (int r = 0; r <= D; ++r) {
         const unsigned pr = peers[r];
@@ -351,38 +369,6 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
         Acc c[VDP];
 #pragma unroll
         for (int k = 0; k < VDP; ++k) c[k] = acc_mul<Acc>(sx.bary[r], v[k]);
-        // Neighbouring pixels usually share a vertex, so groups are mostly runs of
-        // consecutive lanes: then one segmented suffix sum over the warp (5 shuffle steps)
-        // leaves each run's total in its first lane.  Otherwise the leader adds its
-        // group's rows from shared memory one by one.
-        const unsigned run = pr >> leader;
-        if (__all_sync(active, (run & (run + 1u)) == 0u)) {
-            const unsigned last = 31u - __clz(pr);
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-#pragma unroll
-                for (int k = 0; k < VDP; ++k) {
-                    const Acc t = __shfl_down_sync(active, c[k], o);
-                    if (lane + o <= last) c[k] = acc_add(c[k], t);
-                }
-            }
-        } else {
-            if (pr != (1u << lane) && lane != leader) {
-#pragma unroll
-                for (int k = 0; k < VDP; ++k) stage[warp][lane][k] = c[k];
-            }
-            __syncwarp(active);
-            if (lane == leader) {
-                unsigned rest = pr & ~(1u << lane);
-                while (rest) {
-                    const int src = __ffs(rest) - 1;
-                    rest &= rest - 1;
-#pragma unroll
-                    for (int k = 0; k < VDP; ++k) c[k] = acc_add(c[k], stage[warp][src][k]);
-                }
-            }
-            __syncwarp(active);
-        }
         int s = -1;
         if (lane == leader) {
             Key<KW> kr;
@@ -395,12 +381,10 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
             }
             const uint4 w0 = kAhead ? first[r] : __ldcg(&table.key0[home[r]]);
             s = table_insert<KW>(table, kr, home[r], w0, status);
-            if (s >= 0) {
-                atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
-                atomicMin(&ft[s], e0 + (uint32_t)r);   // the leader's entry is the group's smallest
-            }
+            if (s >= 0) atomicMin(&ft[s], e0 + (uint32_t)r);
         }
         s = __shfl_sync(active, s, leader);
+        if (s >= 0) atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
         if (a.rec_slot)
             a.rec_slot[(size_t)r * a.n_total + gi] = s >= 0 ? sg.slot_base + (uint32_t)s : 0xFFFFFFFFu;
     }
