@@ -438,12 +438,21 @@ def run_ours(args):
         plain_stages = {k: round(statistics.mean(s[k] for s in plain_stage), 4)
                         for k in ("ms_splat", "ms_compact", "ms_neighbours", "ms_blur",
                                   "ms_slice", "ms_total")}
-        # algorithmic bytes of one splat launch: every frame's RGB read once (positions and
-        # values come from the same channels) + one key and one FP32 accumulator row per
-        # vertex
-        vd = 4
-        splat_bytes = FRAMES_PER_STEP * n * 3 * 4 + M * (2 * D + vd * 4)
+        # Algorithmic bytes per launch (all frames of the batch; M = measured vertices of the
+        # batch, C = 3 colour channels, Cp = 3 position source channels, vd = 4, p = payload
+        # bytes, 4 for the splat's FP32 accumulators):
+        #   splat  N*4*(Cp + C) read + M*(2d + vd*4) written (one key, one row per vertex)
+        #   blur   (d+1) * 2 * M*vd*p (each axis reads and writes the rows once)
+        #   slice  N*(d+1)*8 (replay record) + M*vd*p (rows read once) + N*4*C written
+        vd, C, Cp = 4, 3, 3
+        p = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[args.payload]
+        N = FRAMES_PER_STEP * n
+        splat_bytes = N * 4 * (Cp + C) + M * (2 * D + vd * 4)
+        blur_bytes = (D + 1) * 2 * M * vd * p
+        slice_bytes = N * (D + 1) * 8 + M * vd * p + N * 4 * C
         achieved = splat_bytes / (splat_ms / 1e3) / 1e9
+        total_bytes = splat_bytes + blur_bytes + slice_bytes
+        lattice_ms = statistics.mean(s["ms_total"] for s in stage)
         traffic = ncu_traffic().get("splat_dram_bytes")
         # FP16 error on the 4K frame against the FP64 lattice
         a = pristine[0].clone()
@@ -472,6 +481,12 @@ def run_ours(args):
                          "frac": round(achieved / hbm, 4), "traffic": traffic,
                          "algorithmic_bytes": splat_bytes,
                          "note": "latency bound on L2 probes and atomics; see profiles/"},
+            "roofline_pipeline": {"bytes": {"splat": splat_bytes, "blur": blur_bytes,
+                                            "slice": slice_bytes},
+                                  "ms": round(lattice_ms, 4),
+                                  "achieved": round(total_bytes / (lattice_ms / 1e3) / 1e9, 2),
+                                  "peak": hbm, "unit": "GB/s",
+                                  "frac": round(total_bytes / (lattice_ms / 1e3) / 1e9 / hbm, 4)},
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s",
                     "h2d_bytes_per_step": px_step * 3 * 4, "d2h_bytes_per_step": px_step * 3 * 4},
             "gpu_launches": args.steps * (KERNELS_PER_LATTICE + blur_launches(D)),

@@ -31,6 +31,14 @@ int Engine::ensure_hmeta(size_t bytes) {
     return PGPU_OK;
 }
 
+int Engine::ensure_copy_streams() {
+    if (copy_in) return PGPU_OK;
+    CUDA_TRY(cudaStreamCreateWithFlags(&copy_out, cudaStreamNonBlocking));
+    for (auto& e : pipe_ev) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CUDA_TRY(cudaStreamCreateWithFlags(&copy_in, cudaStreamNonBlocking));
+    return PGPU_OK;
+}
+
 void Engine::drop_graphs() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     graphs.clear();
@@ -41,6 +49,14 @@ void Engine::shutdown() {
     if (stream) cudaStreamSynchronize(stream);
     drop_graphs();
     for (auto& e : ev)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    for (cudaStream_t* cs : {&copy_in, &copy_out}) {
+        if (*cs) cudaStreamSynchronize(*cs), cudaStreamDestroy(*cs);
+        *cs = nullptr;
+    }
+    for (auto& e : pipe_ev)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    for (auto& e : join_ev)
         if (e) cudaEventDestroy(e), e = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
@@ -89,7 +105,12 @@ MetaLayout layout(int nseg, bool slice_segs) {
 
 }  // namespace
 
-int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
+// One pass over the batch.  Images whose hash-table range overflowed are listed in
+// *failed, with the larger range to use in *cap_next; their output is untouched (the
+// slice skips them), while every other image of the pass is finished.
+static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
+                          const std::vector<uint64_t>* cap_in, std::vector<int>* failed,
+                          std::vector<uint64_t>* cap_next, int pass) {
     const int d = B.d, vd = B.vd;
     const int nseg = (int)B.items.size();
     if (nseg == 0) return PGPU_OK;
@@ -141,6 +162,10 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
     }
     std::vector<uint64_t> cap(nseg);
     for (int k = 0; k < nseg; ++k) {
+        if (cap_in) {
+            cap[k] = (*cap_in)[k];
+            continue;
+        }
         const uint64_t n = B.items[k].n;
         uint64_t est = (uint64_t)std::ceil(ratio[k] * 1.3 * (double)n) + 256;
         est = std::min<uint64_t>(est, n * (uint64_t)(d + 1) + 256);
@@ -152,7 +177,7 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
     int rc;
     if ((rc = E.ensure_hmeta(L.total)) || (rc = E.meta.ensure(L.total))) return rc;
 
-    for (int attempt = 0; attempt < 6; ++attempt) {
+    {
         std::vector<uint64_t> sbase(nseg + 1);
         uint64_t cap_total = 0;
         for (int k = 0; k < nseg; ++k) {
@@ -371,34 +396,41 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
                             "image %d: positions leave the lattice's int16 key range (the reference's "
                             "keys wrap there and its rank indices leave [0, d]); scale them down", k);
             if (segstat[k] & (kStatusProbeLimit | kStatusSpinLimit)) {
-                cap[k] = std::max<uint64_t>((uint64_t)(cap[k] * 2.5), (uint64_t)(counts[k] / load * 2));
-                cap[k] = (cap[k] + 31) & ~31ull;
+                uint64_t c = std::max<uint64_t>((uint64_t)(cap[k] * 2.5), (uint64_t)(counts[k] / load * 2));
+                failed->push_back(k);
+                cap_next->push_back((c + 31) & ~31ull);
                 retry = true;
             }
         }
-        if (retry) continue;
 
         double rmax = 0.0;
+        uint64_t done_vertices = 0;
+        size_t fi = 0;
         for (int k = 0; k < nseg; ++k) {
+            if (fi < failed->size() && (*failed)[fi] == k) {
+                ++fi;
+                continue;
+            }
+            done_vertices += counts[k];
             if (!B.items[k].n) continue;
             const double r = (double)counts[k] / (double)B.items[k].n;
             E.ratio_by_sig[sig[k]] = r;
             rmax = std::max(rmax, r);
         }
         if (E.ratio_by_sig.size() > 4096) E.ratio_by_sig.clear();
-        E.ratio[d] = rmax;
+        if (!retry) E.ratio[d] = rmax;
         E.last_cap = cap_total;
-        if (B.vertices_out) B.vertices_out->assign(counts, counts + nseg);
+        if (B.vertices_out && !retry) B.vertices_out->assign(counts, counts + nseg);
 
         pgpu_stats s;
         memset(&s, 0, sizeof(s));
         s.points = (long long)n_total;
-        s.vertices = M;
+        s.vertices = retry ? (long long)done_vertices : (long long)M;
         s.capacity = (long long)cap_total;
         s.d = d;
         s.vd = vd;
         s.payload = B.payload;
-        s.retries = attempt;
+        s.retries = pass;
         if (!graph) {
             cudaEventElapsedTime(&s.ms_splat, E.ev[0], E.ev[1]);
             cudaEventElapsedTime(&s.ms_compact, E.ev[1], E.ev[2]);
@@ -410,7 +442,44 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
         set_stats(s);
         return PGPU_OK;
     }
-    return fail(PGPU_ERR_CAPACITY, "hash table overfull after retries (d=%d, %d images)", d, nseg);
+}
+
+// Every image of a batch is filtered in place, so an image whose range overflowed cannot
+// simply be rerun with its whole batch: the others are finished.  Only the overflowed
+// ones go again, as a smaller batch with larger ranges.  The statistics cover all passes.
+int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
+    if (B.items.empty()) return PGPU_OK;
+    BatchJob cur = B;
+    std::vector<uint64_t> caps;
+    pgpu_stats sum;
+    memset(&sum, 0, sizeof(sum));
+    for (int pass = 0; pass < 6; ++pass) {
+        std::vector<int> failed;
+        std::vector<uint64_t> next;
+        const int rc = run_batch_pass(E, cur, st, caps.empty() ? nullptr : &caps, &failed, &next, pass);
+        if (rc) return rc;
+        pgpu_stats s;
+        if (get_stats(&s)) {
+            if (pass == 0) sum.points = s.points, sum.d = s.d, sum.vd = s.vd, sum.payload = s.payload;
+            sum.vertices += s.vertices;
+            sum.capacity = std::max(sum.capacity, s.capacity);
+            sum.retries = pass;
+            sum.ms_splat += s.ms_splat, sum.ms_compact += s.ms_compact;
+            sum.ms_neighbours += s.ms_neighbours, sum.ms_blur += s.ms_blur;
+            sum.ms_slice += s.ms_slice, sum.ms_total += s.ms_total;
+        }
+        if (failed.empty()) {
+            set_stats(sum);
+            return PGPU_OK;
+        }
+        BatchJob again = cur;
+        again.items.clear();
+        for (int k : failed) again.items.push_back(cur.items[k]);
+        caps = next;
+        cur = std::move(again);
+    }
+    return fail(PGPU_ERR_CAPACITY, "hash table overfull after retries (d=%d, %d images)", B.d,
+                (int)B.items.size());
 }
 
 }  // namespace pgpu

@@ -96,6 +96,7 @@ int Engine::init(int dev) {
     CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaHostAlloc((void**)&hstat, 64, cudaHostAllocDefault));
     for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+    for (auto& e : join_ev) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return PGPU_OK;
 }
 
@@ -398,14 +399,161 @@ struct ApiScope {
             rc = fail(PGPU_ERR_CUDA, "cudaSetDevice(%d) failed", dev);
             return;
         }
-        st = (opt && opt->memory == PGPU_MEM_DEVICE && opt->stream) ? (cudaStream_t)opt->stream : E->stream;
+        const bool device = opt && opt->memory == PGPU_MEM_DEVICE;
+        st = (device && opt->stream) ? (cudaStream_t)opt->stream : E->stream;
+        // Device memory without a stream belongs to the legacy default stream (stream 0,
+        // torch's default): the engine's own stream does not synchronise with it, so it
+        // waits here for the work queued there before the call, and stream 0 waits on exit
+        // for the call's work.
+        if (device && !opt->stream) {
+            if (cudaEventRecord(E->join_ev[0], cudaStreamLegacy) != cudaSuccess ||
+                cudaStreamWaitEvent(E->stream, E->join_ev[0], 0) != cudaSuccess) {
+                rc = fail(PGPU_ERR_CUDA, "ordering against the default stream failed: %s",
+                          cudaGetErrorString(cudaGetLastError()));
+                return;
+            }
+            joined = true;
+        }
     }
+    ~ApiScope() {
+        if (joined && cudaEventRecord(E->join_ev[1], E->stream) == cudaSuccess)
+            cudaStreamWaitEvent(cudaStreamLegacy, E->join_ev[1], 0);
+    }
+    bool joined = false;
 };
 
 pgpu_options opts_or_default(const pgpu_options* o) {
     pgpu_options d;
     pgpu_default_options(&d);
     return o ? *o : d;
+}
+
+// The batched bilateral lattice job over images [i0, i1) of dv (device views):
+// JointBilateral::apply with each image as its own reference (src/GaussTransform.cpp:646-676).
+void bilateral_job(const pgpu_image* dv, int i0, int i1, const float* filter_width,
+                   const float* color_sigma, const pgpu_options& opt, BatchJob& B) {
+    const int C = dv[i0].channels;
+    B.d = C + 2;
+    B.vd = C + 1;
+    B.payload = opt.payload;
+    B.load = opt.load_factor;
+    B.homog = true;
+    B.replay = true;
+    B.use_graph = (opt.flags & PGPU_FLAG_GRAPH) != 0;
+    B.items.resize(i1 - i0);
+    volatile float one = 1.0f;
+    for (int i = i0; i < i1; ++i) {
+        BatchItem& it = B.items[i - i0];
+        PointSource& s = it.splat;
+        memset(&s, 0, sizeof(s));
+        s.width = dv[i].width;
+        s.height = dv[i].height;
+        s.frames = 1;
+        s.pos = planar(dv[i]);
+        s.pos_channels = C;
+        const float inv_r = one / color_sigma[i];
+        for (int c = 0; c < C; ++c) s.pos_scale[c] = inv_r;
+        s.coord_mask = 3;
+        s.coord_scale[0] = one / filter_width[i];
+        s.coord_scale[1] = one / filter_width[i];
+        s.val = planar(dv[i]);
+        s.val_channels = C;
+        s.homogeneous = 1;
+        it.n = (uint32_t)((size_t)dv[i].width * dv[i].height);
+        it.out = outview(dv[i], C, 1);
+    }
+}
+
+// Host-memory batches run in chunks of whole images of at least kChunkPixels pixels.  Two
+// device slots alternate: while the lattices of chunk k run on the compute stream, chunk
+// k+1 is uploaded on one copy stream and chunk k-1 downloaded on the other, so with
+// pinned host images the transfers hide behind the filtering.  A batch smaller than two
+// chunks is one chunk.  The reported statistics sum over the chunks.
+constexpr size_t kChunkPixels = size_t(1) << 22;
+
+int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int count,
+                         const float* filter_width, const float* color_sigma,
+                         const pgpu_options& opt) {
+    const int C = ims[0].channels;
+    std::vector<int> cut{0};
+    size_t acc = 0, slot_floats = 0, chunk_floats = 0;
+    for (int i = 0; i < count; ++i) {
+        const size_t px = (size_t)ims[i].width * ims[i].height;
+        acc += px;
+        chunk_floats += px * C;
+        if ((acc >= kChunkPixels && i + 1 < count) || i + 1 == count) {
+            cut.push_back(i + 1);
+            slot_floats = std::max(slot_floats, chunk_floats);
+            acc = chunk_floats = 0;
+        }
+    }
+    const int nchunks = (int)cut.size() - 1;
+    int rc;
+    if ((rc = E.img_a.ensure(slot_floats * sizeof(float))) ||
+        (nchunks > 1 && (rc = E.img_b.ensure(slot_floats * sizeof(float)))) ||
+        (rc = E.ensure_copy_streams()))
+        return rc;
+    cudaStream_t cin = E.copy_in, cout = E.copy_out;
+    cudaEvent_t* uploaded = E.pipe_ev;
+    cudaEvent_t* filtered = E.pipe_ev + 2;
+    cudaEvent_t* downloaded = E.pipe_ev + 4;
+    bool slot_used[2] = {false, false};
+    std::vector<pgpu_image> dv(ims, ims + count);
+
+    auto upload = [&](int k) -> int {
+        const int slot = k & 1;
+        float* base = (float*)(slot ? E.img_b.p : E.img_a.p);
+        if (slot_used[slot]) CUDA_TRY(cudaStreamWaitEvent(cin, downloaded[slot], 0));
+        size_t off = 0;
+        for (int i = cut[k]; i < cut[k + 1]; ++i) {
+            dv[i] = dense_like(ims[i], base + off, C);
+            off += (size_t)ims[i].width * ims[i].height * C;
+            int r = copy_view(ims[i], dv[i], C, cudaMemcpyHostToDevice, cin);
+            if (r) return r;
+        }
+        CUDA_TRY(cudaEventRecord(uploaded[slot], cin));
+        return PGPU_OK;
+    };
+    auto run = [&]() -> int {
+        pgpu_stats sum;
+        memset(&sum, 0, sizeof(sum));
+        int r = upload(0);
+        for (int k = 0; k < nchunks && !r; ++k) {
+            const int slot = k & 1;
+            if (k + 1 < nchunks && (r = upload(k + 1))) break;
+            CUDA_TRY(cudaStreamWaitEvent(st, uploaded[slot], 0));
+            BatchJob B;
+            bilateral_job(dv.data(), cut[k], cut[k + 1], filter_width, color_sigma, opt, B);
+            if ((r = run_batch(E, B, st))) break;
+            pgpu_stats s;
+            if (get_stats(&s)) {
+                sum.points += s.points;
+                sum.vertices += s.vertices;
+                sum.capacity = std::max(sum.capacity, s.capacity);
+                sum.d = s.d, sum.vd = s.vd, sum.payload = s.payload;
+                sum.retries += s.retries;
+                sum.ms_splat += s.ms_splat, sum.ms_compact += s.ms_compact;
+                sum.ms_neighbours += s.ms_neighbours, sum.ms_blur += s.ms_blur;
+                sum.ms_slice += s.ms_slice, sum.ms_total += s.ms_total;
+            }
+            CUDA_TRY(cudaEventRecord(filtered[slot], st));
+            CUDA_TRY(cudaStreamWaitEvent(cout, filtered[slot], 0));
+            for (int i = cut[k]; i < cut[k + 1] && !r; ++i)
+                r = copy_view(dv[i], ims[i], C, cudaMemcpyDeviceToHost, cout);
+            if (r) break;
+            CUDA_TRY(cudaEventRecord(downloaded[slot], cout));
+            slot_used[slot] = true;
+        }
+        if (!r) set_stats(sum);
+        return r;
+    };
+    rc = run();
+    // the caller's host images are in use until every copy has landed, error or not
+    const cudaError_t e1 = cudaStreamSynchronize(cin), e2 = cudaStreamSynchronize(cout);
+    if (!rc && (e1 != cudaSuccess || e2 != cudaSuccess))
+        return fail(PGPU_ERR_CUDA, "batch copies failed: %s",
+                    cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    return rc;
 }
 
 }  // namespace
@@ -520,56 +668,12 @@ int pgpu_bilateral_batch(pgpu_image* ims, int count, const float* filter_width,
     ApiScope S(&opt);
     if (S.rc) return S.rc;
     Engine& E = *S.E;
-    std::vector<pgpu_image> dv(ims, ims + count);
-    int rc;
-    if (opt.memory != PGPU_MEM_DEVICE) {   // one staging buffer for the whole batch
-        size_t total = 0;
-        for (int i = 0; i < count; ++i) total += (size_t)ims[i].width * ims[i].height * C;
-        if ((rc = E.img_a.ensure(total * sizeof(float)))) return rc;
-        size_t off = 0;
-        for (int i = 0; i < count; ++i) {
-            dv[i] = dense_like(ims[i], (float*)E.img_a.p + off, C);
-            off += (size_t)ims[i].width * ims[i].height * C;
-            if ((rc = copy_view(ims[i], dv[i], C, cudaMemcpyHostToDevice, S.st))) return rc;
-        }
+    if (opt.memory == PGPU_MEM_DEVICE) {
+        BatchJob B;
+        bilateral_job(ims, 0, count, filter_width, color_sigma, opt, B);
+        return run_batch(E, B, S.st);
     }
-    BatchJob B;
-    B.d = C + 2;
-    B.vd = C + 1;
-    B.payload = opt.payload;
-    B.load = opt.load_factor;
-    B.homog = true;
-    B.replay = true;
-    B.use_graph = (opt.flags & PGPU_FLAG_GRAPH) != 0;
-    B.items.resize(count);
-    volatile float one = 1.0f;
-    for (int i = 0; i < count; ++i) {
-        BatchItem& it = B.items[i];
-        PointSource& s = it.splat;
-        memset(&s, 0, sizeof(s));
-        s.width = dv[i].width;
-        s.height = dv[i].height;
-        s.frames = 1;
-        s.pos = planar(dv[i]);
-        s.pos_channels = C;
-        const float inv_r = one / color_sigma[i];
-        for (int c = 0; c < C; ++c) s.pos_scale[c] = inv_r;
-        s.coord_mask = 3;
-        s.coord_scale[0] = one / filter_width[i];
-        s.coord_scale[1] = one / filter_width[i];
-        s.val = planar(dv[i]);
-        s.val_channels = C;
-        s.homogeneous = 1;
-        it.n = (uint32_t)((size_t)dv[i].width * dv[i].height);
-        it.out = outview(dv[i], C, 1);
-    }
-    if ((rc = run_batch(E, B, S.st))) return rc;
-    if (opt.memory != PGPU_MEM_DEVICE) {
-        for (int i = 0; i < count; ++i)
-            if ((rc = copy_view(dv[i], ims[i], C, cudaMemcpyDeviceToHost, S.st))) return rc;
-        CUDA_TRY(cudaStreamSynchronize(S.st));
-    }
-    return PGPU_OK;
+    return bilateral_batch_host(E, S.st, ims, count, filter_width, color_sigma, opt);
 }
 
 int pgpu_lattice_dump(int d, int vd, int n, const float* pos, const float* val, int payload,

@@ -62,6 +62,10 @@ struct Engine {
     DevBuf img_a, img_b, img_c, img_d;
     unsigned* hstat = nullptr;
     cudaEvent_t ev[8] = {};
+    cudaEvent_t join_ev[2] = {};   // ordering against the legacy default stream
+    // host-memory batches: uploads and downloads overlap the lattices on these streams
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    cudaEvent_t pipe_ev[6] = {};   // per device slot: uploaded, filtered, downloaded
     std::map<int, double> ratio;                  // vertices per point of recent lattices, by d
     std::map<std::string, double> ratio_by_sig;   // ... by image shape and scales
     std::map<std::string, cudaGraphExec_t> graphs;  // captured batch pipelines, by batch shape
@@ -69,6 +73,7 @@ struct Engine {
     uint64_t buffers_epoch = 0;   // bumped whenever a buffer moves (invalidates graphs)
     int init(int dev);
     int ensure_hmeta(size_t bytes);
+    int ensure_copy_streams();
     void drop_graphs();
     void shutdown();   // release stream, events, pinned buffers and graphs
 };

@@ -52,6 +52,37 @@ def test_batch_matches_single_image_path(gpu):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("pinned", [False, True])
+def test_host_batch_in_overlapped_chunks(gpu, pinned):
+    """A host batch of more than two chunks' pixels (chunks of 2^22 pixels) is uploaded,
+    filtered and downloaded chunk by chunk on overlapping streams; every image must still
+    equal the single-image path, and the statistics must cover the whole batch."""
+    import torch
+    # three chunks: images 0-2, 3-5, 6 (slot 0 is reused by the third)
+    sizes = [(1920, 1200), (1600, 1000), (2048, 1152), (640, 480), (1280, 720), (2560, 1440),
+             (1024, 1024)]
+    imgs = [synth.image(w, h, 3, rects=12, seed=40 + k) for k, (w, h) in enumerate(sizes)]
+    ss = [8.0, 12.0, 16.0, 6.0, 10.0, 14.0, 9.0]
+    sr = [0.1, 0.15, 0.08, 0.2, 0.12, 0.1, 0.3]
+    expect = []
+    for im, s, r in zip(imgs, ss, sr):
+        e = im.copy()
+        gpu.Bilateral.apply(e, s, s, 0.0, r)
+        expect.append(e)
+    for rep in range(2):
+        if pinned:
+            keep = [torch.from_numpy(im.copy()).pin_memory() for im in imgs]
+            work = [t.numpy() for t in keep]
+        else:
+            work = [im.copy() for im in imgs]
+        gpu.bilateral_batch(work, ss, sr)
+        st = gpu.last_stats()
+        assert st["points"] == sum(w * h for w, h in sizes)
+        for w, e in zip(work, expect):
+            assert rel_err(w, e) <= RTOL_FP32
+
+
+@pytest.mark.gpu
 def test_batch_on_device_with_graph_replay(gpu):
     import torch
     imgs, ss, sr = uneven_batch(16, seed=4)
@@ -75,6 +106,34 @@ def test_batch_fp16_payload_error_vs_fp64(gpu):
     err = max(rel_err(o, r, floor_frac=1e-2) for o, r in zip(out, ref))
     print("batched fp16 max relative error vs FP64 lattice:", err)
     assert err <= 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("on_device", [False, True])
+def test_batch_retry_leaves_finished_images_alone(gpu, on_device):
+    """A textured image learns its vertex ratio; in the next batch a noisy image with no
+    learned ratio overflows its range and is rerun.  The textured image, finished in the
+    first pass (in place), must not be filtered a second time."""
+    import torch
+    tex = synth.image(200, 150, 3, rects=8, seed=21)
+    gpu.bilateral_batch([tex.copy()], [8.0], [0.1])
+    rng = np.random.default_rng(22)
+    # a shape of its own per variant: ratios are learned by shape and sigmas
+    noisy = rng.random((3, 90, 70 + 7 * int(on_device)), dtype=np.float32)
+    if on_device:
+        work = [torch.from_numpy(tex.copy()).cuda(), torch.from_numpy(noisy.copy()).cuda()]
+    else:
+        work = [tex.copy(), noisy.copy()]
+    gpu.bilateral_batch(work, [8.0, 1.0], [0.1, 0.02])
+    assert gpu.last_stats()["retries"] >= 1
+    if on_device:
+        torch.cuda.synchronize()
+        work = [w.cpu().numpy() for w in work]
+    e0, e1 = tex.copy(), noisy.copy()
+    gpu.Bilateral.apply(e0, 8.0, 8.0, 0.0, 0.1)
+    gpu.Bilateral.apply(e1, 1.0, 1.0, 0.0, 0.02)
+    assert rel_err(work[0], e0) <= RTOL_FP32
+    assert rel_err(work[1], e1) <= RTOL_FP32
 
 
 @pytest.mark.gpu
