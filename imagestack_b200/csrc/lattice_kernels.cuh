@@ -276,14 +276,16 @@ __device__ __forceinline__ double acc_add(double a, double b) { return __dadd_rn
 // splat
 // ---------------------------------------------------------------------------------
 constexpr int kSplatThreads = 256;
-// Tuning (measured on the 4K d=5 bilateral): the splat is latency bound, so resident warps
-// matter more than a few spilled registers — 4 blocks of 256 per SM up to d=6, fewer for
-// the larger per-point state of higher d.  Leaders issue the home-slot loads of all
-// remainders before resolving any for d <= PGPU_SPLAT_AHEAD_MAX_D.
+// Tuning (measured on the 4K d=5 and d=3 bilaterals and the 2M-point d=16 transform): the
+// splat is latency bound, so resident warps matter more than a few spilled registers —
+// 6 blocks of 256 per SM up to d=5 (40 registers; 0.94 -> 0.77 ms at 4K d=5), 4 for d=6,
+// fewer for the larger per-point state of higher d.  For 6 <= d <= PGPU_SPLAT_AHEAD_MAX_D
+// the leaders issue the home-slot loads of all remainders before resolving any; up to
+// d=5 the registers that takes cost more occupancy than the overlap gains.
 #ifndef PGPU_SPLAT_AHEAD_MAX_D
 #define PGPU_SPLAT_AHEAD_MAX_D 8
 #endif
-__host__ __device__ constexpr int splat_min_blocks(int d) { return d <= 6 ? 4 : d <= 8 ? 3 : 2; }
+__host__ __device__ constexpr int splat_min_blocks(int d) { return d <= 5 ? 6 : d <= 6 ? 4 : d <= 8 ? 3 : 2; }
 
 template <int D, int VDP, typename Acc>
 __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kernel(SplatArgs a) {
@@ -318,7 +320,7 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
     // confirmed against the group leader's key (a hash collision inside the warp falls
     // back to matching all key words); each group's leader starts loading its home slot.  For d <= 8 the loads of all d+1
     // remainders are in flight together before any is needed.
-    constexpr bool kAhead = D <= PGPU_SPLAT_AHEAD_MAX_D;
+    constexpr bool kAhead = D > 5 && D <= PGPU_SPLAT_AHEAD_MAX_D;
     unsigned peers[D + 1];
     uint32_t home[D + 1];
     uint4 first[D + 1];
