@@ -18,6 +18,8 @@
 //              by the homogeneous channel (src/GaussTransform.cpp:673-676).
 #pragma once
 
+#include <type_traits>
+
 #include "lattice_device.cuh"
 
 namespace pgpu {
@@ -518,8 +520,55 @@ __device__ __forceinline__ double blur3(double a, double b, double c) {
 // Row of vertex u (zeros for an absent vertex, u < 0), in arithmetic type A.
 template <int VDP, typename PS, typename A>
 __device__ __forceinline__ void load_row(const PS* src, int u, A (&r)[VDP]) {
+    // rows of 4 are read as one vector; an absent vertex (u < 0) reads vertex 0's row,
+    // which exists whenever any vertex does, and is then replaced by zeros
+    const size_t base = (size_t)(u >= 0 ? u : 0) * VDP;
+    if constexpr (std::is_same<PS, float>::value && VDP % 4 == 0) {
 #pragma unroll
-    for (int k = 0; k < VDP; ++k) r[k] = u >= 0 ? (A)Payload<PS>::load(src + (size_t)u * VDP + k) : (A)0;
+        for (int k = 0; k < VDP; k += 4) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(src + base + k));
+            r[k] = (A)q.x, r[k + 1] = (A)q.y, r[k + 2] = (A)q.z, r[k + 3] = (A)q.w;
+        }
+    } else if constexpr ((std::is_same<PS, __half>::value || std::is_same<PS, __nv_bfloat16>::value) &&
+                         VDP % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < VDP; k += 4) {
+            const uint2 q = __ldg(reinterpret_cast<const uint2*>(src + base + k));
+            const PS* h = reinterpret_cast<const PS*>(&q);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) r[k + j] = (A)Payload<PS>::load(h + j);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) r[k] = (A)Payload<PS>::load(src + base + k);
+    }
+    if (u < 0) {
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) r[k] = (A)0;
+    }
+}
+
+template <int VDP, typename PD, typename A>
+__device__ __forceinline__ void store_row(PD* dst, size_t row, const A (&r)[VDP]) {
+    if constexpr (std::is_same<PD, float>::value && VDP % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < VDP; k += 4)
+            *reinterpret_cast<float4*>(dst + row * VDP + k) =
+                make_float4((float)r[k], (float)r[k + 1], (float)r[k + 2], (float)r[k + 3]);
+    } else if constexpr ((std::is_same<PD, __half>::value || std::is_same<PD, __nv_bfloat16>::value) &&
+                         VDP % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < VDP; k += 4) {
+            uint2 q;
+            PD* h = reinterpret_cast<PD*>(&q);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) Payload<PD>::store(h + j, (float)r[k + j]);
+            *reinterpret_cast<uint2*>(dst + row * VDP + k) = q;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) Payload<PD>::store(dst + row * VDP + k, r[k]);
+    }
 }
 
 // [1 2 1]/4 of three rows.  Homogeneous rows (m_0..m_{wc-1}, w): blur w and the products
@@ -533,10 +582,11 @@ __device__ __forceinline__ void combine3(const A (&r1)[VDP], const A (&r0)[VDP],
         for (int k = 0; k < VDP; ++k)
             if (k == wc) { w1 = r1[k]; w0 = r0[k]; w2 = r2[k]; }
         const A nw = blur3(w1, w0, w2);
+        const A inv = nw != (A)0 ? (A)1 / nw : (A)0;
 #pragma unroll
         for (int k = 0; k < VDP; ++k) {
             if (k == wc) out[k] = nw;
-            else if (k < wc && nw != (A)0) out[k] = blur3(w1 * r1[k], w0 * r0[k], w2 * r2[k]) / nw;
+            else if (k < wc) out[k] = blur3(w1 * r1[k], w0 * r0[k], w2 * r2[k]) * inv;
             else out[k] = (A)0;
         }
     } else {
@@ -587,8 +637,7 @@ __global__ void blur_kernel(BlurArgs a) {
             blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, out);
         }
         const size_t row = a.dst_map ? (size_t)__ldg(a.dst_map + vtx) : (size_t)vtx;
-#pragma unroll
-        for (int k = 0; k < VDP; ++k) Payload<PD>::store(dst + row * VDP + k, out[k]);
+        store_row<VDP, PD, A>(dst, row, out);
     }
 }
 
@@ -626,6 +675,36 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
     A acc[VDP];
 #pragma unroll
     for (int k = 0; k < VDP; ++k) acc[k] = (A)0;
+    // Replay slice of small rows: the d+1 slots, then all d+1 rows in flight at once, as
+    // one vector load each (a vertex the splat could not place loads row 0, unused).
+    constexpr bool kGather = D <= 8 && VDP == 4 && sizeof(A) == 4;
+    if (kGather && a.rec_slot && !a.rec_vtx) {
+        int sl[D + 1];
+#pragma unroll
+        for (int r = 0; r <= D; ++r) sl[r] = (int)__ldg(a.rec_slot + (size_t)r * a.n_total + gi);
+        float4 rows[D + 1];
+#pragma unroll
+        for (int r = 0; r <= D; ++r)
+            rows[r] = __ldg(reinterpret_cast<const float4*>(sv) + (sl[r] >= 0 ? sl[r] : 0));
+#pragma unroll
+        for (int r = 0; r <= D; ++r) {
+            if (sl[r] < 0) continue;
+            const float w = sx.bary[r];
+            const A row[4] = {rows[r].x, rows[r].y, rows[r].z, rows[r].w};
+            if constexpr (HOMOG) {   // row (m_0.., w): accumulate (w*m_k, w)
+                A wt = row[0];
+#pragma unroll
+                for (int k = 0; k < VDP; ++k) if (k == a.vd - 1) wt = row[k];
+                const A bw = (A)w * wt;
+#pragma unroll
+                for (int k = 0; k < VDP; ++k)
+                    acc[k] = acc_add(acc[k], (k == a.vd - 1) ? bw : bw * row[k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < VDP; ++k) acc[k] = acc_add(acc[k], (A)w * row[k]);
+            }
+        }
+    } else {
     Key<KW> key;
     if (!a.rec_slot) first_key<D>(sx, key);
 #pragma unroll
@@ -661,6 +740,7 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
                 for (int k = 0; k < VDP; ++k) acc[k] = acc_add(acc[k], (A)w * row[k]);
             }
         }
+    }
     }
     // write
     const uint32_t wdt = (uint32_t)sg.src.width, hgt = (uint32_t)sg.src.height;
