@@ -1,15 +1,16 @@
 """Benchmark: bilateral filtering throughput and latency of the B200 permutohedral lattice.
 
 Headline workload (one "step"): a batch of four 3840x2160 RGB frames through the batched
-lattice with FP16 payload (FP32 accumulation), d=5 positions (r/0.1, g/0.1, b/0.1, x/16,
-y/16), values RGB + homogeneous 1, on seeded synthetic frames (gradients, 64 rectangles,
-Gaussian noise sigma 0.05).  `value` is Mpix/s with the frames already resident in HBM;
-`e2e` is the same step through the C ABI with pinned host frames, host->device and
+lattice (FP32 values by default, --payload to change), d=5 positions (r/0.1, g/0.1, b/0.1,
+x/16, y/16), values RGB + homogeneous 1, on seeded synthetic frames (gradients, 64
+rectangles, Gaussian noise sigma 0.05).  `value` is Mpix/s with the frames already resident
+in HBM; `e2e` is the same step through the C ABI with pinned host frames, host->device and
 device->host copies inside the timed region.  Beside it, the same line reports the plain
-GPU lattice (one FP32 frame per call), the mixed-size batch (256 images, sides
-log-uniform 128..1024, per-image sigmas), a served request stream (Poisson arrivals
-ramped 50 -> 2000 req/s, bilateral RGB and grey joint-bilateral requests, sides 64..2048)
-with p50/p99 latency, and the FP16 error against the FP64 lattice.
+GPU lattice (one FP32 frame per call), the same batch with the FP16 payload, the
+mixed-size batch (256 images, sides log-uniform 128..1024, per-image sigmas, FP16, CUDA
+graph), a served request stream (Poisson arrivals ramped 50 -> 2000 req/s, bilateral RGB
+and grey joint-bilateral requests, sides 64..2048) with p50/p99 latency, and each
+payload's error against the FP64 lattice.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -33,8 +34,13 @@ sys.path.insert(0, ROOT)
 W, H, SIGMA_S, SIGMA_R, RECTS, SEED = 3840, 2160, 16.0, 0.1, 64, 2
 FRAMES_PER_STEP = 4
 METRIC = "bilateral Mpix/s (d=5 4K, batched) vs plain GPU; p50/p99 latency @ err<=1e-3"
-WORKLOAD = ("bilateral RGB 3840x2160 x%d frames per batch, d=5 (sigma_s 16, sigma_r 0.1), "
-            "FP16 payload / FP32 accumulation" % FRAMES_PER_STEP)
+PAYLOAD_NAMES = {"fp32": "FP32 values", "fp16": "FP16 payload / FP32 accumulation",
+                 "bf16": "BF16 payload / FP32 accumulation", "fp64": "FP64 values"}
+
+
+def workload(payload):
+    return ("bilateral RGB 3840x2160 x%d frames per batch, d=5 (sigma_s 16, sigma_r 0.1), %s"
+            % (FRAMES_PER_STEP, PAYLOAD_NAMES[payload]))
 L2_BYTES = 126 * 1024 * 1024
 KERNELS_PER_LATTICE = 9   # splat, mark, 3 scan phases, counts, assign, neighbours, slice
 D = 5
@@ -201,7 +207,7 @@ def run_reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "sample": sample},
+            "config": {"workload": workload(args.payload), "sample": sample},
             "cpu_baseline": {"value": round(value, 4), "unit": "Mpix/s", "cores": procs,
                              "kind": kind, "sample": sample},
             "e2e": {"value": round(value, 4), "unit": "Mpix/s", "h2d_bytes_per_step": 0,
@@ -386,11 +392,21 @@ def run_ours(args):
         ib.Bilateral.apply(work[0], SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload="fp32")
     plain.stats = ib.last_stats
 
+    # the same batch with the 16-bit payload (FP16 rows, FP32 accumulation), beside it
+    alt_payload = "fp16" if args.payload != "fp16" else "fp32"
+
+    def alt():
+        ib.bilateral_batch(work, ss, sr, payload=alt_payload)
+    alt.stats = ib.last_stats
+
     for _ in range(args.warmup):
         prepare()
         headline()
         prepare()
         plain()
+        if not args.quick:
+            prepare()
+            alt()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -398,6 +414,8 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         total_ms, stage = timed_steps(stream, args.steps, headline, prepare)
     plain_ms, plain_stage = timed_steps(stream, args.steps, plain, prepare)
+    if not args.quick:
+        alt_ms, alt_stage = timed_steps(stream, args.steps, alt, prepare)
     if dist:
         t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -454,13 +472,24 @@ def run_ours(args):
         total_bytes = splat_bytes + blur_bytes + slice_bytes
         lattice_ms = statistics.mean(s["ms_total"] for s in stage)
         traffic = ncu_traffic().get("splat_dram_bytes")
-        # FP16 error on the 4K frame against the FP64 lattice
+        # the payload's error on the 4K frame against the FP64 lattice
         a = pristine[0].clone()
         ib.Bilateral.apply(a, SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload=args.payload)
         b = pristine[0].clone()
         ib.Bilateral.apply(b, SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload="fp64")
         torch.cuda.synchronize()
         err4k = rel_err(a.cpu().numpy(), b.cpu().numpy())
+        if not args.quick:
+            c = pristine[0].clone()
+            ib.Bilateral.apply(c, SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload=alt_payload)
+            torch.cuda.synchronize()
+            alt_line = {
+                "payload": alt_payload, "path": "batched",
+                "mpix_s": round(px_step * args.steps / (alt_ms / 1e3) / 1e6, 2),
+                "max_rel_err_vs_fp64": rel_err(c.cpu().numpy(), b.cpu().numpy()),
+                "stages_ms": {k: round(statistics.mean(s_[k] for s_ in alt_stage), 4)
+                              for k in ("ms_splat", "ms_compact", "ms_neighbours", "ms_blur",
+                                        "ms_slice", "ms_total")}}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
@@ -468,7 +497,7 @@ def run_ours(args):
             "dtype": {"fp32": "f32", "fp16": "f16-payload/f32-accum",
                       "bf16": "bf16-payload/f32-accum", "fp64": "f64"}[args.payload],
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "frame": [W, H], "frames_per_step": FRAMES_PER_STEP,
+            "config": {"workload": workload(args.payload), "frame": [W, H], "frames_per_step": FRAMES_PER_STEP,
                        "seed": SEED, "payload": args.payload, "path": "batched",
                        "l2": "flushed between steps (512 MiB write), outside the timed window",
                        "parallelism": "replicas x%d" % world},
@@ -493,6 +522,8 @@ def run_ours(args):
             "stages_ms": stages, "vertices": M, "capacity": stage[-1]["capacity"],
             "clocks": clk.summary(),
         }
+        if not args.quick:
+            line["batched_" + alt_payload] = alt_line
         if world == 1 and not args.quick:
             line["mixed_batch"] = mixed_batch(ib, synth, torch, dev, steps=6)
             line["served"] = served_stream(ib, synth, torch)
@@ -515,7 +546,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--payload", default="fp16", choices=["fp32", "fp16", "bf16", "fp64"])
+    ap.add_argument("--payload", default="fp32", choices=["fp32", "fp16", "bf16", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="headline and plain path only")
     args = ap.parse_args()

@@ -645,6 +645,8 @@ __global__ void blur_kernel(BlurArgs a) {
 // slice
 // ---------------------------------------------------------------------------------
 constexpr int kSliceThreads = 256;
+// latency bound like the splat: 6 blocks of 256 per SM (40 registers) up to d=8
+__host__ __device__ constexpr int slice_min_blocks(int d) { return d <= 8 ? 6 : 1; }
 
 // A: arithmetic and storage type of the filtered rows (float, or double for the FP64
 // lattice); rows live in slot space (svals[slot*VDP ..]).  With rec_slot the slots come
@@ -652,7 +654,7 @@ constexpr int kSliceThreads = 256;
 // src/Permutohedral.h:418-427); without it the keys are looked up (re-elevation slice at
 // other positions, :405-407), and a vertex the splat never created contributes zero.
 template <int D, int VDP, typename A, bool HOMOG>
-__global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
+__global__ void __launch_bounds__(kSliceThreads, slice_min_blocks(D)) slice_kernel(SliceArgs a) {
     constexpr int KW = key_words(D);
     __shared__ float s_delta[(D + 1) * kSliceThreads];
     __shared__ unsigned char s_coord[(D + 1) * kSliceThreads];
@@ -686,12 +688,22 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
 #pragma unroll
         for (int r = 0; r <= D; ++r)
             rows[r] = __ldg(reinterpret_cast<const float4*>(sv) + (sl[r] >= 0 ? sl[r] : 0));
+        // homogeneous rows with the weight in the last lane (vd == 4, the bilateral's
+        // RGB + 1) take the weight from a fixed lane
+        const bool wlast = a.vd == VDP;
 #pragma unroll
         for (int r = 0; r <= D; ++r) {
             if (sl[r] < 0) continue;
             const float w = sx.bary[r];
             const A row[4] = {rows[r].x, rows[r].y, rows[r].z, rows[r].w};
             if constexpr (HOMOG) {   // row (m_0.., w): accumulate (w*m_k, w)
+                if (wlast) {
+                    const A bw = (A)w * row[VDP - 1];
+#pragma unroll
+                    for (int k = 0; k < VDP - 1; ++k) acc[k] = acc_add(acc[k], bw * row[k]);
+                    acc[VDP - 1] = acc_add(acc[VDP - 1], bw);
+                    continue;
+                }
                 A wt = row[0];
 #pragma unroll
                 for (int k = 0; k < VDP; ++k) if (k == a.vd - 1) wt = row[k];
@@ -747,18 +759,18 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kernel(SliceArgs a) {
     const uint32_t x = i % wdt, q = i / wdt, y = q % hgt, t = q / hgt;
     const OutView& ov = sg.out;
     float* o = ov.base + (long long)t * ov.tstride + (long long)y * ov.ystride + x;
+    A wsum = acc[0];
+#pragma unroll
+    for (int j = 0; j < VDP; ++j) if (j == a.vd - 1) wsum = acc[j];
+    // a 16-bit payload's result is normalised with one reciprocal (its error budget is
+    // 1e-3); FP32 and FP64 divide per channel, as src/GaussTransform.cpp:673-676 does
+    const A inv = (A)1 / wsum;
 #pragma unroll
     for (int k = 0; k < VDP; ++k) {
         if (k < ov.channels) {
             float r;
-            if (ov.normalize) {
-                A wsum = acc[0];
-#pragma unroll
-                for (int j = 0; j < VDP; ++j) if (j == a.vd - 1) wsum = acc[j];
-                r = (float)(acc[k] / wsum);
-            } else {
-                r = (float)acc[k];
-            }
+            if (ov.normalize) r = HOMOG ? (float)(acc[k] * inv) : (float)(acc[k] / wsum);
+            else r = (float)acc[k];
             o[(long long)k * ov.cstride] = r;
         }
     }
