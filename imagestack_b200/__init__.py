@@ -63,7 +63,7 @@ class Stats(C.Structure):
 
 EXPORTS = ["pgpu_default_options", "pgpu_last_error", "pgpu_version", "pgpu_device_count",
            "pgpu_gauss_transform", "pgpu_joint_bilateral", "pgpu_bilateral", "pgpu_last_stats",
-           "pgpu_lattice_dump", "pgpu_bilateral_batch"]
+           "pgpu_lattice_dump", "pgpu_bilateral_batch", "pgpu_exact_gauss_transform_f64"]
 
 _lib = None
 
@@ -89,6 +89,8 @@ def lib():
     L.pgpu_lattice_dump.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                     P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p]
+    L.pgpu_exact_gauss_transform_f64.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = L
     return L
 
@@ -96,6 +98,30 @@ def lib():
 def _check(rc: int):
     if rc != OK:
         raise PgpuError(rc, lib().pgpu_last_error().decode(errors="replace"))
+
+
+def exact_gauss_transform_f64(queries, positions, values):
+    """FP64 brute-force Gauss transform on the GPU: for each query row,
+    sum_j exp(-|q - p_j|^2 / 2) v_j over all rows of `positions` (already divided by the
+    sigmas), as the EXACT method of GaussTransform::apply (src/GaussTransform.cpp:135-162)
+    defines it but with an exact exponential.  CUDA float32 tensors, interleaved
+    (queries nq x d, positions n x d, values n x vd); returns an nq x vd float64 tensor.
+    It states the error of lattice results and is not a filtering path."""
+    import torch
+    q = queries.contiguous()
+    p = positions.contiguous()
+    v = values.contiguous()
+    for t in (q, p, v):
+        if not (t.is_cuda and t.dtype == torch.float32 and t.dim() == 2):
+            raise PgpuError(ERR_ARGUMENT, "CUDA float32 matrices expected")
+    if q.shape[1] != p.shape[1] or p.shape[0] != v.shape[0]:
+        raise PgpuError(ERR_ARGUMENT, "mismatched shapes")
+    out = torch.empty((q.shape[0], v.shape[1]), dtype=torch.float64, device=q.device)
+    stream = C.c_void_p(torch.cuda.current_stream(q.device).cuda_stream)
+    _check(lib().pgpu_exact_gauss_transform_f64(q.shape[1], v.shape[1], q.shape[0], q.data_ptr(),
+                                                p.shape[0], p.data_ptr(), v.data_ptr(),
+                                                out.data_ptr(), stream))
+    return out
 
 
 def last_stats() -> dict:

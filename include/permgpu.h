@@ -210,6 +210,16 @@ int pgpu_bilateral_noalloc(const float *d_in, float *d_out, int width, int heigh
                            int channels, float filter_width, float filter_height,
                            float color_sigma, void *stream);
 
+/* FP64 brute-force Gauss transform at sampled queries, the error oracle for lattice
+ * results: out[i][c] = sum_j exp(-|q_i - p_j|^2 / 2) v_j[c] over all n sources, positions
+ * already divided by their sigmas.  It is the kernel of GaussTransform::apply's EXACT
+ * method (src/GaussTransform.cpp:135-162) with an exact double exponential instead of its
+ * table; not a filtering path.  Device memory, interleaved: q nq x d, p n x d and
+ * v n x vd float32, out nq x vd double; d 1..16, vd 1..8.  Returns after `stream`
+ * (cudaStream_t, NULL: the legacy default stream) has finished. */
+int pgpu_exact_gauss_transform_f64(int d, int vd, int nq, const float *q, int n,
+                                   const float *p, const float *v, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

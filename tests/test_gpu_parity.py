@@ -219,3 +219,24 @@ def test_low_precision_payload_error_vs_fp64(gpu, payload, tol):
     err = rel_err(out, ref, floor_frac=1e-2)
     print(payload, "max relative error vs FP64 lattice:", err)
     assert err <= tol
+
+
+def test_exact_gauss_transform_f64_matches_oracle(gpu):
+    """The GPU FP64 brute-force transform (the error oracle) against the C oracle's FP64
+    brute force, and the lattice's own error against it (reported: the permutohedral
+    lattice approximates the Gaussian, so only a loose bound holds)."""
+    import torch
+    g = golden("lattice_rgb_d5")
+    pos, val = g["pos"], g["val"]
+    rng = np.random.default_rng(5)
+    qi = rng.choice(pos.shape[0], 64, replace=False)
+    cpu = oracle.exact_gauss_transform(pos[qi], pos, val)
+    dev = gpu.exact_gauss_transform_f64(torch.from_numpy(pos[qi]).cuda(),
+                                        torch.from_numpy(pos).cuda(),
+                                        torch.from_numpy(val).cuda()).cpu().numpy()
+    assert rel_err(dev, cpu, floor_frac=1e-12) <= 1e-10
+    lat = gpu.lattice_dump(pos, val)["out"][qi]
+    norm = lambda a: a[:, :-1] / a[:, -1:]
+    err = rel_err(norm(lat), norm(cpu), floor_frac=1e-2)
+    print("lattice vs exact Gauss transform, max relative error:", err)
+    assert err < 0.5
