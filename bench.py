@@ -41,6 +41,8 @@ PAYLOAD_NAMES = {"fp32": "FP32 values", "fp16": "FP16 payload / FP32 accumulatio
 def workload(payload):
     return ("bilateral RGB 3840x2160 x%d frames per batch, d=5 (sigma_s 16, sigma_r 0.1), %s"
             % (FRAMES_PER_STEP, PAYLOAD_NAMES[payload]))
+
+
 L2_BYTES = 126 * 1024 * 1024
 KERNELS_PER_LATTICE = 9   # splat, mark, 3 scan phases, counts, assign, neighbours, slice
 D = 5
@@ -121,10 +123,8 @@ class ClockSampler:
 
 
 def dist_init():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from imagestack_b200.replicas import rank_env
+    return rank_env()
 
 
 def rel_err(a, b, floor_frac=1e-2):
@@ -397,8 +397,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    frames = [synth.image(W, H, 3, rects=RECTS, seed=SEED + 17 * rank + k)
-              for k in range(FRAMES_PER_STEP)]
+    from imagestack_b200.replicas import frame_seeds, max_over_ranks
+    frames = [synth.image(W, H, 3, rects=RECTS, seed=s)
+              for s in frame_seeds(rank, FRAMES_PER_STEP, SEED)]
     pristine = [torch.from_numpy(f).to(dev) for f in frames]
     work = [torch.empty_like(p) for p in pristine]
     flush = torch.empty(4 * L2_BYTES // 4, dtype=torch.float32, device=dev)
@@ -443,10 +444,7 @@ def run_ours(args):
     plain_ms, plain_stage = timed_steps(stream, args.steps, plain, prepare)
     if not args.quick:
         alt_ms, alt_stage = timed_steps(stream, args.steps, alt, prepare)
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dev)
     ms_per_step = total_ms / args.steps
     px_step = W * H * FRAMES_PER_STEP
     value = world * px_step * args.steps / (total_ms / 1e3) / 1e6
@@ -466,10 +464,7 @@ def run_ours(args):
         if i >= args.warmup:
             e2e_times.append(el)
     e2e_s = sum(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dev)
     e2e = world * px_step * e2e_steps / e2e_s / 1e6
 
     if rank == 0:
