@@ -61,6 +61,8 @@ class Stats(C.Structure):
                 ("ms_blur", C.c_float), ("ms_slice", C.c_float), ("ms_total", C.c_float)]
 
 
+from .tmpfile import load_tmp, save_tmp  # noqa: E402,F401  (ImageStack .tmp files)
+
 EXPORTS = ["pgpu_default_options", "pgpu_last_error", "pgpu_version", "pgpu_device_count",
            "pgpu_gauss_transform", "pgpu_joint_bilateral", "pgpu_bilateral", "pgpu_last_stats",
            "pgpu_lattice_dump", "pgpu_bilateral_batch", "pgpu_exact_gauss_transform_f64"]
