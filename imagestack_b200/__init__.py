@@ -58,7 +58,8 @@ class Stats(C.Structure):
     _fields_ = [("points", C.c_longlong), ("vertices", C.c_longlong), ("capacity", C.c_longlong),
                 ("d", C.c_int), ("vd", C.c_int), ("payload", C.c_int), ("retries", C.c_int),
                 ("ms_splat", C.c_float), ("ms_compact", C.c_float), ("ms_neighbours", C.c_float),
-                ("ms_blur", C.c_float), ("ms_slice", C.c_float), ("ms_total", C.c_float)]
+                ("ms_blur", C.c_float), ("ms_slice", C.c_float), ("ms_total", C.c_float),
+                ("load_factor", C.c_float), ("blur_pairs", C.c_int)]
 
 
 from .tmpfile import load_tmp, save_tmp  # noqa: E402,F401  (ImageStack .tmp files)
@@ -250,14 +251,17 @@ class Bilateral:
 
 
 FLAG_GRAPH = 1
+FLAG_AUTOTUNE = 2
 
 
 def bilateral_batch(images, filter_widths, color_sigmas, payload: str = "fp32",
-                    graph: bool = False, load_factor: float = 0.5):
+                    graph: bool = False, load_factor: float = 0.5, autotune: bool = False):
     """Bilateral filter of many images (same channel count, any sizes) in one set of
     launches, each in place with its own sigmas; the result of each equals
     Bilateral.apply on it.  All numpy (host) or all torch CUDA tensors (device, run on
-    torch's current stream)."""
+    torch's current stream).  graph: capture the launches as a CUDA graph and replay it
+    for later batches of the same shape.  autotune: the first calls of each batch shape
+    try candidate load factors and blur pairings, later calls use the fastest."""
     n = len(images)
     if len(filter_widths) != n or len(color_sigmas) != n:
         raise PgpuError(ERR_ARGUMENT, "one filter width and colour sigma per image")
@@ -274,7 +278,7 @@ def bilateral_batch(images, filter_widths, color_sigmas, payload: str = "fp32",
     stream = _torch_stream(images[0]) if (n and mem == MEM_DEVICE) else None
     opt = _options(mem, payload, stream=stream, load_factor=load_factor,
                    device=(images[0].device.index or 0) if (n and mem == MEM_DEVICE) else 0)
-    opt.flags = FLAG_GRAPH if graph else 0
+    opt.flags = (FLAG_GRAPH if graph else 0) | (FLAG_AUTOTUNE if autotune else 0)
     _check(lib().pgpu_bilateral_batch(views, n, fw, cs, C.byref(opt)))
     return images
 

@@ -324,6 +324,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             bp.vtx2slot = (const uint32_t*)E.vtx2slot.p;
             bp.wc = vd - 1;
             bp.sms = E.sms;
+            bp.pairs = B.blur_pairs;
             if (blur_all_axes(bp, st)) return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
             CUDA_TRY(cudaGetLastError());
             if (timed) CUDA_TRY(cudaEventRecord(E.ev[4], st));
@@ -359,6 +360,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
                      (unsigned long long)ns_total, (unsigned long long)cap_total, nwords, E.key0.p,
                      E.tvals.p, E.nbr.p, E.rec.p, E.meta.p, (void*)E.hmeta, E.sval.p);
             std::string gk(key);
+            gk += B.blur_pairs ? ":p" : ":s";
             for (int k = 0; k < nseg; ++k) gk += ":" + std::to_string(cap[k]) + "/" + std::to_string(B.items[k].n);
             auto it = E.graphs.find(gk);
             if (it == E.graphs.end()) {
@@ -431,6 +433,8 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         s.vd = vd;
         s.payload = B.payload;
         s.retries = pass;
+        s.load_factor = load;
+        s.blur_pairs = B.blur_pairs ? 1 : 0;
         if (!graph) {
             cudaEventElapsedTime(&s.ms_splat, E.ev[0], E.ev[1]);
             cudaEventElapsedTime(&s.ms_compact, E.ev[1], E.ev[2]);
@@ -447,9 +451,42 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
 // Every image of a batch is filtered in place, so an image whose range overflowed cannot
 // simply be rerun with its whole batch: the others are finished.  Only the overflowed
 // ones go again, as a smaller batch with larger ranges.  The statistics cover all passes.
+// Autotuner candidates: hash-table load factor and blur pairing.  The first calls of a
+// batch shape try them in turn; later calls of the shape use the fastest by the lattice's
+// device time.  Keys, vertex order and FP32/FP64 results do not depend on the choice; a
+// 16-bit payload tries fused pairs only, because one axis per pass rounds its rows to 16
+// bits between axes, which the pair keeps in FP32 registers.
+struct TuneCandidate {
+    float load;
+    bool pairs;
+};
+constexpr TuneCandidate kTune[] = {{0.5f, true}, {0.35f, true}, {0.7f, true}, {0.5f, false}};
+constexpr int kTuneCount = (int)(sizeof(kTune) / sizeof(kTune[0]));
+
+static std::string tune_key(const BatchJob& B) {
+    uint64_t n = 0;
+    for (const BatchItem& it : B.items) n += it.n;
+    int lg = 0;
+    while ((1ull << lg) < n) ++lg;
+    char buf[96];
+    snprintf(buf, sizeof(buf), "%d:%d:%d:%d:%d:%zu:%d", B.d, B.vd, B.payload, (int)B.homog,
+             (int)B.replay, B.items.size(), lg);
+    return buf;
+}
+
 int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
     if (B.items.empty()) return PGPU_OK;
     BatchJob cur = B;
+    int cand = -1;
+    Engine::Tuning* tune = nullptr;
+    if (B.autotune && !B.rec_vtx && !B.dump_splat) {
+        if (E.tuning.size() > 1024) E.tuning.clear();
+        tune = &E.tuning[tune_key(B)];
+        tune->count = (B.payload == kPayloadF16 || B.payload == kPayloadBF16) ? 3 : kTuneCount;
+        cand = tune->trials < tune->count ? tune->trials : tune->best;
+        cur.load = kTune[cand].load;
+        cur.blur_pairs = kTune[cand].pairs;
+    }
     std::vector<uint64_t> caps;
     pgpu_stats sum;
     memset(&sum, 0, sizeof(sum));
@@ -469,7 +506,18 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
             sum.ms_slice += s.ms_slice, sum.ms_total += s.ms_total;
         }
         if (failed.empty()) {
+            sum.load_factor = s.load_factor;
+            sum.blur_pairs = s.blur_pairs;
             set_stats(sum);
+            if (tune && tune->trials < tune->count) {
+                tune->ms[tune->trials++] = sum.ms_total;
+                if (tune->trials == tune->count) {
+                    int best = 0;
+                    for (int c = 1; c < tune->count; ++c)
+                        if (tune->ms[c] < tune->ms[best]) best = c;
+                    tune->best = best;
+                }
+            }
             return PGPU_OK;
         }
         BatchJob again = cur;

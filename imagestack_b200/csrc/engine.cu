@@ -440,6 +440,7 @@ void bilateral_job(const pgpu_image* dv, int i0, int i1, const float* filter_wid
     B.homog = true;
     B.replay = true;
     B.use_graph = (opt.flags & PGPU_FLAG_GRAPH) != 0;
+    B.autotune = (opt.flags & PGPU_FLAG_AUTOTUNE) != 0;
     B.items.resize(i1 - i0);
     volatile float one = 1.0f;
     for (int i = i0; i < i1; ++i) {
@@ -531,6 +532,7 @@ int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int 
                 sum.vertices += s.vertices;
                 sum.capacity = std::max(sum.capacity, s.capacity);
                 sum.d = s.d, sum.vd = s.vd, sum.payload = s.payload;
+                sum.load_factor = s.load_factor, sum.blur_pairs = s.blur_pairs;
                 sum.retries += s.retries;
                 sum.ms_splat += s.ms_splat, sum.ms_compact += s.ms_compact;
                 sum.ms_neighbours += s.ms_neighbours, sum.ms_blur += s.ms_blur;

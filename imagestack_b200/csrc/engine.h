@@ -69,6 +69,14 @@ struct Engine {
     std::map<int, double> ratio;                  // vertices per point of recent lattices, by d
     std::map<std::string, double> ratio_by_sig;   // ... by image shape and scales
     std::map<std::string, cudaGraphExec_t> graphs;  // captured batch pipelines, by batch shape
+    // autotuner state per batch shape: candidate trials so far, their times, the choice
+    struct Tuning {
+        int trials = 0;
+        int count = 0;   // candidates this shape tries
+        float ms[8] = {};
+        int best = 0;
+    };
+    std::map<std::string, Tuning> tuning;
     size_t last_cap = 0;
     uint64_t buffers_epoch = 0;   // bumped whenever a buffer moves (invalidates graphs)
     int init(int dev);
@@ -107,6 +115,8 @@ struct BatchJob {
     bool homog = false;    // the last value channel is the homogeneous weight
     bool replay = true;    // slice at the splat points
     bool use_graph = false;   // capture / replay the launch sequence as a CUDA graph
+    bool autotune = false;    // pick load factor and blur pairing per batch shape
+    bool blur_pairs = true;   // blur two axes per launch
     std::vector<BatchItem> items;
     // parity dumps (single-item jobs)
     int* rec_vtx = nullptr;

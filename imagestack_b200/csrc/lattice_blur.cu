@@ -72,7 +72,7 @@ int blur_all_axes(const BlurPlan& p, cudaStream_t st) {
     bool src_f32 = p.src_f32;
     int flip = 0;
     for (int j = 0; j < axes;) {
-        const bool pair = j + 1 < axes;
+        const bool pair = p.pairs && j + 1 < axes;
         const int step = pair ? 2 : 1;
         const bool last = j + step >= axes;
         BlurArgs ba;

@@ -62,6 +62,7 @@ struct BlurPlan {
     void* sval;
     const uint32_t* vtx2slot;
     int wc, sms;
+    bool pairs = true;     // fuse consecutive axes into one launch
 };
 int blur_all_axes(const BlurPlan& p, cudaStream_t st);   // 0 on success
 

@@ -66,6 +66,8 @@ typedef struct pgpu_stats {
     long long capacity;    /* hash-table slots used */
     int d, vd, payload, retries;
     float ms_splat, ms_compact, ms_neighbours, ms_blur, ms_slice, ms_total;
+    float load_factor;     /* hash-table load factor used */
+    int blur_pairs;        /* 1: blur axes fused in pairs, 0: one axis per pass */
 } pgpu_stats;
 
 /* Fill *opt with the defaults. */
@@ -110,8 +112,14 @@ int pgpu_bilateral(pgpu_image *im, float filter_width, float filter_height,
  * must share the channel count (1..7) and be single frames larger than 1x1 with
  * 0 < filter width < 10 x their width and height.  Every image keeps its own lattice
  * (its own hash-table range).  opt->flags & PGPU_FLAG_GRAPH captures the launch sequence
- * as a CUDA graph and replays it for later batches of the same shape. */
+ * as a CUDA graph and replays it for later batches of the same shape.
+ * opt->flags & PGPU_FLAG_AUTOTUNE lets the first calls of each batch shape (the number
+ * of images, the point count to a power of two, d, the payload) try candidate settings
+ * — hash-table load factor 0.5, 0.35 or 0.7, blur axes fused in pairs or (FP32/FP64
+ * payloads only) one per pass — and keeps the fastest for later calls of that shape
+ * (opt->load_factor is then unused); results do not depend on the choice. */
 #define PGPU_FLAG_GRAPH 1
+#define PGPU_FLAG_AUTOTUNE 2
 int pgpu_bilateral_batch(pgpu_image *ims, int count, const float *filter_width,
                          const float *color_sigma, const pgpu_options *opt);
 

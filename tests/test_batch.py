@@ -97,6 +97,50 @@ def test_batch_on_device_with_graph_replay(gpu):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("graph", [False, True])
+def test_autotuned_batch_tries_candidates_then_keeps_one(gpu, graph):
+    """With autotune the first four calls of a batch shape try (load factor, blur pairing)
+    candidates and later calls keep the fastest; every call's results equal the
+    single-image path."""
+    import torch
+    imgs, ss, sr = uneven_batch(10 + int(graph), seed=12)
+    expect = []
+    for im, s, r in zip(imgs, ss, sr):
+        e = im.copy()
+        gpu.Bilateral.apply(e, s, s, 0.0, r)
+        expect.append(e)
+    seen = []
+    for call in range(6):
+        dev = [torch.from_numpy(im.copy()).cuda() for im in imgs]
+        gpu.bilateral_batch(dev, ss, sr, graph=graph, autotune=True)
+        st = gpu.last_stats()
+        seen.append((round(st["load_factor"], 2), st["blur_pairs"]))
+        torch.cuda.synchronize()
+        for d, e in zip(dev, expect):
+            assert rel_err(d.cpu().numpy(), e) <= RTOL_FP32
+    assert seen[:4] == [(0.5, 1), (0.35, 1), (0.7, 1), (0.5, 0)]
+    assert seen[4] == seen[5] and seen[4] in seen[:4]
+
+
+@pytest.mark.gpu
+def test_autotuned_fp16_batch_keeps_blur_pairs(gpu):
+    """A 16-bit payload only tries fused blur pairs (one axis per pass would round its
+    rows to 16 bits between axes), and stays within its error bound."""
+    imgs, ss, sr = uneven_batch(9, seed=13, lo=128, hi=384)
+    ref = [im.copy() for im in imgs]
+    gpu.bilateral_batch(ref, ss, sr, payload="fp64")
+    seen = []
+    for call in range(5):
+        out = [im.copy() for im in imgs]
+        gpu.bilateral_batch(out, ss, sr, payload="fp16", autotune=True)
+        st = gpu.last_stats()
+        seen.append((round(st["load_factor"], 2), st["blur_pairs"]))
+        assert max(rel_err(o, r, floor_frac=1e-2) for o, r in zip(out, ref)) <= 1e-3
+    assert all(p == 1 for _, p in seen)
+    assert [l for l, _ in seen[:3]] == [0.5, 0.35, 0.7] and seen[3] == seen[4]
+
+
+@pytest.mark.gpu
 def test_batch_fp16_payload_error_vs_fp64(gpu):
     imgs, ss, sr = uneven_batch(12, seed=5, lo=128, hi=512)
     ref = [im.copy() for im in imgs]
