@@ -314,7 +314,7 @@ def mixed_batch(ib, synth, torch, dev, steps):
             "max_rel_err_fp16_vs_fp64": err}
 
 
-def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0):
+def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0, workers=4, max_batch=32):
     """BASELINE config 5: Poisson arrivals ramped rate0 -> rate1 req/s over `seconds`;
     half bilateral RGB (d=5), half joint bilateral of a grey image on a grey guide (d=3);
     sides log-uniform 64..2048, sigmas as the mixed batch; FP16 payload, 40 GB budget.
@@ -338,7 +338,7 @@ def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0):
         pool.append(dict(kind=ib.REQ_BILATERAL if kind == 0 else ib.REQ_JOINT_BILATERAL,
                          img=img, ref=ref, outs=outs, busy=[None] * 4,
                          ss=float(4 + 28 * rng.random()), sr=float(0.05 + 0.25 * rng.random())))
-    srv = ib.Server(workers=4, max_batch=32, payload="fp16", memory_budget=40 << 30)
+    srv = ib.Server(workers=workers, max_batch=max_batch, payload="fp16", memory_budget=40 << 30)
     # warm each worker's workspace on the pool
     tickets = []
     for q in pool:
@@ -381,7 +381,7 @@ def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0):
             "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
             "max_ms": round(st["max_ms"], 3), "throughput_mpix_s": round(st["mpix_per_s"], 2),
             "throughput_req_s": round(st["req_per_s"], 1), "batches": int(st["batches"]),
-            "payload": "fp16", "workers": 4, "memory_budget_gib": 40}
+            "payload": "fp16", "workers": workers, "max_batch": max_batch, "memory_budget_gib": 40}
 
 
 def run_ours(args):

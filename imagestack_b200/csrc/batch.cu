@@ -22,7 +22,7 @@ int Engine::ensure_hmeta(size_t bytes) {
     if (hmeta) cudaFreeHost(hmeta);
     hmeta = nullptr;
     hmeta_bytes = 0;
-    const size_t nb = bytes + bytes / 4 + 4096;
+    const size_t nb = std::max<size_t>(2 * bytes, 65536);
     if (cudaHostAlloc((void**)&hmeta, nb, cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
         return fail(PGPU_ERR_MEMORY, "pinned allocation of %zu bytes failed", nb);

@@ -43,14 +43,21 @@ bool get_stats(pgpu_stats* s) { if (t_have_stats) *s = t_stats; return t_have_st
 // ---------------------------------------------------------------------------------
 // buffers and engines
 // ---------------------------------------------------------------------------------
+static thread_local cudaStream_t t_call_stream = nullptr;
+void set_call_stream(cudaStream_t st) { t_call_stream = st; }
+cudaStream_t call_stream() { return t_call_stream; }
+
+// Every call is synchronous, so when a buffer grows (at the start of a call) no earlier
+// work still uses the old block, whichever stream it ran on.
 int DevBuf::ensure(size_t need) {
     if (need == 0) need = 16;
     if (need <= bytes) return PGPU_OK;
-    if (p) cudaFree(p);
+    const cudaStream_t st = t_call_stream;
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     bytes = 0;
-    const size_t nb = need + need / 8;
-    if (cudaMalloc(&p, nb) != cudaSuccess) {
+    const size_t nb = need + need / 2;
+    if (cudaMallocAsync(&p, nb, st) != cudaSuccess) {
         cudaGetLastError();
         p = nullptr;
         return fail(PGPU_ERR_MEMORY, "device allocation of %zu bytes failed", nb);
@@ -59,8 +66,10 @@ int DevBuf::ensure(size_t need) {
     return PGPU_OK;
 }
 
+// released when no work uses the buffer any more (calls are synchronous); the free is
+// queued on the legacy stream, which outlives every engine stream
 void DevBuf::release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, cudaStreamLegacy);
     p = nullptr;
     bytes = 0;
 }
@@ -401,6 +410,7 @@ struct ApiScope {
         }
         const bool device = opt && opt->memory == PGPU_MEM_DEVICE;
         st = (device && opt->stream) ? (cudaStream_t)opt->stream : E->stream;
+        set_call_stream(st);
         // Device memory without a stream belongs to the legacy default stream (stream 0,
         // torch's default): the engine's own stream does not synchronise with it, so it
         // waits here for the work queued there before the call, and stream 0 waits on exit
@@ -418,6 +428,7 @@ struct ApiScope {
     ~ApiScope() {
         if (joined && cudaEventRecord(E->join_ev[1], E->stream) == cudaSuccess)
             cudaStreamWaitEvent(cudaStreamLegacy, E->join_ev[1], 0);
+        set_call_stream(nullptr);
     }
     bool joined = false;
 };
@@ -495,6 +506,10 @@ int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int 
         (rc = E.ensure_copy_streams()))
         return rc;
     cudaStream_t cin = E.copy_in, cout = E.copy_out;
+    // the slots were allocated in order on the compute stream: the copy streams start after
+    CUDA_TRY(cudaEventRecord(E.join_ev[0], st));
+    CUDA_TRY(cudaStreamWaitEvent(cin, E.join_ev[0], 0));
+    CUDA_TRY(cudaStreamWaitEvent(cout, E.join_ev[0], 0));
     cudaEvent_t* uploaded = E.pipe_ev;
     cudaEvent_t* filtered = E.pipe_ev + 2;
     cudaEvent_t* downloaded = E.pipe_ev + 4;

@@ -29,7 +29,15 @@ bool get_stats(pgpu_stats* s);
                                 __FILE__, __LINE__);                                    \
     } while (0)
 
-// grow-only device allocation
+// The stream of the calling thread's current library call (the legacy default stream
+// outside one): workspace buffers are allocated and freed in order on it.
+void set_call_stream(cudaStream_t st);
+cudaStream_t call_stream();
+
+// Grow-only device buffer from the stream-ordered allocator: growing it frees the old
+// block and allocates the new one on the call's stream, which — unlike cudaMalloc and
+// cudaFree — does not synchronise the device, so engines on other streams (the server's
+// workers) are not stalled.  Buffers grow by half again each time.
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;

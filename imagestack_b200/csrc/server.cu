@@ -81,6 +81,7 @@ public:
     void worker(int w) {
         Engine& E = *engines[w];
         cudaSetDevice(cfg.device);
+        set_call_stream(E.stream);   // this worker's workspace lives on its stream
         std::vector<Req*> batch;
         for (;;) {
             size_t fp = 0;
