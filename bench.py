@@ -504,6 +504,17 @@ def run_ours(args):
         total_bytes = splat_bytes + blur_bytes + slice_bytes
         lattice_ms = statistics.mean(s["ms_total"] for s in stage)
         traffic = ncu_traffic().get("splat_dram_bytes")
+        # the splat's atomic roofline: one float4 RED per (point, remainder) against the
+        # measured RED rate at scattered rows of an L2-resident table (16 MB: the L2 atomic
+        # units' ceiling), and, for reference, of a table as large as the batch's
+        red_peak = ib.probe_red_rate(1 << 20)
+        red_table = ib.probe_red_rate(int(stage[-1]["capacity"]))
+        red_splat = N * (D + 1) / (splat_ms / 1e3)
+        atomics = {"kernel": "splat", "bound": "l2_atomics", "unit": "1e9 float4 RED/s",
+                   "achieved": round(red_splat / 1e9, 2), "peak": round(red_peak / 1e9, 2),
+                   "frac": round(red_splat / red_peak, 4),
+                   "uniform_random_rows_of_the_batch_table": round(red_table / 1e9, 2),
+                   "peak_kind": "measured by pgpu_probe_red_rate in this run (16 MB table)"}
         # the payload's error on the 4K frame against the FP64 lattice
         a = pristine[0].clone()
         ib.Bilateral.apply(a, SIGMA_S, SIGMA_S, 0.0, SIGMA_R, payload=args.payload)
@@ -542,6 +553,7 @@ def run_ours(args):
                          "frac": round(achieved / hbm, 4), "traffic": traffic,
                          "algorithmic_bytes": splat_bytes,
                          "note": "latency bound on L2 probes and atomics; see profiles/"},
+            "roofline_atomics": atomics,
             "roofline_pipeline": {"bytes": {"splat": splat_bytes, "blur": blur_bytes,
                                             "slice": slice_bytes},
                                   "ms": round(lattice_ms, 4),

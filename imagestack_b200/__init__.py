@@ -66,7 +66,8 @@ from .tmpfile import load_tmp, save_tmp  # noqa: E402,F401  (ImageStack .tmp fil
 
 EXPORTS = ["pgpu_default_options", "pgpu_last_error", "pgpu_version", "pgpu_device_count",
            "pgpu_gauss_transform", "pgpu_joint_bilateral", "pgpu_bilateral", "pgpu_last_stats",
-           "pgpu_lattice_dump", "pgpu_bilateral_batch", "pgpu_exact_gauss_transform_f64"]
+           "pgpu_lattice_dump", "pgpu_bilateral_batch", "pgpu_exact_gauss_transform_f64",
+           "pgpu_probe_red_rate"]
 
 _lib = None
 
@@ -94,6 +95,8 @@ def lib():
                                     C.c_void_p, C.c_void_p]
     L.pgpu_exact_gauss_transform_f64.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.pgpu_probe_red_rate.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_void_p,
+                                      C.POINTER(C.c_double)]
     _lib = L
     return L
 
@@ -125,6 +128,21 @@ def exact_gauss_transform_f64(queries, positions, values):
                                                 p.shape[0], p.data_ptr(), v.data_ptr(),
                                                 out.data_ptr(), stream))
     return out
+
+
+def probe_red_rate(rows: int, per_thread: int = 64, blocks: int | None = None) -> float:
+    """Float4 reductions per second this GPU retires at pseudo-random rows of a table of
+    `rows` x 16 bytes (the splat's atomic access); the splat's roofline for atomics."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    table = torch.zeros((rows, 4), dtype=torch.float32, device=dev)
+    if blocks is None:
+        blocks = 8 * torch.cuda.get_device_properties(dev).multi_processor_count
+    out = C.c_double(0.0)
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    _check(lib().pgpu_probe_red_rate(table.data_ptr(), rows, per_thread, blocks, stream,
+                                     C.byref(out)))
+    return out.value
 
 
 def last_stats() -> dict:

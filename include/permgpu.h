@@ -228,6 +228,13 @@ int pgpu_bilateral_noalloc(const float *d_in, float *d_out, int width, int heigh
 int pgpu_exact_gauss_transform_f64(int d, int vd, int nq, const float *q, int n,
                                    const float *p, const float *v, double *out, void *stream);
 
+/* Throughput probe (no counterpart in the reference): float4 reductions per second at
+ * pseudo-random rows of `table` (device memory, rows x 16 bytes, contents changed), from
+ * blocks x 256 threads adding per_thread rows each — the access the splat makes once per
+ * (point, remainder); its measured rate is the splat's atomic roofline. */
+int pgpu_probe_red_rate(void *table, long long rows, int per_thread, int blocks, void *stream,
+                        double *reds_per_second);
+
 #ifdef __cplusplus
 }
 #endif

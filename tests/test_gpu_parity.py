@@ -240,3 +240,18 @@ def test_exact_gauss_transform_f64_matches_oracle(gpu):
     err = rel_err(norm(lat), norm(cpu), floor_frac=1e-2)
     print("lattice vs exact Gauss transform, max relative error:", err)
     assert err < 0.5
+
+
+def test_red_probe_does_the_adds_it_times(gpu):
+    """The atomic-roofline probe: two launches (warm-up, timed) of blocks x 256 threads,
+    each adding a float4 of ones `per_thread` times at scattered rows."""
+    import ctypes as C
+
+    import torch
+    rows, per_thread, blocks = 1 << 16, 8, 64
+    table = torch.zeros((rows, 4), dtype=torch.float32, device="cuda")
+    rate = C.c_double(0.0)
+    rc = gpu.lib().pgpu_probe_red_rate(table.data_ptr(), rows, per_thread, blocks, None,
+                                      C.byref(rate))
+    assert rc == 0 and rate.value > 0
+    assert float(table.sum().item()) == 2 * blocks * 256 * per_thread * 4
