@@ -51,7 +51,8 @@ class Image(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("payload", C.c_int), ("memory", C.c_int), ("device", C.c_int),
-                ("stream", C.c_void_p), ("load_factor", C.c_float), ("flags", C.c_int)]
+                ("stream", C.c_void_p), ("load_factor", C.c_float), ("flags", C.c_int),
+                ("method", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -194,11 +195,17 @@ def _torch_stream(a):
     return C.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)
 
 
-def _method_ok(method: str):
-    if method != "permutohedral_gpu":
+METHODS = {"permutohedral_gpu": 0, "grid_gpu": 1}   # PGPU_METHOD_PERMUTOHEDRAL, _GRID
+
+
+def _method_ok(method: str) -> int:
+    """The library's method code for a method token: permutohedral_gpu (the lattice) or
+    grid_gpu (the bilateral grid); the reference's other methods stay on its CPU path."""
+    if method not in METHODS:
         raise PgpuError(ERR_UNSUPPORTED,
-                        "only the permutohedral_gpu method runs here; the reference's other "
+                        "methods here: permutohedral_gpu, grid_gpu; the reference's other "
                         "methods stay on its CPU path")
+    return METHODS[method]
 
 
 class GaussTransform:
@@ -207,7 +214,7 @@ class GaussTransform:
     @staticmethod
     def apply(slice_positions, splat_positions, values, sigmas, method: str = "permutohedral_gpu",
               payload: str = "fp32", load_factor: float = 0.5):
-        _method_ok(method)
+        mcode = _method_ok(method)
         same = slice_positions is None or slice_positions is splat_positions
         sp, mem = _view(splat_positions, "splat")
         va, mem2 = _view(values, "values")
@@ -226,6 +233,7 @@ class GaussTransform:
         stream = _torch_stream(splat_positions) if mem == MEM_DEVICE else None
         opt = _options(mem, payload, stream=stream, load_factor=load_factor,
                        device=(splat_positions.device.index or 0) if mem == MEM_DEVICE else 0)
+        opt.method = mcode
         _check(lib().pgpu_gauss_transform(None if same else C.byref(sl), C.byref(sp), C.byref(va),
                                           sig, len(sigmas), C.byref(ov), C.byref(opt)))
         return out
@@ -238,7 +246,7 @@ class JointBilateral:
     def apply(image, reference, filter_width: float, filter_height: float, filter_frames: float,
               color_sigma: float, method: str = "permutohedral_gpu", payload: str = "fp32",
               load_factor: float = 0.5):
-        _method_ok(method)
+        mcode = _method_ok(method)
         im, mem = _view(image, "image")
         ref, mem2 = _view(reference, "reference")
         if mem != mem2:
@@ -246,6 +254,7 @@ class JointBilateral:
         stream = _torch_stream(image) if mem == MEM_DEVICE else None
         opt = _options(mem, payload, stream=stream, load_factor=load_factor,
                        device=(image.device.index or 0) if mem == MEM_DEVICE else 0)
+        opt.method = mcode
         _check(lib().pgpu_joint_bilateral(C.byref(im), C.byref(ref), filter_width, filter_height,
                                           filter_frames, color_sigma, C.byref(opt)))
         return image
@@ -258,11 +267,12 @@ class Bilateral:
     def apply(image, filter_width: float, filter_height: float, filter_frames: float,
               color_sigma: float, method: str = "permutohedral_gpu", payload: str = "fp32",
               load_factor: float = 0.5):
-        _method_ok(method)
+        mcode = _method_ok(method)
         im, mem = _view(image, "image")
         stream = _torch_stream(image) if mem == MEM_DEVICE else None
         opt = _options(mem, payload, stream=stream, load_factor=load_factor,
                        device=(image.device.index or 0) if mem == MEM_DEVICE else 0)
+        opt.method = mcode
         _check(lib().pgpu_bilateral(C.byref(im), filter_width, filter_height, filter_frames,
                                     color_sigma, C.byref(opt)))
         return image

@@ -151,6 +151,11 @@ int vdp_for(int vd) { return vd <= 2 ? 2 : vd <= 4 ? 4 : vd <= 8 ? 8 : 0; }
 // one lattice: splat, compact, neighbours, blur, slice
 // ---------------------------------------------------------------------------------
 int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st) {
+    if (J.method == PGPU_METHOD_GRID) {
+        if (J.rec_vtx || J.dump_splat) return fail(PGPU_ERR_UNSUPPORTED, "the grid method has no lattice dumps");
+        return run_grid(E, J, st);
+    }
+    if (J.method != PGPU_METHOD_PERMUTOHEDRAL) return fail(PGPU_ERR_ARGUMENT, "unknown method %d", J.method);
     BatchJob B;
     B.d = J.d;
     B.vd = J.vd;
@@ -255,7 +260,8 @@ OutView outview(const pgpu_image& v, int channels, int normalize) {
 // ---------------------------------------------------------------------------------
 int gauss_transform_device(Engine& E, const pgpu_image* slice, const pgpu_image& splat,
                            const pgpu_image& values, const float* sigmas, int n_sigmas,
-                           const pgpu_image& out, int payload, float load, cudaStream_t st) {
+                           const pgpu_image& out, int payload, float load, cudaStream_t st,
+                           int method) {
     if (splat.width != values.width || splat.height != values.height || splat.frames != values.frames)
         return fail(PGPU_ERR_ARGUMENT, "Weights and locations of the Gaussians must be the same size");
     const bool replay = !slice || same_view(*slice, splat);
@@ -299,6 +305,7 @@ int gauss_transform_device(Engine& E, const pgpu_image* slice, const pgpu_image&
         J.n_slice = (uint32_t)((size_t)sl.width * sl.height * sl.frames);
     }
     J.out = outview(out, values.channels, 0);
+    J.method = method;
     return run_lattice(E, J, st);
 }
 
@@ -315,7 +322,8 @@ static pgpu_image region(const pgpu_image& v, int x, int y, int t, int w, int h,
 }
 
 int joint_bilateral_device(Engine& E, const pgpu_image& im, const pgpu_image& ref, float fw,
-                           float fh, float ft, float cs, int payload, float load, cudaStream_t st) {
+                           float fh, float ft, float cs, int payload, float load, cudaStream_t st,
+                           int method) {
     if (im.width != ref.width || im.height != ref.height || im.frames != ref.frames)
         return fail(PGPU_ERR_ARGUMENT, "Image and reference must be the same size");
     if (im.width == 1) fw = 0;
@@ -325,7 +333,7 @@ int joint_bilateral_device(Engine& E, const pgpu_image& im, const pgpu_image& re
         for (int x = 0; x < im.width; x++) {
             int rc = joint_bilateral_device(E, region(im, x, 0, 0, 1, im.height, im.frames),
                                             region(ref, x, 0, 0, 1, ref.height, ref.frames), 0, fh,
-                                            ft, cs, payload, load, st);
+                                            ft, cs, payload, load, st, method);
             if (rc) return rc;
         }
         return PGPU_OK;
@@ -334,7 +342,7 @@ int joint_bilateral_device(Engine& E, const pgpu_image& im, const pgpu_image& re
         for (int y = 0; y < im.height; y++) {
             int rc = joint_bilateral_device(E, region(im, 0, y, 0, im.width, 1, im.frames),
                                             region(ref, 0, y, 0, ref.width, 1, ref.frames), fw, 0,
-                                            ft, cs, payload, load, st);
+                                            ft, cs, payload, load, st, method);
             if (rc) return rc;
         }
         return PGPU_OK;
@@ -343,7 +351,7 @@ int joint_bilateral_device(Engine& E, const pgpu_image& im, const pgpu_image& re
         for (int t = 0; t < im.frames; t++) {
             int rc = joint_bilateral_device(E, region(im, 0, 0, t, im.width, im.height, 1),
                                             region(ref, 0, 0, t, ref.width, ref.height, 1), fw, fh,
-                                            0, cs, payload, load, st);
+                                            0, cs, payload, load, st, method);
             if (rc) return rc;
         }
         return PGPU_OK;
@@ -381,6 +389,7 @@ int joint_bilateral_device(Engine& E, const pgpu_image& im, const pgpu_image& re
     J.homog = true;
     J.replay = true;
     J.out = outview(im, im.channels, 1);
+    J.method = method;
     return run_lattice(E, J, st);
 }
 
@@ -585,6 +594,7 @@ void pgpu_default_options(pgpu_options* opt) {
     opt->device = 0;
     opt->stream = nullptr;
     opt->load_factor = 0.5f;
+    opt->method = PGPU_METHOD_PERMUTOHEDRAL;
 }
 
 const char* pgpu_last_error(void) { return last_error(); }
@@ -610,7 +620,7 @@ int pgpu_gauss_transform(const pgpu_image* slice, const pgpu_image* splat, const
     Engine& E = *S.E;
     if (opt.memory == PGPU_MEM_DEVICE) {
         int rc = gauss_transform_device(E, slice, *splat, *values, sigmas, n_sigmas, *out,
-                                        opt.payload, opt.load_factor, S.st);
+                                        opt.payload, opt.load_factor, S.st, opt.method);
         return rc;
     }
     const bool replay = !slice || same_view(*slice, *splat);
@@ -624,7 +634,7 @@ int pgpu_gauss_transform(const pgpu_image* slice, const pgpu_image* splat, const
         return rc;
     dout = dense_like(sl, (float*)E.img_d.p, values->channels);
     rc = gauss_transform_device(E, replay ? nullptr : &dslice, dsplat, dvals, sigmas, n_sigmas, dout,
-                                opt.payload, opt.load_factor, S.st);
+                                opt.payload, opt.load_factor, S.st, opt.method);
     if (rc) return rc;
     if ((rc = download(dout, *out, values->channels, S.st))) return rc;
     CUDA_TRY(cudaStreamSynchronize(S.st));
@@ -641,7 +651,7 @@ int pgpu_joint_bilateral(pgpu_image* im, const pgpu_image* ref, float filter_wid
     Engine& E = *S.E;
     if (opt.memory == PGPU_MEM_DEVICE)
         return joint_bilateral_device(E, *im, *ref, filter_width, filter_height, filter_frames,
-                                      color_sigma, opt.payload, opt.load_factor, S.st);
+                                      color_sigma, opt.payload, opt.load_factor, S.st, opt.method);
     const bool same = same_view(*im, *ref);
     pgpu_image dim, dref;
     int rc;
@@ -649,7 +659,7 @@ int pgpu_joint_bilateral(pgpu_image* im, const pgpu_image* ref, float filter_wid
     if (same) dref = dim;
     else if ((rc = upload(E, E.img_b, *ref, &dref, S.st))) return rc;
     rc = joint_bilateral_device(E, dim, dref, filter_width, filter_height, filter_frames, color_sigma,
-                                opt.payload, opt.load_factor, S.st);
+                                opt.payload, opt.load_factor, S.st, opt.method);
     if (rc) return rc;
     if ((rc = download(dim, *im, im->channels, S.st))) return rc;
     CUDA_TRY(cudaStreamSynchronize(S.st));

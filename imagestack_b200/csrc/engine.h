@@ -61,6 +61,7 @@ struct Engine {
     DevBuf vtx2slot;   // slot of each vertex
     DevBuf sval;       // filtered rows in slot space, arithmetic type, read by the slice
     DevBuf rec;        // slot of every (point, remainder), [r][n], recorded by the splat
+    DevBuf grid;       // the dense grid of the grid method
     DevBuf dstat;
     // batch metadata: statuses, counts, segment tables (device copy of hmeta)
     DevBuf meta;
@@ -151,11 +152,14 @@ struct LatticeJob {
     size_t dump_bytes = 0;
     uint32_t* vertices_out = nullptr;
     bool homog = false;   // the last value channel is the homogeneous weight
+    int method = PGPU_METHOD_PERMUTOHEDRAL;   // or PGPU_METHOD_GRID (grid.cu)
 };
 
 LatticeConsts make_consts(int d);
 int vdp_for(int vd);
 int run_lattice(Engine& E, const LatticeJob& J, cudaStream_t st);
+// the bilateral grid (GaussTransform::apply's GRID branch) over the same job description
+int run_grid(Engine& E, const LatticeJob& J, cudaStream_t st);
 
 inline float half_bits_to_float(uint16_t h) {
     const uint32_t sign = (uint32_t)(h >> 15) << 31;

@@ -1,0 +1,310 @@
+// The bilateral grid on the GPU: the GRID branch of GaussTransform::apply
+// (src/GaussTransform.cpp:227-290), which JointBilateral::apply picks by default for at
+// most four position channels (:553-564), with the reference's DenseGrid
+// (src/DenseGrid.h): a dense grid over the positions' bounding box, multilinear splatting
+// into the 2^d corners of each point's cell, two [1 2 1]/4 passes per dimension (taps 5),
+// and multilinear slicing.
+//
+//   preview  min and max of every scaled position coordinate (block reduction, then
+//            order-preserving integer atomics: exact in any order)
+//   splat    one thread per point; FP32 atomics into the corners (the reference adds in
+//            point order, so sums agree to rounding)
+//   blur     one launch per dimension; one thread per grid row and value channel runs the
+//            reference's in-place recurrence (src/DenseGrid.h:199-236) with its exact
+//            arithmetic, including the last cell's double-precision step
+//   slice    one thread per point; the corners gathered in the reference's order
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "engine.h"
+
+namespace pgpu {
+namespace {
+
+constexpr int kGridTaps = 5;        // GaussTransform::apply builds DenseGrid(d, vd, 5)
+constexpr int kGridMaxD = 5;        // 2^d corners per point; the reference's AUTO uses d <= 4
+constexpr int kGridMaxVd = 8;
+constexpr int kGridThreads = 256;
+constexpr long long kGridMaxCells = 1LL << 30;   // floats in the grid
+
+struct GridArgs {
+    int vd;
+    float sf;                            // scaleFactor, the same in every dimension
+    float minp[kGridMaxD];               // minPosition
+    int sizes[kGridMaxD];
+    long long stride[kGridMaxD + 1];     // stride[0] = vd
+    float* grid;
+};
+
+// float <-> unsigned mapping that preserves order, for min/max by integer atomics
+__device__ __forceinline__ unsigned ordered_bits(float f) {
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+float unordered_float(unsigned u) {
+    const unsigned b = (u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u;
+    float f;
+    memcpy(&f, &b, 4);
+    return f;
+}
+
+// DenseGrid::preview (src/DenseGrid.h:142-160): the bounding box of position * scaleFactor
+template <int D>
+__global__ void __launch_bounds__(kGridThreads) grid_minmax_kernel(PointSource src, uint32_t n, float sf,
+                                                                   unsigned* mm) {
+    __shared__ unsigned smin[D], smax[D];
+    if (threadIdx.x < D) {
+        smin[threadIdx.x] = 0xFFFFFFFFu;
+        smax[threadIdx.x] = 0u;
+    }
+    __syncthreads();
+    unsigned lo[D], hi[D];
+#pragma unroll
+    for (int c = 0; c < D; ++c) lo[c] = 0xFFFFFFFFu, hi[c] = 0u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float p[D];
+        load_position<D>(src, i, p);
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            const unsigned o = ordered_bits(__fmul_rn(p[c], sf));
+            lo[c] = min(lo[c], o);
+            hi[c] = max(hi[c], o);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[c] = min(lo[c], __shfl_xor_sync(0xFFFFFFFFu, lo[c], o));
+            hi[c] = max(hi[c], __shfl_xor_sync(0xFFFFFFFFu, hi[c], o));
+        }
+        if ((threadIdx.x & 31u) == 0) {
+            atomicMin(&smin[c], lo[c]);
+            atomicMax(&smax[c], hi[c]);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < D) {
+        atomicMin(&mm[threadIdx.x], smin[threadIdx.x]);
+        atomicMax(&mm[D + threadIdx.x], smax[threadIdx.x]);
+    }
+}
+
+// DenseGrid::query (src/DenseGrid.h:240-285): integral cell and fractions of one point
+template <int D>
+__device__ __forceinline__ void grid_cell(const GridArgs& g, const float (&p)[D], int (&I)[D], float (&F)[D],
+                                          float (&Fi)[D]) {
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+        const float f = __fsub_rn(__fmul_rn(p[c], g.sf), g.minp[c]);
+        I[c] = (int)(short)floorf(f);
+        F[c] = __fsub_rn(f, (float)I[c]);
+        Fi[c] = __fsub_rn(1.0f, F[c]);
+    }
+}
+
+// Corner `corner` of the cell: its weight (the reference's product order) and offset; a
+// corner past the grid's last cell has weight exactly 0 (the point lies on the last
+// plane), and is skipped.
+template <int D>
+__device__ __forceinline__ bool grid_corner(const GridArgs& g, const int (&I)[D], const float (&F)[D],
+                                            const float (&Fi)[D], int corner, float& w, long long& off) {
+    w = 1.0f;
+    off = 0;
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        const int ij = I[j] + ((corner >> j) & 1);
+        ok = ok && ij >= 0 && ij < g.sizes[j];
+        off += (long long)ij * g.stride[j];
+        w = __fmul_rn(w, ((corner >> j) & 1) ? F[j] : Fi[j]);
+    }
+    return ok;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kGridThreads) grid_splat_kernel(PointSource src, uint32_t n, GridArgs g) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float p[D], v[kGridMaxVd];
+    load_point<D, kGridMaxVd>(src, i, p, v);
+    int I[D];
+    float F[D], Fi[D];
+    grid_cell<D>(g, p, I, F, Fi);
+    for (int corner = 0; corner < (1 << D); ++corner) {
+        float w;
+        long long off;
+        if (!grid_corner<D>(g, I, F, Fi, corner, w, off)) continue;
+#pragma unroll
+        for (int k = 0; k < kGridMaxVd; ++k)
+            if (k < g.vd) atomicAdd(g.grid + off + k, __fmul_rn(w, v[k]));
+    }
+}
+
+// DenseGrid::blur_ (src/DenseGrid.h:186-238) along dimension j: rows x vd threads, each
+// running taps/2 in-place [1 2 1]/4 passes over its row with zero boundaries.
+__global__ void __launch_bounds__(kGridThreads) grid_blur_kernel(GridArgs g, int d, int j, long long rows) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= rows * g.vd) return;
+    const int k = (int)(t % g.vd);
+    long long rem = t / g.vd, start = k;
+    for (int i = 0; i < d; ++i) {
+        if (i == j) continue;
+        start += (rem % g.sizes[i]) * g.stride[i];
+        rem /= g.sizes[i];
+    }
+    float* row = g.grid + start;
+    const long long s = g.stride[j];
+    const int len = g.sizes[j];
+    for (int it = 0; it < kGridTaps / 2; ++it) {
+        float t1 = __fdiv_rn(row[0], 2.0f);                            // rowPtr[k]/2
+        for (int x = 0; x < len - 1; ++x) {
+            const float t2 = __fmul_rn(0.5f, __fadd_rn(row[x * s], row[(x + 1) * s]));
+            row[x * s] = __fmul_rn(0.5f, __fadd_rn(t1, t2));
+            t1 = t2;
+        }
+        // the last cell: 0.5*(tmp1 + 0.5*rowPtr[k]) evaluates in double (double literals)
+        const long long last = (long long)(len - 1) * s;
+        row[last] = (float)__dmul_rn(0.5, __dadd_rn((double)t1, __dmul_rn(0.5, (double)row[last])));
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(kGridThreads) grid_slice_kernel(PointSource src, uint32_t n, GridArgs g,
+                                                                  OutView out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float p[D];
+    load_position<D>(src, i, p);
+    int I[D];
+    float F[D], Fi[D];
+    grid_cell<D>(g, p, I, F, Fi);
+    float acc[kGridMaxVd];
+#pragma unroll
+    for (int k = 0; k < kGridMaxVd; ++k) acc[k] = 0.0f;
+    for (int corner = 0; corner < (1 << D); ++corner) {
+        float w;
+        long long off;
+        if (!grid_corner<D>(g, I, F, Fi, corner, w, off)) continue;
+#pragma unroll
+        for (int k = 0; k < kGridMaxVd; ++k)
+            if (k < g.vd) acc[k] = __fadd_rn(acc[k], __fmul_rn(w, g.grid[off + k]));
+    }
+    const uint32_t wdt = (uint32_t)src.width, hgt = (uint32_t)src.height;
+    const uint32_t x = i % wdt, q = i / wdt, y = q % hgt, t = q / hgt;
+    float* o = out.base + (long long)t * out.tstride + (long long)y * out.ystride + x;
+    float wsum = acc[0];
+#pragma unroll
+    for (int k = 0; k < kGridMaxVd; ++k) if (k == g.vd - 1) wsum = acc[k];
+#pragma unroll
+    for (int k = 0; k < kGridMaxVd; ++k)
+        if (k < out.channels) o[(long long)k * out.cstride] = out.normalize ? acc[k] / wsum : acc[k];
+}
+
+template <int D>
+void launch_minmax(const PointSource& s, uint32_t n, float sf, unsigned* mm, int sms, cudaStream_t st) {
+    uint64_t blocks = (n + kGridThreads - 1) / kGridThreads;
+    if (blocks > (uint64_t)sms * 8) blocks = (uint64_t)sms * 8;
+    if (blocks < 1) blocks = 1;
+    grid_minmax_kernel<D><<<(unsigned)blocks, kGridThreads, 0, st>>>(s, n, sf, mm);
+}
+template <int D>
+void launch_splat(const PointSource& s, uint32_t n, const GridArgs& g, cudaStream_t st) {
+    if (n) grid_splat_kernel<D><<<(n + kGridThreads - 1) / kGridThreads, kGridThreads, 0, st>>>(s, n, g);
+}
+template <int D>
+void launch_slice(const PointSource& s, uint32_t n, const GridArgs& g, const OutView& o, cudaStream_t st) {
+    if (n) grid_slice_kernel<D><<<(n + kGridThreads - 1) / kGridThreads, kGridThreads, 0, st>>>(s, n, g, o);
+}
+
+#define PGPU_GRID_DISPATCH(d, call)          \
+    switch (d) {                             \
+    case 1: { constexpr int DD = 1; call; } break; \
+    case 2: { constexpr int DD = 2; call; } break; \
+    case 3: { constexpr int DD = 3; call; } break; \
+    case 4: { constexpr int DD = 4; call; } break; \
+    case 5: { constexpr int DD = 5; call; } break; \
+    }
+
+}  // namespace
+
+int run_grid(Engine& E, const LatticeJob& J, cudaStream_t st) {
+    const int d = J.d, vd = J.vd;
+    if (d < 1 || d > kGridMaxD)
+        return fail(PGPU_ERR_UNSUPPORTED, "the grid method takes 1..%d position dimensions (got %d)",
+                    kGridMaxD, d);
+    if (vd < 1 || vd > kGridMaxVd) return fail(PGPU_ERR_UNSUPPORTED, "%d value channels", vd);
+    if (J.payload != kPayloadF32) return fail(PGPU_ERR_UNSUPPORTED, "the grid method computes in FP32 only");
+    // DenseGrid's constructor (src/DenseGrid.h:111-127): sqrtf(1.0/3 + (taps-1)*0.25)
+    const float sf = sqrtf((float)(1.0 / 3 + (kGridTaps - 1) * 0.25));
+    const PointSource& sl = J.replay ? J.splat : J.slice;
+    const uint32_t nsl = J.replay ? J.n : J.n_slice;
+    int rc;
+    if ((rc = E.meta.ensure(64))) return rc;
+    unsigned* mm = (unsigned*)E.meta.p;
+    CUDA_TRY(cudaEventRecord(E.ev[0], st));
+    CUDA_TRY(cudaMemsetAsync(mm, 0xFF, sizeof(unsigned) * d, st));
+    CUDA_TRY(cudaMemsetAsync(mm + d, 0, sizeof(unsigned) * d, st));
+    PGPU_GRID_DISPATCH(d, launch_minmax<DD>(J.splat, J.n, sf, mm, E.sms, st));
+    if (!J.replay) PGPU_GRID_DISPATCH(d, launch_minmax<DD>(sl, nsl, sf, mm, E.sms, st));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(E.hstat, mm, sizeof(unsigned) * 2 * d, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+
+    GridArgs g;
+    memset(&g, 0, sizeof(g));
+    g.vd = vd;
+    g.sf = sf;
+    g.stride[0] = vd;
+    for (int i = 0; i < d; ++i) {
+        const float lo = unordered_float(E.hstat[i]), hi = unordered_float(E.hstat[d + i]);
+        if (!std::isfinite(lo) || !std::isfinite(hi))
+            return fail(PGPU_ERR_ARGUMENT, "positions are not finite");
+        g.minp[i] = lo;
+        const float span = hi - lo;   // float subtraction, as maxPosition[i] - minPosition[i]
+        g.sizes[i] = (int)(std::ceil(span) + 1);
+        g.stride[i + 1] = g.stride[i] * g.sizes[i];
+        if (g.sizes[i] < 1 || g.stride[i + 1] > kGridMaxCells)
+            return fail(PGPU_ERR_CAPACITY, "the grid would need more than %lld cells", kGridMaxCells);
+    }
+    const long long cells = g.stride[d];
+    if ((rc = E.grid.ensure((size_t)cells * sizeof(float)))) return rc;
+    g.grid = (float*)E.grid.p;
+    CUDA_TRY(cudaMemsetAsync(g.grid, 0, (size_t)cells * sizeof(float), st));
+    CUDA_TRY(cudaEventRecord(E.ev[1], st));
+    PGPU_GRID_DISPATCH(d, launch_splat<DD>(J.splat, J.n, g, st));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(E.ev[3], st));
+    for (int j = 0; j < d; ++j) {
+        const long long rows = cells / ((long long)vd * g.sizes[j]);
+        const long long threads = rows * vd;
+        grid_blur_kernel<<<(unsigned)((threads + kGridThreads - 1) / kGridThreads), kGridThreads, 0, st>>>(
+            g, d, j, rows);
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(E.ev[4], st));
+    PGPU_GRID_DISPATCH(d, launch_slice<DD>(sl, nsl, g, J.out, st));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(E.ev[5], st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+
+    pgpu_stats s;
+    memset(&s, 0, sizeof(s));
+    s.points = J.n;
+    s.vertices = cells / vd;        // grid cells
+    s.capacity = cells / vd;
+    s.d = d;
+    s.vd = vd;
+    s.payload = J.payload;
+    cudaEventElapsedTime(&s.ms_splat, E.ev[1], E.ev[3]);
+    cudaEventElapsedTime(&s.ms_compact, E.ev[0], E.ev[1]);   // the bounding-box preview
+    cudaEventElapsedTime(&s.ms_blur, E.ev[3], E.ev[4]);
+    cudaEventElapsedTime(&s.ms_slice, E.ev[4], E.ev[5]);
+    cudaEventElapsedTime(&s.ms_total, E.ev[0], E.ev[5]);
+    set_stats(s);
+    return PGPU_OK;
+}
+
+}  // namespace pgpu

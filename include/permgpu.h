@@ -57,8 +57,16 @@ typedef struct pgpu_options {
     int device;         /* CUDA device ordinal */
     void *stream;       /* cudaStream_t for PGPU_MEM_DEVICE calls; NULL: library stream */
     float load_factor;  /* hash-table target load in (0, 0.9]; 0: default 0.5 */
-    int flags;          /* reserved, 0 */
+    int flags;          /* PGPU_FLAG_* (pgpu_bilateral_batch), else 0 */
+    int method;         /* PGPU_METHOD_PERMUTOHEDRAL (default) or PGPU_METHOD_GRID */
 } pgpu_options;
+
+/* PGPU_METHOD_GRID: the bilateral grid, GaussTransform::apply's GRID branch
+ * (src/GaussTransform.cpp:227-290, src/DenseGrid.h: multilinear splat and slice, two
+ * [1 2 1]/4 passes per dimension), for gauss_transform and joint_bilateral/bilateral;
+ * 1..5 position dimensions, FP32 only. */
+#define PGPU_METHOD_PERMUTOHEDRAL 0
+#define PGPU_METHOD_GRID 1
 
 typedef struct pgpu_stats {
     long long points;      /* splatted points */
