@@ -1,5 +1,5 @@
-// ImageStack plugin: the `permutohedral_gpu` method for -gausstransform, -jointbilateral
-// and -bilateral.
+// ImageStack plugin: the `permutohedral_gpu` (lattice) and `grid_gpu` (bilateral grid)
+// methods for -gausstransform, -jointbilateral and -bilateral.
 //
 //     ImageStack -plugin libpermgpu_imagestack.so -load im.tmp \
 //                -bilateral 0.1 16 16 0 permutohedral_gpu -save out.tmp
@@ -27,7 +27,12 @@ using namespace ImageStack;
 
 namespace {
 
-const char* kMethod = "permutohedral_gpu";
+// method tokens: the permutohedral lattice and the bilateral grid on the GPU
+int method_code(const string& tok) {
+    if (tok == "permutohedral_gpu") return PGPU_METHOD_PERMUTOHEDRAL;
+    if (tok == "grid_gpu") return PGPU_METHOD_GRID;
+    return -1;
+}
 
 pgpu_image view_of(const Image& im) {
     pgpu_image v;
@@ -42,20 +47,23 @@ pgpu_image view_of(const Image& im) {
     return v;
 }
 
-void check(int rc) {
-    if (rc != PGPU_OK) panic("permutohedral_gpu: %s\n", pgpu_last_error());
+void check(int rc, int method) {
+    if (rc != PGPU_OK)
+        panic("%s: %s\n", method == PGPU_METHOD_GRID ? "grid_gpu" : "permutohedral_gpu", pgpu_last_error());
 }
 
-pgpu_options host_options() {
+pgpu_options host_options(int method) {
     pgpu_options o;
     pgpu_default_options(&o);
     o.memory = PGPU_MEM_HOST;
+    o.method = method;
     return o;
 }
 
 // GaussTransform::apply for the GPU method: a new un-normalised image with the slice
 // positions' size and the values' channels (src/GaussTransform.cpp:194).
-Image gauss_transform_gpu(Image slice, Image splat, Image values, const vector<float>& sigmas) {
+Image gauss_transform_gpu(Image slice, Image splat, Image values, const vector<float>& sigmas,
+                          int method = PGPU_METHOD_PERMUTOHEDRAL) {
     assert(splat.width == values.width && splat.height == values.height &&
                splat.frames == values.frames,
            "Weights and locations of the Gaussians must be the same size\n");
@@ -64,16 +72,17 @@ Image gauss_transform_gpu(Image slice, Image splat, Image values, const vector<f
            " the same number of channels.\n");
     Image out(slice.width, slice.height, slice.frames, values.channels);
     pgpu_image s = view_of(slice), p = view_of(splat), v = view_of(values), o = view_of(out);
-    const pgpu_options opt = host_options();
+    const pgpu_options opt = host_options(method);
     check(pgpu_gauss_transform(slice == splat ? nullptr : &s, &p, &v, sigmas.data(),
-                               (int)sigmas.size(), &o, &opt));
+                               (int)sigmas.size(), &o, &opt), method);
     return out;
 }
 
-void joint_bilateral_gpu(Image im, Image ref, float fw, float fh, float ft, float cs) {
+void joint_bilateral_gpu(Image im, Image ref, float fw, float fh, float ft, float cs,
+                         int method = PGPU_METHOD_PERMUTOHEDRAL) {
     pgpu_image a = view_of(im), b = view_of(ref);
-    const pgpu_options opt = host_options();
-    check(pgpu_joint_bilateral(&a, &b, fw, fh, ft, cs, &opt));
+    const pgpu_options opt = host_options(method);
+    check(pgpu_joint_bilateral(&a, &b, fw, fh, ft, cs, &opt), method);
 }
 
 class GpuGaussTransform : public GaussTransform {
@@ -81,7 +90,8 @@ public:
     void help() {
         GaussTransform::help();
         pprintf("With -plugin libpermgpu_imagestack.so the method may also be"
-                " permutohedral_gpu: the permutohedral lattice on a B200 GPU.\n");
+                " permutohedral_gpu (the permutohedral lattice) or grid_gpu (the bilateral"
+                " grid), on a B200 GPU.\n");
     }
 
     bool test() {
@@ -102,7 +112,8 @@ public:
     }
 
     void parse(vector<string> args) {
-        if (args.empty() || args[0] != kMethod) {
+        const int method = args.empty() ? -1 : method_code(args[0]);
+        if (method < 0) {
             GaussTransform::parse(args);
             return;
         }
@@ -117,7 +128,7 @@ public:
             panic("-gausstransform takes one argument, two arguments, or one plus the"
                   " number of channels in the second image on the stack arguments\n");
         }
-        Image im = gauss_transform_gpu(stack(0), stack(1), stack(2), sigmas);
+        Image im = gauss_transform_gpu(stack(0), stack(1), stack(2), sigmas, method);
         pop();
         push(im);
     }
@@ -125,8 +136,8 @@ public:
 
 // shared argument grammar of -jointbilateral and -bilateral (src/GaussTransform.cpp:473-499)
 bool parse_bilateral_args(const vector<string>& args, const char* name, float* cs, float* fw,
-                          float* fh, float* ft) {
-    if (args.size() != 5 || args[4] != kMethod) return false;
+                          float* fh, float* ft, int* method) {
+    if (args.size() != 5 || (*method = method_code(args[4])) < 0) return false;
     *cs = readFloat(args[0]);
     *fw = *fh = readFloat(args[1]);
     *fh = readFloat(args[2]);
@@ -140,7 +151,7 @@ public:
     void help() {
         JointBilateral::help();
         pprintf("With -plugin libpermgpu_imagestack.so the method may also be"
-                " permutohedral_gpu.\n");
+                " permutohedral_gpu or grid_gpu.\n");
     }
 
     bool test() {
@@ -156,11 +167,12 @@ public:
 
     void parse(vector<string> args) {
         float cs, fw, fh, ft;
-        if (!parse_bilateral_args(args, "-jointbilateral", &cs, &fw, &fh, &ft)) {
+        int method;
+        if (!parse_bilateral_args(args, "-jointbilateral", &cs, &fw, &fh, &ft, &method)) {
             JointBilateral::parse(args);
             return;
         }
-        joint_bilateral_gpu(stack(0), stack(1), fw, fh, ft, cs);
+        joint_bilateral_gpu(stack(0), stack(1), fw, fh, ft, cs, method);
     }
 };
 
@@ -169,7 +181,7 @@ public:
     void help() {
         Bilateral::help();
         pprintf("With -plugin libpermgpu_imagestack.so the method may also be"
-                " permutohedral_gpu.\n");
+                " permutohedral_gpu or grid_gpu.\n");
     }
 
     bool test() {
@@ -183,12 +195,13 @@ public:
 
     void parse(vector<string> args) {
         float cs, fw, fh, ft;
-        if (!parse_bilateral_args(args, "-bilateral", &cs, &fw, &fh, &ft)) {
+        int method;
+        if (!parse_bilateral_args(args, "-bilateral", &cs, &fw, &fh, &ft, &method)) {
             Bilateral::parse(args);
             return;
         }
         Image im = stack(0);
-        joint_bilateral_gpu(im, im, fw, fh, ft, cs);
+        joint_bilateral_gpu(im, im, fw, fh, ft, cs, method);
     }
 };
 

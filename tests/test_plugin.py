@@ -124,3 +124,16 @@ def test_cli_jointbilateral_and_gausstransform_gpu_match_cpu(tmp_path):
 def test_cli_operation_self_tests_pass_with_plugin(tmp_path):
     out = run_cli(["-test", "gausstransform", "jointbilateral", "bilateral"], tmp_path)
     assert out.count("Passed") >= 3 and "Failed" not in out, out[-2000:]
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_cli_grid_gpu_matches_cli_grid(tmp_path):
+    """-bilateral ... grid_gpu against the reference CLI's own grid method (a grey image:
+    three position channels, where JointBilateral's AUTO picks the grid)."""
+    img = synth.luminance(synth.image(240, 160, 3, rects=8, seed=7))
+    save_tmp(tmp_path / "in.tmp", img)
+    for m in ("grid", "grid_gpu"):
+        run_cli(["-load", "in.tmp", "-bilateral", "0.1", "8", "8", "0", m, "-save", "g_%s.tmp" % m],
+                tmp_path)
+    assert rel_err(load_tmp(tmp_path / "g_grid_gpu.tmp"), load_tmp(tmp_path / "g_grid.tmp")) <= 1e-5
