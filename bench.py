@@ -264,6 +264,26 @@ def exact_error(ib, torch, frame, filtered, samples=4096, seed=7):
             "oracle": "FP64 brute force over all %d pixels on the GPU (%.2f s)" % (h * w, secs)}
 
 
+def grey_4k(ib, synth, torch, frame, steps=10):
+    """The 4K config's grey variant: joint bilateral of the frame's luminance with itself
+    (d=3: luminance/0.1, x/16, y/16), by the permutohedral lattice and by the bilateral
+    grid (the method JointBilateral::apply's AUTO picks for three position channels)."""
+    lum = (0.299 * frame[0] + 0.587 * frame[1] + 0.114 * frame[2])[None].contiguous()
+    work = torch.empty_like(lum)
+    stream = torch.cuda.current_stream(lum.device)
+    out = {}
+    for method in ("permutohedral_gpu", "grid_gpu"):
+        def fn():
+            ib.Bilateral.apply(work, SIGMA_S, SIGMA_S, 0.0, SIGMA_R, method=method)
+        for _ in range(3):
+            work.copy_(lum)
+            fn()
+        ms, _ = timed_steps(stream, steps, fn, lambda: work.copy_(lum))
+        out[method] = {"ms_per_frame": round(ms / steps, 4),
+                       "mpix_s": round(W * H * steps / (ms / 1e3) / 1e6, 1)}
+    return out
+
+
 def mixed_batch(ib, synth, torch, dev, steps):
     """256 uneven RGB images, per-image sigmas, one batched launch
     sequence (FP16 payload, CUDA graph) against the plain per-image FP32 path."""
@@ -417,7 +437,7 @@ def run_ours(args):
         flush.fill_(1.0)     # evict L2 between steps; both outside the timed window
 
     def headline():
-        ib.bilateral_batch(work, ss, sr, payload=args.payload, autotune=True)
+        ib.bilateral_batch(work, ss, sr, payload=args.payload, autotune=not args.no_autotune)
     headline.stats = ib.last_stats
 
     def plain():
@@ -428,10 +448,10 @@ def run_ours(args):
     alt_payload = "fp16" if args.payload != "fp16" else "fp32"
 
     def alt():
-        ib.bilateral_batch(work, ss, sr, payload=alt_payload, autotune=True)
+        ib.bilateral_batch(work, ss, sr, payload=alt_payload, autotune=not args.no_autotune)
     alt.stats = ib.last_stats
 
-    for _ in range(TUNE_TRIALS):   # the autotuner's trials, before the warm-up proper
+    for _ in range(0 if args.no_autotune else TUNE_TRIALS):   # the autotuner's trials
         prepare()
         headline()
         if not args.quick:
@@ -469,7 +489,7 @@ def run_ours(args):
         for hn, f in zip(host_np, frames):
             hn[...] = f
         t0 = time.perf_counter()
-        ib.bilateral_batch(host_np, ss, sr, payload=args.payload, autotune=True)
+        ib.bilateral_batch(host_np, ss, sr, payload=args.payload, autotune=not args.no_autotune)
         el = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(el)
@@ -572,6 +592,7 @@ def run_ours(args):
         if not args.quick:
             line["batched_" + alt_payload] = alt_line
             line["exact_gt_err"] = exact_error(ib, torch, pristine[0], a)
+            line["grey_4k_d3"] = grey_4k(ib, synth, torch, pristine[0])
         if world == 1 and not args.quick:
             line["mixed_batch"] = mixed_batch(ib, synth, torch, dev, steps=6)
             line["served"] = served_stream(ib, synth, torch)
@@ -597,6 +618,9 @@ def main():
     ap.add_argument("--payload", default="fp32", choices=["fp32", "fp16", "bf16", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="headline and plain path only")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="fixed batch settings (load factor 0.5, blur axes in pairs): a launch "
+                         "sequence that does not depend on the tuner, for profiler captures")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
