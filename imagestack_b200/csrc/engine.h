@@ -62,6 +62,7 @@ struct Engine {
     DevBuf sval;       // filtered rows in slot space, arithmetic type, read by the slice
     DevBuf rec;        // slot of every (point, remainder), [r][n], recorded by the splat
     DevBuf grid;       // the dense grid of the grid method
+    DevBuf tags;       // one tag byte per hash slot (compaction -> neighbour lookups)
     DevBuf dstat;
     // batch metadata: statuses, counts, segment tables (device copy of hmeta)
     DevBuf meta;

@@ -212,6 +212,32 @@ __device__ __forceinline__ int table_find(const TableView& t, const Key<KW>& k, 
     return -1;
 }
 
+// One byte per slot summarising its key (0: empty), written by the compaction: lookups of
+// keys that are mostly absent (the blur's neighbours) read the small tag array, which
+// stays in L2, and touch a slot's key only when its tag matches.
+__device__ __forceinline__ uint8_t slot_tag(uint32_t h) { return (uint8_t)(h | 1u); }
+
+template <int KW>
+__device__ __forceinline__ int table_find_tagged(const TableView& t, const uint8_t* tags, const Key<KW>& k,
+                                                 uint32_t h) {
+    const uint8_t tag = slot_tag(h);
+    uint32_t s = home_slot(h, t.cap);
+    for (int probe = 0; probe < kMaxProbe; ++probe) {
+        const uint8_t g = __ldg(tags + s);
+        if (g == 0) return -1;
+        if (g == tag) {
+            const uint4 w = __ldg(&t.key0[s]);
+            bool same = KW == 1 ? words_equal(w, k.w[0]) : prefix_equal(w, k.w[0]);
+#pragma unroll
+            for (int i = 1; i < KW; ++i)
+                same = same && words_equal(__ldg(&t.keyn[(size_t)(i - 1) * t.stride + s]), k.w[i]);
+            if (same) return (int)s;
+        }
+        s = (s + 1 == t.cap) ? 0u : s + 1;
+    }
+    return -1;
+}
+
 // ---------------------------------------------------------------------------------
 // The simplex that encloses one point: src/Permutohedral.h:293-356.
 // ---------------------------------------------------------------------------------

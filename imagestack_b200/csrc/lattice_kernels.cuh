@@ -131,6 +131,7 @@ struct CompactArgs {
     const void* tvals;     // slot accumulators
     void* vvals;           // vertex values (payload type)
     int wc;                // homogeneous weight channel (homogeneous rows only)
+    uint8_t* tags = nullptr;   // optional slot tags (zeroed), written for occupied slots
 };
 
 struct NbrArgs {
@@ -146,6 +147,7 @@ struct NbrArgs {
     uint32_t vcap;
     const uint32_t* nverts;
     int2* nbr;             // (d+1) x vcap pairs
+    const uint8_t* tags = nullptr;   // slot tags of the compaction, or null: plain lookups
 };
 
 // One launch blurs along one axis (nbrA) or, fused, along two consecutive axes (nbrA then
@@ -412,6 +414,15 @@ __global__ void scan_down_kernel(const uint32_t* __restrict__ bitmap, uint32_t n
 // stored as (v_0/w, ..., v_{wc-1}/w, w) — homogeneous coordinates normalised by their own
 // weight.  A filtered value is then a convex combination of stored values, so a 16-bit
 // payload's rounding of w enters the normalised output only at second order.
+template <int KW>
+__device__ __forceinline__ void write_tag(const CompactArgs& a, uint32_t s) {
+    Key<KW> k;
+    k.w[0] = a.table.key0[s];
+#pragma unroll
+    for (int i = 1; i < KW; ++i) k.w[i] = a.table.keyn[(size_t)(i - 1) * a.table.stride + s];
+    a.tags[s] = slot_tag(key_hash<KW>(k));
+}
+
 template <int KW, int VDP, typename Acc, typename P, bool HOMOG>
 __global__ void assign_kernel(CompactArgs a) {
     const Acc* tvals = reinterpret_cast<const Acc*>(a.tvals);
@@ -429,6 +440,7 @@ __global__ void assign_kernel(CompactArgs a) {
 #pragma unroll
             for (int k = 1; k < KW; ++k)
                 a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.stride + s];
+            if (a.tags) write_tag<KW>(a, s);
             Acc wt = tvals[(size_t)s * VDP];
 #pragma unroll
             for (int k = 0; k < VDP; ++k) if (k == a.wc) wt = tvals[(size_t)s * VDP + k];
@@ -453,6 +465,7 @@ __global__ void assign_kernel(CompactArgs a) {
 #pragma unroll
         for (int k = 1; k < KW; ++k)
             a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.stride + s];
+        if (a.tags) write_tag<KW>(a, s);
 #pragma unroll
         for (int k = 0; k < VDP; ++k)
             Payload<P>::store(vvals + (size_t)vtx * VDP + k, tvals[(size_t)s * VDP + k]);
@@ -492,8 +505,15 @@ __global__ void neighbours_kernel(NbrArgs a) {
             Key<KW> k1, k2;
             pack_key<D>(n1, k1);
             pack_key<D>(n2, k2);
-            const int s1 = table_find<KW>(table, k1, key_hash<KW>(k1));
-            const int s2 = table_find<KW>(table, k2, key_hash<KW>(k2));
+            // tagged lookups exist for multi-word keys only (the host sets tags for those)
+            int s1, s2;
+            if (KW > 1 && a.tags) {
+                s1 = table_find_tagged<KW>(table, a.tags + base, k1, key_hash<KW>(k1));
+                s2 = table_find_tagged<KW>(table, a.tags + base, k2, key_hash<KW>(k2));
+            } else {
+                s1 = table_find<KW>(table, k1, key_hash<KW>(k1));
+                s2 = table_find<KW>(table, k2, key_hash<KW>(k2));
+            }
             a.nbr[(size_t)j * a.vcap + vtx] =
                 make_int2(s1 >= 0 ? (int)__ldg(a.slot2vtx + base + s1) : -1,
                           s2 >= 0 ? (int)__ldg(a.slot2vtx + base + s2) : -1);
