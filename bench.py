@@ -334,7 +334,7 @@ def mixed_batch(ib, synth, torch, dev, steps):
             "max_rel_err_fp16_vs_fp64": err}
 
 
-def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0, workers=4, max_batch=32):
+def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0, workers=2, max_batch=32):
     """BASELINE config 5: Poisson arrivals ramped rate0 -> rate1 req/s over `seconds`;
     half bilateral RGB (d=5), half joint bilateral of a grey image on a grey guide (d=3);
     sides log-uniform 64..2048, sigmas as the mixed batch; FP16 payload, 40 GB budget.

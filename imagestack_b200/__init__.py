@@ -337,7 +337,7 @@ class Server:
     to each request's output array.  Requests of different sizes and kinds are batched as
     they arrive and run on several device streams at once."""
 
-    def __init__(self, workers: int = 4, max_batch: int = 64, payload: str = "fp32",
+    def __init__(self, workers: int = 2, max_batch: int = 64, payload: str = "fp32",
                  memory_budget: int = 40 << 30, device: int = 0, load_factor: float = 0.5):
         L = lib()
         L.pgpu_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]

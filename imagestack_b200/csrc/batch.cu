@@ -75,6 +75,14 @@ namespace {
 
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// Vertices per point learned from earlier lattices, shared by every engine of the process
+// (the server's workers each have one): by image signature, and the latest batch's
+// largest ratio per d as the guess for an unseen signature.  A guess that is too small
+// makes the image overflow its hash range and run again.
+std::mutex g_ratio_mu;
+std::map<std::string, double> g_ratio_by_sig;
+std::map<int, double> g_ratio;
+
 // an image's key for the learned vertex ratio: its shape and position scales
 std::string item_signature(int d, const PointSource& s) {
     char buf[320];
@@ -160,11 +168,14 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     // slots per lattice: (learned vertices per point) x 1.3 x points / load
     std::vector<std::string> sig(nseg);
     std::vector<double> ratio(nseg);
-    const double dflt = E.ratio.count(d) ? E.ratio[d] : 1.0;
-    for (int k = 0; k < nseg; ++k) {
-        sig[k] = item_signature(d, B.items[k].splat);
-        auto it = E.ratio_by_sig.find(sig[k]);
-        ratio[k] = it != E.ratio_by_sig.end() ? it->second : dflt;
+    {
+        std::lock_guard<std::mutex> lk(g_ratio_mu);
+        const double dflt = g_ratio.count(d) ? g_ratio[d] : 1.0;
+        for (int k = 0; k < nseg; ++k) {
+            sig[k] = item_signature(d, B.items[k].splat);
+            auto it = g_ratio_by_sig.find(sig[k]);
+            ratio[k] = it != g_ratio_by_sig.end() ? it->second : dflt;
+        }
     }
     std::vector<uint64_t> cap(nseg);
     for (int k = 0; k < nseg; ++k) {
@@ -418,19 +429,22 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         double rmax = 0.0;
         uint64_t done_vertices = 0;
         size_t fi = 0;
-        for (int k = 0; k < nseg; ++k) {
-            if (fi < failed->size() && (*failed)[fi] == k) {
-                ++fi;
-                continue;
+        {
+            std::lock_guard<std::mutex> lk(g_ratio_mu);
+            if (g_ratio_by_sig.size() > 4096) g_ratio_by_sig.clear();
+            for (int k = 0; k < nseg; ++k) {
+                if (fi < failed->size() && (*failed)[fi] == k) {
+                    ++fi;
+                    continue;
+                }
+                done_vertices += counts[k];
+                if (!B.items[k].n) continue;
+                const double r = (double)counts[k] / (double)B.items[k].n;
+                g_ratio_by_sig[sig[k]] = r;
+                rmax = std::max(rmax, r);
             }
-            done_vertices += counts[k];
-            if (!B.items[k].n) continue;
-            const double r = (double)counts[k] / (double)B.items[k].n;
-            E.ratio_by_sig[sig[k]] = r;
-            rmax = std::max(rmax, r);
+            if (!retry) g_ratio[d] = rmax;
         }
-        if (E.ratio_by_sig.size() > 4096) E.ratio_by_sig.clear();
-        if (!retry) E.ratio[d] = rmax;
         E.last_cap = cap_total;
         if (B.vertices_out && !retry) B.vertices_out->assign(counts, counts + nseg);
 

@@ -76,8 +76,6 @@ struct Engine {
     // host-memory batches: uploads and downloads overlap the lattices on these streams
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
     cudaEvent_t pipe_ev[6] = {};   // per device slot: uploaded, filtered, downloaded
-    std::map<int, double> ratio;                  // vertices per point of recent lattices, by d
-    std::map<std::string, double> ratio_by_sig;   // ... by image shape and scales
     std::map<std::string, cudaGraphExec_t> graphs;  // captured batch pipelines, by batch shape
     // autotuner state per batch shape: candidate trials so far, their times, the choice
     struct Tuning {

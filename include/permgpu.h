@@ -144,7 +144,7 @@ int pgpu_bilateral_batch(pgpu_image *ims, int count, const float *filter_width,
 
 typedef struct pgpu_server_config {
     int device;
-    int workers;                 /* worker threads (streams); 0: 4 */
+    int workers;                 /* worker threads (streams); 0: 2 */
     int max_batch;               /* requests per batch; 0: 64 */
     int payload;                 /* PGPU_PAYLOAD_* of every lattice */
     float load_factor;           /* hash-table load; 0: 0.5 */
