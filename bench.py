@@ -285,7 +285,7 @@ def grey_4k(ib, synth, torch, frame, steps=10):
 
 
 def mixed_batch(ib, synth, torch, dev, steps):
-    """256 uneven RGB images, per-image sigmas, one batched launch
+    """The mixed-size batch: 256 uneven RGB images, per-image sigmas, one batched launch
     sequence (FP16 payload, CUDA graph) against the plain per-image FP32 path."""
     specs = synth.batch_specs(256, 128, 1024, seed=SEED)
     imgs = [torch.from_numpy(synth.image(w, h, 3, rects=16, seed=s)).to(dev)
@@ -335,7 +335,7 @@ def mixed_batch(ib, synth, torch, dev, steps):
 
 
 def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0, workers=2, max_batch=32):
-    """BASELINE config 5: Poisson arrivals ramped rate0 -> rate1 req/s over `seconds`;
+    """The served stream: Poisson arrivals ramped rate0 -> rate1 req/s over `seconds`;
     half bilateral RGB (d=5), half joint bilateral of a grey image on a grey guide (d=3);
     sides log-uniform 64..2048, sigmas as the mixed batch; FP16 payload, 40 GB budget.
     Requests reuse a pool of pinned host images; each has its own pinned output."""
