@@ -485,10 +485,11 @@ void bilateral_job(const pgpu_image* dv, int i0, int i1, const float* filter_wid
     }
 }
 
-// Host-memory batches run in chunks of whole images of at least kChunkPixels pixels.  Two
-// device slots alternate: while the lattices of chunk k run on the compute stream, chunk
-// k+1 is uploaded on one copy stream and chunk k-1 downloaded on the other, so with
-// pinned host images the transfers hide behind the filtering.  A batch smaller than two
+// Host-memory batches run in chunks of whole images of at least kChunkPixels pixels on three
+// device slots in turn: while the lattices of chunk k run on the compute stream, chunk k+1
+// is uploaded on one copy stream and chunk k-1 downloaded on the other, so with pinned host
+// images the transfers hide behind the filtering.  (With two slots, the upload of chunk
+// k+1 would wait for the download of chunk k-1 from the same slot.)  A batch smaller than two
 // chunks is one chunk.  The reported statistics sum over the chunks.
 constexpr size_t kChunkPixels = size_t(1) << 22;
 
@@ -512,6 +513,7 @@ int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int 
     int rc;
     if ((rc = E.img_a.ensure(slot_floats * sizeof(float))) ||
         (nchunks > 1 && (rc = E.img_b.ensure(slot_floats * sizeof(float)))) ||
+        (nchunks > 2 && (rc = E.img_c.ensure(slot_floats * sizeof(float)))) ||
         (rc = E.ensure_copy_streams()))
         return rc;
     cudaStream_t cin = E.copy_in, cout = E.copy_out;
@@ -520,14 +522,15 @@ int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int 
     CUDA_TRY(cudaStreamWaitEvent(cin, E.join_ev[0], 0));
     CUDA_TRY(cudaStreamWaitEvent(cout, E.join_ev[0], 0));
     cudaEvent_t* uploaded = E.pipe_ev;
-    cudaEvent_t* filtered = E.pipe_ev + 2;
-    cudaEvent_t* downloaded = E.pipe_ev + 4;
-    bool slot_used[2] = {false, false};
+    cudaEvent_t* filtered = E.pipe_ev + 3;
+    cudaEvent_t* downloaded = E.pipe_ev + 6;
+    bool slot_used[3] = {false, false, false};
+    DevBuf* slots[3] = {&E.img_a, &E.img_b, &E.img_c};
     std::vector<pgpu_image> dv(ims, ims + count);
 
     auto upload = [&](int k) -> int {
-        const int slot = k & 1;
-        float* base = (float*)(slot ? E.img_b.p : E.img_a.p);
+        const int slot = k % 3;
+        float* base = (float*)slots[slot]->p;
         if (slot_used[slot]) CUDA_TRY(cudaStreamWaitEvent(cin, downloaded[slot], 0));
         size_t off = 0;
         for (int i = cut[k]; i < cut[k + 1]; ++i) {
@@ -544,7 +547,7 @@ int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int 
         memset(&sum, 0, sizeof(sum));
         int r = upload(0);
         for (int k = 0; k < nchunks && !r; ++k) {
-            const int slot = k & 1;
+            const int slot = k % 3;
             if (k + 1 < nchunks && (r = upload(k + 1))) break;
             CUDA_TRY(cudaStreamWaitEvent(st, uploaded[slot], 0));
             BatchJob B;

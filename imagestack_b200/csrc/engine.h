@@ -75,7 +75,7 @@ struct Engine {
     cudaEvent_t join_ev[2] = {};   // ordering against the legacy default stream
     // host-memory batches: uploads and downloads overlap the lattices on these streams
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
-    cudaEvent_t pipe_ev[6] = {};   // per device slot: uploaded, filtered, downloaded
+    cudaEvent_t pipe_ev[9] = {};   // per device slot (3): uploaded, filtered, downloaded
     std::map<std::string, cudaGraphExec_t> graphs;  // captured batch pipelines, by batch shape
     // autotuner state per batch shape: candidate trials so far, their times, the choice
     struct Tuning {
