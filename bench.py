@@ -176,6 +176,36 @@ def cpu_baseline_single():
                       "1 thread, fresh process (%.2f s)" % t}
 
 
+def _cpu_mixed_worker(spec):
+    """The reference's Bilateral::apply on one image of the mixed batch (regenerated here
+    from its seed, not timed); returns (pixels, apply seconds)."""
+    os.environ["OMP_NUM_THREADS"] = "1"
+    import oracle
+    from imagestack_b200 import synth
+    w, h, ss, sr, seed = spec
+    img = synth.image(w, h, 3, rects=16, seed=seed)
+    _, t = oracle.reference_bilateral(img, ss, sr)
+    return w * h, t
+
+
+def cpu_baseline_mixed():
+    """The mixed batch (256 uneven RGB images, their own sigmas) through the reference on
+    all host cores, one single-threaded process per core over disjoint images."""
+    import multiprocessing as mp
+    from imagestack_b200 import synth
+    specs = synth.batch_specs(256, 128, 1024, seed=SEED)
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        pool.map(_cpu_mixed_worker, [(64, 64, 8.0, 0.1, 1)] * procs)   # start the workers
+        t0 = time.perf_counter()
+        res = pool.map(_cpu_mixed_worker, specs, chunksize=1)
+        wall = time.perf_counter() - t0
+    px = sum(r[0] for r in res)
+    return {"value": round(px / wall / 1e6, 2), "unit": "Mpix/s", "cores": procs,
+            "kind": "reference", "sample": "the 256-image mixed batch, FP32, one Bilateral::apply "
+            "per image, %d single-threaded processes (%.2f s wall)" % (procs, wall)}
+
+
 def run_reference_arm(args):
     world, rank, _ = dist_init()
     if rank != 0:
@@ -614,6 +644,8 @@ def run_ours(args):
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline_single()
+                if not args.quick:
+                    line["cpu_baseline_mixed_batch"] = cpu_baseline_mixed()
             except Exception as e:   # report, never fail the GPU line
                 line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
         print(json.dumps(line), flush=True)
