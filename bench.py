@@ -314,6 +314,30 @@ def grey_4k(ib, synth, torch, frame, steps=10):
     return out
 
 
+def gauss_transform_d16(ib, synth, torch, dev, reps=3):
+    """GaussTransform::apply on 2M points of a 16-D Gaussian mixture (4 value channels +
+    the homogeneous one, unit sigmas), the high-dimensional case where keys take three
+    words.  Two untimed calls first: the first learns the vertices-per-point ratio of this
+    shape, the second grows the hash table to the capacity that ratio asks for."""
+    import numpy as np
+    n, d = 2_000_000, 16
+    pos, vals = synth.gauss_mixture(n, d=d, seed=SEED)
+    P = torch.from_numpy(np.ascontiguousarray(pos.T.reshape(d, 1, -1))).to(dev)
+    V = torch.from_numpy(np.ascontiguousarray(vals.T.reshape(vals.shape[1], 1, -1))).to(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def fn():
+        ib.GaussTransform.apply(None, P, V, [1.0] * d)
+    fn.stats = ib.last_stats
+    for _ in range(2):
+        fn()
+    ms, st = timed_steps(stream, reps, fn, lambda: None)
+    return {"points": n, "d": d, "ms_per_call": round(ms / reps, 3),
+            "device_ms": round(sum(s["ms_total"] for s in st) / reps, 3),
+            "vertices": st[-1]["vertices"],
+            "mpoints_s": round(n * reps / (ms / 1e3) / 1e6, 1)}
+
+
 def mixed_batch(ib, synth, torch, dev, steps):
     """The mixed-size batch: 256 uneven RGB images, per-image sigmas, one batched launch
     sequence (FP16 payload, CUDA graph) against the plain per-image FP32 path."""
@@ -636,6 +660,7 @@ def run_ours(args):
             line["batched_" + alt_payload] = alt_line
             line["exact_gt_err"] = exact_error(ib, torch, pristine[0], a)
             line["grey_4k_d3"] = grey_4k(ib, synth, torch, pristine[0])
+            line["gauss_transform_d16"] = gauss_transform_d16(ib, synth, torch, dev)
         if world == 1 and not args.quick:
             line["mixed_batch"] = mixed_batch(ib, synth, torch, dev, steps=6)
             line["served"] = served_stream_fresh()
