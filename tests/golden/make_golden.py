@@ -23,6 +23,15 @@ from rand() seeded by the clock (src/main.cpp:67-75) and compare loosely
   gt_config1_512        512x512 RGB, 16 rectangles, -gausstransform order (x/8, y/8,
                         r/0.1, g/0.1, b/0.1): SHA-256 digests of keys and replay records
                         and 4096 sampled output rows (the full arrays are tens of MB)
+  nlmeans_d8            the shape of NLMeans::apply's filter (src/GaussTransform.cpp:867-874):
+                        80x60 RGB joint-bilateral filtered against a 6-channel patch-feature
+                        guide (linear mixes of shifted image channels, standing in for the
+                        PCA projections), spatial sigma 4, patch sigma 0.3, frames INF, so
+                        d = 6 + 2 = 8 (two key words)
+  chromablur_d3         the shape of ChromaBlur::apply (src/GaussTransform.cpp:792-804): a
+                        72x56 YUV image filtered against its luminance, sigmas (2, 0.5), by
+                        the reference's PERMUTOHEDRAL and GRID methods (AUTO picks GRID for
+                        three position channels)
 """
 from __future__ import annotations
 
@@ -121,5 +130,35 @@ def main():
          sum_splat=big.splat.astype(np.float64).sum(0), sum_blur=big.blur.astype(np.float64).sum(0))
 
 
+def high_d_callers():
+    """Fixtures of the reference's own callers of JointBilateral::apply beyond the bilateral
+    filter: NLMeans (d = PCA dimensions + 2) and ChromaBlur (d = 3)."""
+    rgb = synth.image(80, 60, 3, rects=10, seed=808)
+    mix = (synth.uniform(808, 3, 6 * 3 * 5).astype(np.float32) * 2.0 - 1.0).reshape(6, 3, 5)
+    shifts = [(0, 0), (0, 1), (1, 0), (0, -1), (-1, 0)]
+    guide = np.zeros((6, 60, 80), np.float32)
+    for k in range(6):
+        for c in range(3):
+            for j, (dy, dx) in enumerate(shifts):
+                guide[k] += mix[k, c, j] * np.roll(rgb[c], (dy, dx), axis=(0, 1))
+    inf = float("inf")
+    nl_out, _ = oracle.reference_joint_bilateral(rgb, guide, 4.0, 0.3, sigma_t=inf)
+    save("nlmeans_d8", image=rgb, guide=guide, sigma_s=np.float32(4), sigma_p=np.float32(0.3),
+         out=nl_out)
+
+    rgb = synth.image(72, 56, 3, rects=8, seed=909)
+    y = 0.299 * rgb[0] + 0.587 * rgb[1] + 0.114 * rgb[2]
+    yuv = np.stack([y, 0.492 * (rgb[2] - y), 0.877 * (rgb[0] - y)]).astype(np.float32)
+    lum = y[None].astype(np.float32)
+    perm, _ = oracle.reference_joint_bilateral(yuv, lum, 2.0, 0.5)
+    grid, _ = oracle.reference_joint_bilateral(yuv, lum, 2.0, 0.5, method="grid")
+    save("chromablur_d3", image=yuv, guide=lum, sigma_s=np.float32(2), sigma_c=np.float32(0.5),
+         out_permutohedral=perm, out_grid=grid)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["high_d"]:   # only the fixtures of the high-dimensional callers
+        high_d_callers()
+    else:
+        main()
+        high_d_callers()

@@ -255,3 +255,31 @@ def test_red_probe_does_the_adds_it_times(gpu):
                                       C.byref(rate))
     assert rc == 0 and rate.value > 0
     assert float(table.sum().item()) == 2 * blocks * 256 * per_thread * 4
+
+
+def test_nlmeans_filter_shape_d8_matches_reference(gpu):
+    """NLMeans::apply's filter (src/GaussTransform.cpp:867-874): the image joint-bilateral
+    filtered against patch features, frames INF, so d = 6 + 2 = 8 and keys of two words."""
+    g = golden("nlmeans_d8")
+    im = g["image"].copy()
+    gpu.JointBilateral.apply(im, g["guide"], float(g["sigma_s"]), float(g["sigma_s"]),
+                             float("inf"), float(g["sigma_p"]))
+    assert gpu.last_stats()["d"] == 8
+    assert rel_err(im, g["out"]) <= RTOL_FP32
+
+
+@pytest.mark.parametrize("method,key", [("permutohedral_gpu", "out_permutohedral"),
+                                        ("grid_gpu", "out_grid")])
+def test_chromablur_filter_shape_matches_reference(gpu, method, key):
+    """ChromaBlur::apply's filter (src/GaussTransform.cpp:792-804): YUV against its
+    luminance, by the lattice and by the grid (the method AUTO picks there).  U and V are
+    signed and pass through zero, where summation order alone moves the last FP32 bits by
+    more than 1e-5 of the value (the reference's own FP32 output is 1.4e-7 absolute from
+    the FP64 lattice here), so the relative error is taken against max(|x|, 1e-3 max|x|)."""
+    g = golden("chromablur_d3")
+    im = g["image"].copy()
+    gpu.JointBilateral.apply(im, g["guide"], float(g["sigma_s"]), float(g["sigma_s"]), 0.0,
+                             float(g["sigma_c"]), method=method)
+    err = rel_err(im, g[key], floor_frac=1e-3)
+    print(method, "relative error against the reference:", err)
+    assert err <= RTOL_FP32

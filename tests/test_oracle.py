@@ -197,3 +197,19 @@ def test_reference_operations_agree_with_oracle_lattice():
     d = oracle.oracle_lattice(pos, val)
     norm = (d.out[:, :3] / d.out[:, 3:4]).reshape(60, 80, 3).transpose(2, 0, 1)
     np.testing.assert_array_equal(norm, out)
+
+
+@pytest.mark.parametrize("name,guide_key,sr_key,out_key", [
+    ("nlmeans_d8", "guide", "sigma_p", "out"),
+    ("chromablur_d3", "guide", "sigma_c", "out_permutohedral")])
+def test_oracle_high_dimensional_callers(name, guide_key, sr_key, out_key):
+    """NLMeans's filter (a 6-channel patch-feature guide, d = 8) and ChromaBlur's (YUV
+    against its luminance, d = 3): the oracle reproduces the reference bit for bit."""
+    g = golden(name)
+    im = g["image"]
+    pos, val = oracle.bilateral_points(im, g[guide_key], float(g["sigma_s"]), float(g[sr_key]))
+    assert pos.shape[1] == g[guide_key].shape[0] + 2
+    d = oracle.oracle_lattice(pos, val)
+    c, h, w = im.shape
+    norm = (d.out[:, :c] / d.out[:, c:c + 1]).reshape(h, w, c).transpose(2, 0, 1)
+    np.testing.assert_array_equal(norm, g[out_key])
