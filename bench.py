@@ -140,20 +140,28 @@ def rel_err(a, b, floor_frac=1e-2):
 # CPU baselines: the reference's own code (oracle/_ref), or the C restatement if absent
 # --------------------------------------------------------------------------------------
 
-_CROPS = {}
+_FRAMES = {}
+
+
+def headline_config(payload, world):
+    """The `config` of the headline line; the reference arm reports exactly this dict."""
+    return {"workload": workload(payload), "frame": [W, H], "frames_per_step": FRAMES_PER_STEP,
+            "seed": SEED, "payload": payload, "path": "batched",
+            "l2": "flushed between steps (512 MiB write), outside the timed window",
+            "parallelism": "replicas x%d" % world}
 
 
 def _cpu_worker(args):
-    """One reference Bilateral::apply on a crop of the frame; returns (apply seconds,
-    kind).  The crop is generated once per process and is not timed."""
-    w, h, seed = args
+    """One reference Bilateral::apply on a full frame of the headline workload (frame
+    seed `seed`); returns (apply seconds, kind).  The frame is generated once per process
+    and is not timed."""
+    seed = args[0] if isinstance(args, (tuple, list)) else args
     os.environ["OMP_NUM_THREADS"] = "1"
     import oracle
     from imagestack_b200 import synth
-    key = (w, h, seed)
-    if key not in _CROPS:
-        _CROPS[key] = synth.image(w, h, 3, rects=max(4, RECTS * w * h // (W * H)), seed=seed)
-    img = _CROPS[key]
+    if seed not in _FRAMES:
+        _FRAMES[seed] = synth.image(W, H, 3, rects=RECTS, seed=seed)
+    img = _FRAMES[seed]
     if oracle.reference_available():
         _, t = oracle.reference_bilateral(img, SIGMA_S, SIGMA_R)
         return t, "reference"
@@ -163,17 +171,31 @@ def _cpu_worker(args):
     return time.perf_counter() - t0, "port"
 
 
-def cpu_baseline_single():
-    """Reference Bilateral::apply on one full frame, one thread, in a fresh process."""
+def _cpu_fresh_process(seed, build):
+    """_cpu_worker in a process of its own (the reference's timing drifts with reuse)."""
     code = ("import sys,json; sys.path.insert(0,%r); import bench; "
-            "print(json.dumps(bench._cpu_worker((%d,%d,%d))))" % (ROOT, W, H, SEED))
-    env = dict(os.environ, OMP_NUM_THREADS="1")
+            "print(json.dumps(bench._cpu_worker(%d)))" % (ROOT, seed))
+    env = dict(os.environ, OMP_NUM_THREADS="1", PGPU_REFERENCE_BUILD=build)
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
-                       timeout=600)
-    t, kind = json.loads(r.stdout.strip().splitlines()[-1])
-    return {"value": round(W * H / t / 1e6, 4), "unit": "Mpix/s", "cores": 1, "kind": kind,
-            "sample": "one full 3840x2160 frame, Bilateral::apply(permutohedral), "
-                      "1 thread, fresh process (%.2f s)" % t}
+                       timeout=900)
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def cpu_baseline_single(build="strict", runs=3):
+    """Reference Bilateral::apply on one full frame (the headline's first frame), one
+    thread, the median of `runs` fresh processes.  build "strict": the reference compiled
+    with IEEE-exact flags (the parity oracle); "shipped": its shipped -ffast-math flags."""
+    from imagestack_b200.replicas import frame_seeds
+    seed = frame_seeds(0, FRAMES_PER_STEP, SEED)[0]
+    res = [_cpu_fresh_process(seed, build) for _ in range(runs)]
+    times = sorted(t for t, _ in res)
+    t = statistics.median(times)
+    flags = ("-O3 -ffp-contract=off (strict IEEE)" if build == "strict"
+             else "-O3 -ffast-math (the reference's shipped flags)")
+    return {"value": round(W * H / t / 1e6, 4), "unit": "Mpix/s", "cores": 1, "kind": res[0][1],
+            "sample": "one full 3840x2160 frame (seed %d), Bilateral::apply(permutohedral), "
+                      "1 thread, median of %d fresh processes (%s s), reference built %s"
+                      % (seed, runs, ", ".join("%.2f" % x for x in times), flags)}
 
 
 def _cpu_mixed_worker(spec):
@@ -207,38 +229,46 @@ def cpu_baseline_mixed():
 
 
 def run_reference_arm(args):
+    """The reference's own CPU path on the headline workload: full 3840x2160 frames of the
+    headline batch (the same seeds), one Bilateral::apply per frame, one single-threaded
+    process per host core (the lattice is serial), each step every process filtering one
+    frame; throughput over the whole host."""
     world, rank, _ = dist_init()
     if rank != 0:
         return
     import multiprocessing as mp
+
+    from imagestack_b200.replicas import frame_seeds
     try:
         import psutil
         mem = psutil.virtual_memory().available
     except Exception:
         mem = 64 << 30
     cores = os.cpu_count() or 1
-    # a quarter frame per worker per step; about 1 GB of host memory per worker
-    cw, ch = W // 2, H // 2
-    procs = max(1, min(cores, int(mem // (1 << 30)) - 2, 64))
+    # a full 4K frame through the reference takes about 1.5 GB of host memory
+    procs = max(1, min(cores, int(mem // (2 << 30)) - 1, 64))
+    seeds = frame_seeds(0, FRAMES_PER_STEP, SEED)
     ctx = mp.get_context("spawn")
     times = []
     kind = "reference"
     with ctx.Pool(procs) as pool:
         for step in range(args.warmup + args.steps):
-            # every worker filters its own crop; a step lasts as long as the slowest apply
-            res = pool.map(_cpu_worker, [(cw, ch, SEED + i) for i in range(procs)], chunksize=1)
+            # every process filters one frame of the headline batch; a step lasts as long
+            # as the slowest apply
+            res = pool.map(_cpu_worker, [seeds[(step * procs + i) % len(seeds)] for i in range(procs)],
+                           chunksize=1)
             kind = res[0][1]
             if step >= args.warmup:
                 times.append(max(r[0] for r in res))
-    ms = 1e3 * sum(times) / len(times)
-    value = procs * cw * ch / (ms / 1e3) / 1e6
-    sample = ("%d single-threaded processes, each Bilateral::apply on a %dx%d crop of the "
-              "frame per step" % (procs, cw, ch))
+    ms = 1e3 * statistics.median(times)
+    value = procs * W * H / (ms / 1e3) / 1e6
+    sample = ("%d single-threaded processes, each Bilateral::apply on one full 3840x2160 frame "
+              "of the headline batch per step (median step)" % procs)
     line = {"metric": METRIC, "value": round(value, 4), "unit": "Mpix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload(args.payload), "sample": sample},
+            "config": headline_config(args.payload, world),
             "cpu_baseline": {"value": round(value, 4), "unit": "Mpix/s", "cores": procs,
                              "kind": kind, "sample": sample},
             "e2e": {"value": round(value, 4), "unit": "Mpix/s", "h2d_bytes_per_step": 0,
@@ -627,10 +657,7 @@ def run_ours(args):
             "dtype": {"fp32": "f32", "fp16": "f16-payload/f32-accum",
                       "bf16": "bf16-payload/f32-accum", "fp64": "f64"}[args.payload],
             "data": "synthetic",
-            "config": {"workload": workload(args.payload), "frame": [W, H], "frames_per_step": FRAMES_PER_STEP,
-                       "seed": SEED, "payload": args.payload, "path": "batched",
-                       "l2": "flushed between steps (512 MiB write), outside the timed window",
-                       "parallelism": "replicas x%d" % world},
+            "config": headline_config(args.payload, world),
             "plain_gpu": {"mpix_s": round(plain_mpix, 2), "payload": "fp32",
                           "path": "one frame per call", "stages_ms": plain_stages},
             "max_rel_err_vs_fp64": {"4k_frame": err4k, "tolerance": 1e-3,
@@ -668,7 +695,8 @@ def run_ours(args):
             line["p99_ms"] = line["served"]["p99_ms"]
         if world == 1 and not args.no_cpu_baseline:
             try:
-                line["cpu_baseline"] = cpu_baseline_single()
+                line["cpu_baseline"] = cpu_baseline_single("strict")
+                line["cpu_baseline_shipped_flags"] = cpu_baseline_single("shipped")
                 if not args.quick:
                     line["cpu_baseline_mixed_batch"] = cpu_baseline_mixed()
             except Exception as e:   # report, never fail the GPU line

@@ -77,14 +77,28 @@ def link(objs):
     return LIB
 
 
-REF_SRC = "/root/reference/src"
+def reference_src():
+    """The reference's src/ folder, for the plugin's headers: $IMAGESTACK_SRC if set, else
+    whatever the oracle's Makefile (the recipe that reads the reference sources) reports;
+    None where the sources are absent."""
+    env = os.environ.get("IMAGESTACK_SRC")
+    if env:
+        return env if os.path.isdir(env) else None
+    try:
+        r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "print-src"],
+                           capture_output=True, text=True, timeout=60)
+    except (OSError, subprocess.SubprocessError):
+        return None
+    out = r.stdout.strip().splitlines()
+    return out[-1] if r.returncode == 0 and out and os.path.isdir(out[-1]) else None
 
 
-def build_plugin():
+def build_plugin(ref_src=None):
     """ImageStack plugin: subclasses of the reference's Operation classes, so it compiles
     against the reference headers; built only where those headers exist."""
     src = os.path.join(CSRC, "plugin", "imagestack_plugin.cpp")
-    if not (os.path.isdir(REF_SRC) and os.path.exists(src)):
+    REF_SRC = ref_src or reference_src()
+    if not (REF_SRC and os.path.exists(src)):
         return None
     if _stale(PLUGIN, [src, LIB, os.path.join(INCLUDE, "permgpu.h")]):
         _run([HOSTCXX, "-std=gnu++0x", "-O2", "-fPIC", "-shared", "-w",

@@ -14,7 +14,6 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
-#include <mutex>
 
 #include "engine.h"
 
@@ -61,22 +60,17 @@ static_assert(kUsed <= kScratchBytes, "no-alloc scratch layout does not fit");
 // it to a kernel; pass the address cudaGetSymbolAddress returns for the current device.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-unsigned char* g_scratch_dev[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array in the current context.  Looked up on every call
+// (the lookup allocates nothing): a cached address would go stale if the context were
+// destroyed and recreated (cudaDeviceReset, a host that recreates its primary context),
+// because the module, and with it the array, is then loaded again at a new address.
 int scratch_address(int dev, unsigned char** out) {
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_dev[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(PGPU_ERR_CUDA, "cudaGetSymbolAddress(no-alloc scratch) failed on device %d: %s",
-                        dev, cudaGetErrorString(e));
-        g_scratch_dev[dev] = (unsigned char*)p;
-    }
-    *out = g_scratch_dev[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(PGPU_ERR_CUDA, "cudaGetSymbolAddress(no-alloc scratch) failed on device %d: %s",
+                    dev, cudaGetErrorString(e));
+    *out = (unsigned char*)p;
     return PGPU_OK;
 }
 
@@ -103,7 +97,7 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
                     "pgpu_bilateral_noalloc filters both pixel axes: it needs 0 < filter width "
                     "< 10 x width and 0 < filter height < 10 x height");
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
         cudaGetLastError();
         return fail(PGPU_ERR_NO_DEVICE, "no current CUDA device");
     }
@@ -112,10 +106,18 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
         major != 10)
         return fail(PGPU_ERR_NO_DEVICE, "device %d is not an sm_100 (B200) GPU", dev);
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaStream_t st = (cudaStream_t)stream;
+    // The call waits for its stream and uploads its descriptor from the host stack, so it
+    // cannot be recorded into a CUDA graph: refuse it while the stream is capturing.
+    cudaStreamCaptureStatus cap_status = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(st, &cap_status));
+    if (cap_status != cudaStreamCaptureStatusNone)
+        return fail(PGPU_ERR_UNSUPPORTED,
+                    "pgpu_bilateral_noalloc cannot run inside a stream capture (it waits for its "
+                    "stream and uploads its descriptor from host memory)");
     unsigned char* base = nullptr;
     int rc = scratch_address(dev, &base);
     if (rc) return rc;
-    cudaStream_t st = (cudaStream_t)stream;
 
     const int d = channels + 2;
     const int vd = channels + 1;

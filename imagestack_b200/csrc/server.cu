@@ -36,6 +36,7 @@ struct Req {
     size_t footprint = 0;
     Clock::time_point t_submit, t_done;
     int status = -1;           // -1 while queued or running
+    bool claimed = false;      // a thread is waiting for it (one waiter per ticket)
     std::string error;
 };
 
@@ -114,7 +115,7 @@ public:
                 peak = std::max(peak, inflight);
                 running += (long long)batch.size();
             }
-            const int rc = run(E, batch);
+            const int rc = run_and_drain(E, batch);
             const std::string err = rc ? std::string(last_error()) : std::string();
             {
                 std::lock_guard<std::mutex> lk(mu);
@@ -139,6 +140,19 @@ public:
             cv_done.notify_all();
             cv_work.notify_all();
         }
+    }
+
+    // run() and then wait for the worker's stream whatever run() returned: a failure can
+    // leave copies from or to the requests' host buffers queued, and the caller may free
+    // or reuse those buffers as soon as the request is published as finished
+    int run_and_drain(Engine& E, const std::vector<Req*>& batch) {
+        int rc = run(E, batch);
+        const std::string err = rc ? std::string(last_error()) : std::string();
+        const cudaError_t se = cudaStreamSynchronize(E.stream);
+        if (rc) return fail(rc, "%s", err.c_str());
+        if (se != cudaSuccess)
+            return fail(PGPU_ERR_CUDA, "server stream: %s", cudaGetErrorString(se));
+        return PGPU_OK;
     }
 
     // stage the batch's images, run the batched lattice, copy the results back
@@ -347,9 +361,15 @@ int pgpu_server_wait(void* server, long long ticket, int timeout_ms) {
     auto it = S->reqs.find(ticket);
     if (it == S->reqs.end()) return fail(PGPU_ERR_ARGUMENT, "unknown ticket %lld", ticket);
     Req* q = it->second;
+    // the first waiter to find the request done deletes it, so a second concurrent waiter
+    // on the same ticket is refused rather than left reading freed memory
+    if (q->claimed) return fail(PGPU_ERR_ARGUMENT, "ticket %lld is already being waited for", ticket);
+    q->claimed = true;
     if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(std::max(timeout_ms, 0)),
-                             [&] { return q->status >= 0; }))
+                             [&] { return q->status >= 0; })) {
+        q->claimed = false;   // a later wait may try again
         return fail(PGPU_ERR_TIMEOUT, "request %lld not done after %d ms", ticket, timeout_ms);
+    }
     const int rc = q->status;
     if (rc) fail(rc, "%s", q->error.c_str());
     S->reqs.erase(it);

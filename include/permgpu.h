@@ -173,7 +173,10 @@ int pgpu_server_create(const pgpu_server_config *cfg, void **server);
 /* Queue a request (its images must stay valid until it completes); *ticket identifies it.
  * A request whose footprint alone exceeds the budget is refused with PGPU_ERR_ADMISSION. */
 int pgpu_server_submit(void *server, const pgpu_request *req, long long *ticket);
-/* Wait up to timeout_ms for a request; returns its status, or PGPU_ERR_TIMEOUT. */
+/* Wait up to timeout_ms for a request; returns its status, or PGPU_ERR_TIMEOUT.  A request
+ * is reported finished only after its worker's stream is idle, so its host buffers are
+ * free to reuse when this returns, on success and on failure alike.  One thread waits per
+ * ticket: a second concurrent wait on the same ticket returns PGPU_ERR_ARGUMENT. */
 int pgpu_server_wait(void *server, long long ticket, int timeout_ms);
 /* Wait up to timeout_ms until nothing is queued or running. */
 int pgpu_server_drain(void *server, int timeout_ms);
@@ -216,12 +219,14 @@ int pgpu_lattice_dump(int d, int vd, int n, const float *pos, const float *val, 
  *                anything else is rejected with PGPU_ERR_UNSUPPORTED before any work
  *   stream       cudaStream_t to run on (NULL: the legacy default stream); the call
  *                returns after that stream has finished the filter
- * The first call on a device looks up the array's device address (once per device,
- * with that device current); make that first call before any stream capture.  All calls
- * on a device share the one array: calls that overlap on the GPU (other streams, other
- * host threads) race and corrupt each other, so serialise them.  A frame whose lattice
- * needs more hash slots than the array holds returns PGPU_ERR_CAPACITY and leaves d_out
- * unwritten. */
+ * Every call looks up the array's device address in the current context (a lookup, not
+ * an allocation).  A call waits for its stream and uploads a small descriptor from host
+ * memory, so it cannot be recorded into a CUDA graph: while `stream` is capturing, the
+ * call returns PGPU_ERR_UNSUPPORTED without doing anything.  All calls on a device share
+ * the one array, which keeps the last call's contents (each call clears what must start
+ * at zero): calls that overlap on the GPU (other streams, other host threads) race and
+ * corrupt each other, so serialise them.  A frame whose lattice needs more hash slots
+ * than the array holds returns PGPU_ERR_CAPACITY and leaves d_out unwritten. */
 int pgpu_bilateral_noalloc(const float *d_in, float *d_out, int width, int height,
                            int channels, float filter_width, float filter_height,
                            float color_sigma, void *stream);

@@ -23,6 +23,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liblattice_oracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_HARNESS_SO = os.path.join(REF_DIR, "libref_harness.so")
+# the same harness over the reference built with its shipped flags (-ffast-math); for
+# timing only, loaded instead of the strict one when PGPU_REFERENCE_BUILD=shipped
+REF_HARNESS_FAST_SO = os.path.join(REF_DIR, "libref_harness_fast.so")
 REF_CLI = os.path.join(REF_DIR, "ImageStack")
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -62,14 +65,18 @@ def _load_oracle():
     return _lo
 
 
+def _harness_path() -> str:
+    return REF_HARNESS_FAST_SO if os.environ.get("PGPU_REFERENCE_BUILD") == "shipped" else REF_HARNESS_SO
+
+
 def reference_available() -> bool:
-    return os.path.exists(REF_HARNESS_SO)
+    return os.path.exists(_harness_path())
 
 
 def _load_ref():
     global _ref
     if _ref is None:
-        lib = C.CDLL(REF_HARNESS_SO)
+        lib = C.CDLL(_harness_path())
         lib.refh_last_error.restype = C.c_char_p
         lib.refh_lattice_create.restype = C.c_void_p
         lib.refh_lattice_create.argtypes = [C.c_int, C.c_int, C.c_int]

@@ -32,6 +32,12 @@ from rand() seeded by the clock (src/main.cpp:67-75) and compare loosely
                         72x56 YUV image filtered against its luminance, sigmas (2, 0.5), by
                         the reference's PERMUTOHEDRAL and GRID methods (AUTO picks GRID for
                         three position channels)
+  gt_d16_2m             the full-size high-dimensional Gauss transform: 2,000,000 points of
+                        synth.gauss_mixture(d=16, seed=2) (the benchmark's input), 4 values
+                        + 1, unit sigmas, replay slice: vertex count, SHA-256 digests of the
+                        keys and replay records, 4096 sampled output rows and per-channel
+                        sums of the vertex values (about 5 minutes of reference CPU time;
+                        `python tests/golden/make_golden.py gt_d16_2m` makes only this one)
 """
 from __future__ import annotations
 
@@ -130,6 +136,17 @@ def main():
          sum_splat=big.splat.astype(np.float64).sum(0), sum_blur=big.blur.astype(np.float64).sum(0))
 
 
+def gt_d16_2m():
+    """The high-dimensional Gauss transform at its full size, pinned by digests."""
+    pos, val = synth.gauss_mixture(2_000_000, d=16, seed=2)
+    big = oracle.reference_lattice(pos, val)
+    rows = (synth.uniform(1616, 1, 4096) * pos.shape[0]).astype(np.int64)
+    save("gt_d16_2m", vertices=np.int64(big.keys.shape[0]),
+         keys_sha256=np.array(digest(big.keys)), replay_vtx_sha256=np.array(digest(big.replay_vtx)),
+         replay_w_sha256=np.array(digest(big.replay_w)), rows=rows, out_rows=big.out[rows],
+         sum_splat=big.splat.astype(np.float64).sum(0), sum_blur=big.blur.astype(np.float64).sum(0))
+
+
 def high_d_callers():
     """Fixtures of the reference's own callers of JointBilateral::apply beyond the bilateral
     filter: NLMeans (d = PCA dimensions + 2) and ChromaBlur (d = 3)."""
@@ -159,6 +176,9 @@ def high_d_callers():
 if __name__ == "__main__":
     if sys.argv[1:] == ["high_d"]:   # only the fixtures of the high-dimensional callers
         high_d_callers()
+    elif sys.argv[1:] == ["gt_d16_2m"]:
+        gt_d16_2m()
     else:
         main()
         high_d_callers()
+        gt_d16_2m()

@@ -195,3 +195,44 @@ def test_batch_retries_only_what_overflows(gpu):
     gpu.Bilateral.apply(e1, 1.0, 1.0, 0.0, 0.02)
     assert rel_err(work[0], e0) <= RTOL_FP32
     assert rel_err(work[1], e1) <= RTOL_FP32
+
+
+def _oracle_bilateral(img, ss, sr):
+    """The C oracle's bilateral of one planar image (positions (c/sr, x/ss, y/ss), values
+    (c, 1), normalised by the homogeneous channel)."""
+    import oracle
+    c, h, w = img.shape
+    pos, val = oracle.bilateral_points(img, img, ss, sr)
+    out = oracle.oracle_lattice(pos, val).out
+    return (out[:, :c] / out[:, c:c + 1]).reshape(h, w, c).transpose(2, 0, 1)
+
+
+@pytest.mark.gpu
+def test_full_mixed_batch_matches_the_oracle_and_fp16_the_fp64_lattice(gpu):
+    """The 256-image mixed batch at its real size (sides 128..1024, per-image sigmas), in
+    one batched call from device memory.  FP32: the eight largest and eight smallest images
+    equal the C oracle within 1e-5 — the oracle is pinned bit for bit to the reference, so
+    this checks the batch's segment offsets where the images are large.  FP16 payload:
+    every image within 1e-3 of the FP64 lattice (relative to max(|x|, 1e-2 max|x|))."""
+    import torch
+    specs = synth.batch_specs(256, 128, 1024, seed=2)
+    imgs = [synth.image(w, h, 3, rects=16, seed=s) for (w, h, _, _, s) in specs]
+    ss = [s[2] for s in specs]
+    sr = [s[3] for s in specs]
+    dev = [torch.from_numpy(im).cuda() for im in imgs]
+    work = [d.clone() for d in dev]
+    gpu.bilateral_batch(work, ss, sr, payload="fp32", graph=True)
+    torch.cuda.synchronize()
+    px = [im.shape[1] * im.shape[2] for im in imgs]
+    order = np.argsort(px)
+    for k in list(order[:8]) + list(order[-8:]):
+        expect = _oracle_bilateral(imgs[k], ss[k], sr[k])
+        assert rel_err(work[k].cpu().numpy(), expect) <= RTOL_FP32, "image %d (%d px)" % (k, px[k])
+    half = [d.clone() for d in dev]
+    gpu.bilateral_batch(half, ss, sr, payload="fp16", graph=True)
+    torch.cuda.synchronize()
+    for k in range(256):
+        ref = dev[k].clone()
+        gpu.Bilateral.apply(ref, ss[k], ss[k], 0.0, sr[k], payload="fp64")
+        torch.cuda.synchronize()
+        assert rel_err(half[k].cpu().numpy(), ref.cpu().numpy(), floor_frac=1e-2) <= 1e-3, k

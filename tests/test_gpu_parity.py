@@ -283,3 +283,27 @@ def test_chromablur_filter_shape_matches_reference(gpu, method, key):
     err = rel_err(im, g[key], floor_frac=1e-3)
     print(method, "relative error against the reference:", err)
     assert err <= RTOL_FP32
+
+
+def test_full_size_d16_gauss_transform_matches_reference_digests(gpu):
+    """The 2,000,000-point d=16 Gauss transform (three key words, slot tags and the
+    pending-slot protocol at full scale): the vertex count, the keys in vertex order and
+    the replay records equal the reference's byte for byte, sampled outputs and
+    per-channel value sums within 1e-5."""
+    g = golden("gt_d16_2m")
+    pos, val = synth.gauss_mixture(2_000_000, d=16, seed=2)
+    d = gpu.lattice_dump(pos, val)
+    assert d["keys"].shape[0] == int(g["vertices"])
+    assert sha(d["keys"]) == str(g["keys_sha256"])
+    assert sha(d["replay_vtx"]) == str(g["replay_vtx_sha256"])
+    assert sha(d["replay_w"]) == str(g["replay_w_sha256"])
+    # values are uniform in [-1, 1], so a channel's sum can cancel to near zero while the
+    # splat's atomics (summing in another order than the reference) err relative to the
+    # gross sum; the homogeneous weight in the last channel bounds that gross sum, so each
+    # row's error is taken relative to its largest magnitude
+    a = d["out"][g["rows"]].astype(np.float64)
+    b = g["out_rows"].astype(np.float64)
+    scale = np.abs(b).max(1, keepdims=True)
+    assert float((np.abs(a - b) / scale).max()) <= RTOL_FP32
+    np.testing.assert_allclose(d["splat"].astype(np.float64).sum(0), g["sum_splat"], rtol=1e-5, atol=1e-2)
+    np.testing.assert_allclose(d["blur"].astype(np.float64).sum(0), g["sum_blur"], rtol=1e-5, atol=1e-2)

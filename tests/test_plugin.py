@@ -1,6 +1,7 @@
 """The drop-in path: the reference ImageStack CLI (oracle/_ref/ImageStack, built from the
 reference sources) with `-plugin libpermgpu_imagestack.so`, images exchanged as .tmp files
-(the reference's raw float format, src/FileTMP.cpp)."""
+(the reference's raw float format, src/FileTMP.cpp), read and written by
+imagestack_b200.tmpfile."""
 import os
 import subprocess
 
@@ -10,29 +11,11 @@ import pytest
 import imagestack_b200 as ib
 import oracle
 from imagestack_b200 import synth
+from imagestack_b200.tmpfile import load_tmp, save_tmp
 
 PLUGIN = os.path.join(os.path.dirname(ib.LIB_PATH), "libpermgpu_imagestack.so")
 needs_cli = pytest.mark.skipif(not (os.path.exists(oracle.REF_CLI) and os.path.exists(PLUGIN)),
                                reason="reference CLI or plugin not built")
-
-
-def save_tmp(path, a):
-    """(c, f, h, w) or (c, h, w) float32 -> .tmp: five int32 (w, h, f, c, type 0), then the
-    samples channel by channel, frame by frame, row by row."""
-    a = np.ascontiguousarray(a, np.float32)
-    if a.ndim == 3:
-        a = a[:, None]
-    c, f, h, w = a.shape
-    with open(path, "wb") as fh:
-        np.array([w, h, f, c, 0], np.int32).tofile(fh)
-        a.tofile(fh)
-
-
-def load_tmp(path):
-    with open(path, "rb") as fh:
-        w, h, f, c, t = np.fromfile(fh, np.int32, 5)
-        assert t == 0
-        return np.fromfile(fh, np.float32, c * f * h * w).reshape(c, f, h, w)
 
 
 def run_cli(args, tmp_path, plugin=True):

@@ -126,3 +126,52 @@ def test_admission_refuses_what_cannot_fit_and_serialises_under_a_small_budget(g
         assert st["peak_bytes"] <= 200 << 20
     for q, (_, out) in zip(reqs, tickets):
         assert rel_err(out, direct(gpu, q, "fp32")) <= RTOL_FP32
+
+
+@pytest.mark.gpu
+def test_a_failing_request_is_reported_and_the_server_keeps_serving(gpu):
+    """A Gauss transform whose positions leave the lattice's int16 key range fails inside
+    the batch; wait() returns its error only after the worker's stream is idle (its output
+    stays unwritten), and later requests are served normally."""
+    import torch
+    reqs = mixed_requests(3, seed=9)
+    with gpu.Server(workers=2, payload="fp32") as srv:
+        w, h = 64, 48
+        pos = torch.full((3, h, w), 1e6, dtype=torch.float32).pin_memory().numpy()
+        vals = torch.ones((2, h, w), dtype=torch.float32).pin_memory().numpy()
+        out = torch.full((2, h, w), float("nan")).pin_memory().numpy()
+        t = srv.submit(gpu.REQ_GAUSS_TRANSFORM, vals, out, ref=pos, sigmas=[1.0, 1.0, 1.0])
+        with pytest.raises(gpu.PgpuError) as e:
+            srv.wait(t)
+        assert e.value.code == gpu.ERR_ARGUMENT
+        assert np.isnan(out).all()
+        tickets = [submit(srv, q) for q in reqs]
+        for tk, _ in tickets:
+            srv.wait(tk)
+        st = srv.stats()
+        assert st["failed"] == 1 and st["completed"] == len(reqs)
+    for q, (_, o) in zip(reqs, tickets):
+        assert rel_err(o, direct(gpu, q, "fp32")) <= RTOL_FP32
+
+
+@pytest.mark.gpu
+def test_one_waiter_per_ticket(gpu):
+    """Two threads waiting on one ticket: one gets the result, the other is refused with
+    ERR_ARGUMENT (already being waited for, or already collected), never a crash."""
+    q = mixed_requests(1, seed=10)[0]
+    with gpu.Server(workers=1, payload="fp32") as srv:
+        t, _ = submit(srv, q)
+        codes = []
+
+        def waiter():
+            try:
+                srv.wait(t)
+                codes.append(0)
+            except gpu.PgpuError as e:
+                codes.append(e.code)
+        th = [threading.Thread(target=waiter) for _ in range(2)]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+    assert sorted(codes) == [0, gpu.ERR_ARGUMENT]

@@ -66,3 +66,51 @@ def test_noalloc_refuses_sizes_beyond_its_array(gpu):
     four = torch.zeros((4, 64, 64), device="cuda")
     assert noalloc(four.data_ptr(), four.data_ptr(), 64, 64, 4, 8.0, 8.0, 0.1, None) == \
         gpu.ERR_UNSUPPORTED
+
+
+def test_noalloc_overfull_lattice_leaves_output_unwritten_and_recovers(gpu):
+    """A frame inside the size limits whose lattice still needs more hash slots than the
+    array holds (uniform noise with small sigmas: almost every (pixel, remainder) is its own
+    vertex) is refused with ERR_CAPACITY and d_out is left as it was; the next call starts
+    from a clean array and matches pgpu_bilateral again."""
+    import torch
+    noalloc = _noalloc(gpu)
+    stream = torch.cuda.current_stream().cuda_stream
+    rng = np.random.default_rng(5)
+    noise = torch.from_numpy(rng.random((3, 512, 512), dtype=np.float32)).cuda()
+    out = torch.full_like(noise, float("nan"))
+    torch.cuda.synchronize()
+    rc = noalloc(noise.data_ptr(), out.data_ptr(), 512, 512, 3, 1.0, 1.0, 0.02, stream)
+    torch.cuda.synchronize()
+    assert rc == gpu.ERR_CAPACITY, gpu.lib().pgpu_last_error().decode()
+    assert torch.isnan(out).all().item()
+    img = synth.image(256, 256, 3, rects=8, seed=33)
+    expect = torch.from_numpy(img.copy()).cuda()
+    gpu.Bilateral.apply(expect, 8.0, 8.0, 0.0, 0.1)
+    src = torch.from_numpy(img).cuda()
+    out2 = torch.full_like(src, float("nan"))
+    torch.cuda.synchronize()
+    assert noalloc(src.data_ptr(), out2.data_ptr(), 256, 256, 3, 8.0, 8.0, 0.1, stream) == 0
+    torch.cuda.synchronize()
+    assert rel_err(out2.cpu().numpy(), expect.cpu().numpy()) <= RTOL_FP32
+
+
+def test_noalloc_refuses_to_run_inside_a_stream_capture(gpu):
+    """A call waits for its stream, so it cannot be part of a CUDA graph: during a capture
+    it returns ERR_UNSUPPORTED and queues nothing."""
+    import torch
+    noalloc = _noalloc(gpu)
+    img = torch.zeros((1, 64, 64), device="cuda")
+    out = torch.zeros_like(img)
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g, stream=side):
+        out.add_(1.0)   # the graph needs one node of its own
+        rc = noalloc(img.data_ptr(), out.data_ptr(), 64, 64, 1, 4.0, 4.0, 0.1,
+                     torch.cuda.current_stream().cuda_stream)
+    assert rc == gpu.ERR_UNSUPPORTED
+    assert b"capture" in gpu.lib().pgpu_last_error()
+    g.replay()
+    torch.cuda.synchronize()
+    assert (out == 1.0).all().item()
