@@ -10,6 +10,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -124,6 +126,8 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     if (nseg == 0) return PGPU_OK;
     const DimOps* ops = dim_ops(d);
     if (!ops) return fail(PGPU_ERR_UNSUPPORTED, "%d position dimensions (supported: 1..%d)", d, kMaxD);
+    if (!ops->prepare())
+        return fail(PGPU_ERR_CUDA, "tile splat set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
     const int vdp = vdp_for(vd);
     if (!vdp) return fail(PGPU_ERR_UNSUPPORTED, "%d value channels (supported: 1..8)", vd);
     if (B.payload < 0 || B.payload > 3) return fail(PGPU_ERR_ARGUMENT, "unknown payload %d", B.payload);
@@ -143,38 +147,36 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     const bool use_tags = kw > 1;
     const bool graph = B.use_graph && !dumps;
 
-    // points, blocks and first-touch entries, lattice after lattice
+    // points and first-touch entries, lattice after lattice
     uint64_t n_total = 0, ns_total = 0;
-    uint64_t blocks = 0, slice_blocks = 0;
-    std::vector<uint32_t> pbase(nseg), bbase(nseg), spbase(nseg), sbbase(nseg);
+    std::vector<uint32_t> pbase(nseg), spbase(nseg);
     for (int k = 0; k < nseg; ++k) {
         const BatchItem& it = B.items[k];
         pbase[k] = (uint32_t)n_total;
-        bbase[k] = (uint32_t)blocks;
         n_total += it.n;
-        blocks += (it.n + kSplatThreads - 1) / kSplatThreads;
-        const uint64_t ns = B.replay ? it.n : it.n_slice;
         spbase[k] = (uint32_t)ns_total;
-        sbbase[k] = (uint32_t)slice_blocks;
-        ns_total += ns;
-        slice_blocks += (ns + kSliceThreads - 1) / kSliceThreads;
+        ns_total += B.replay ? it.n : it.n_slice;
     }
     const uint64_t entries = n_total * (uint64_t)(d + 1);
-    if (entries >= 0xFFFFFFFFull || ns_total * (uint64_t)(d + 1) >= 0xFFFFFFFFull || blocks >= 0x7FFFFFFFull)
+    if (entries >= 0xFFFFFFFFull || ns_total * (uint64_t)(d + 1) >= 0xFFFFFFFFull)
         return fail(PGPU_ERR_UNSUPPORTED, "too many points for one batch (%llu)",
                     (unsigned long long)n_total);
     const uint32_t nwords = (uint32_t)((entries + 31) / 32);
 
     // slots per lattice: (learned vertices per point) x 1.3 x points / load
     std::vector<std::string> sig(nseg);
-    std::vector<double> ratio(nseg);
+    std::vector<double> ratio(nseg), density(nseg);
     {
         std::lock_guard<std::mutex> lk(g_ratio_mu);
-        const double dflt = g_ratio.count(d) ? g_ratio[d] : 1.0;
+        const bool have_d = g_ratio.count(d) != 0;
+        const double dflt = have_d ? g_ratio[d] : 1.0;
         for (int k = 0; k < nseg; ++k) {
             sig[k] = item_signature(d, B.items[k].splat);
             auto it = g_ratio_by_sig.find(sig[k]);
             ratio[k] = it != g_ratio_by_sig.end() ? it->second : dflt;
+            // what the splat choice goes by: the learned ratio, else the latest batch's for
+            // this d, else nothing known (0: the tile splat)
+            density[k] = it != g_ratio_by_sig.end() ? it->second : have_d ? dflt : 0.0;
         }
     }
     std::vector<uint64_t> cap(nseg);
@@ -189,6 +191,49 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         const uint64_t c = (uint64_t)std::ceil((double)est / load);
         cap[k] = std::max<uint64_t>((c + 31) & ~31ull, 256);
     }
+
+    // Splat kernel per lattice: the tile splat (shared-memory table per 32x32 tile) where
+    // neighbouring points share vertices, which the learned vertices-per-point ratio tells
+    // (4K d=5 bilateral: 0.18; a 32x32 tile then holds about 370 of its 6144 entries'
+    // vertices); the direct splat for sparse lattices (ratio above kTileRatioMax, where a
+    // tile's distinct vertices would overflow its 1024 shared-memory slots), multi-word
+    // keys and FP64 accumulators.  With nothing learned yet for the image or its d, the
+    // tile splat.  PGPU_SPLAT=direct or =tile in the environment overrides the choice
+    // where both exist (the parity tests compare the two).
+    constexpr double kTileRatioMax = 0.8;
+    const char* mode = std::getenv("PGPU_SPLAT");
+    const int forced = !mode ? 0 : !strcmp(mode, "direct") ? 1 : !strcmp(mode, "tile") ? 2 : 0;
+    const bool tile_ok = kw == 1 && B.payload != kPayloadF64 && forced != 1;
+    std::vector<Segment> segs(nseg), slsegs(B.replay ? 0 : nseg);
+    uint64_t blocks = 0, tile_blocks = 0, slice_blocks = 0;
+    for (int k = 0; k < nseg; ++k) {
+        const BatchItem& it = B.items[k];
+        Segment& sgm = segs[k];
+        memset(&sgm, 0, sizeof(sgm));
+        sgm.src = it.splat;
+        sgm.out = it.out;
+        sgm.n = it.n;
+        sgm.point_base = pbase[k];
+        const bool tiled = tile_ok && (forced == 2 || (density[k] <= kTileRatioMax && it.n >= 256));
+        uint32_t nb_splat = 0, nb_tile = 0, nb_slice = 0;
+        segment_geometry(sgm, B.replay ? it.splat : it.slice, tiled, &nb_splat, &nb_tile, &nb_slice);
+        sgm.splat_base = (uint32_t)blocks;
+        sgm.tile_base = (uint32_t)tile_blocks;
+        sgm.block_base = (uint32_t)slice_blocks;
+        blocks += nb_splat;
+        tile_blocks += nb_tile;
+        slice_blocks += nb_slice;
+        if (!B.replay) {
+            Segment& sl = slsegs[k];
+            sl = sgm;
+            sl.src = it.slice;
+            sl.n = it.n_slice;
+            sl.point_base = spbase[k];
+        }
+    }
+    if (blocks >= 0x7FFFFFFFull || tile_blocks >= 0x7FFFFFFFull || slice_blocks >= 0x7FFFFFFFull)
+        return fail(PGPU_ERR_UNSUPPORTED, "too many points for one batch (%llu)",
+                    (unsigned long long)n_total);
 
     const MetaLayout L = layout(nseg, !B.replay);
     int rc;
@@ -229,23 +274,13 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             hentry[k] = k < nseg ? pbase[k] * (uint32_t)(d + 1) : (uint32_t)entries;
         }
         for (int k = 0; k < nseg; ++k) {
-            const BatchItem& it = B.items[k];
-            Segment s;
-            memset(&s, 0, sizeof(s));
-            s.src = it.splat;
-            s.out = it.out;
-            s.n = it.n;
-            s.point_base = pbase[k];
-            s.block_base = bbase[k];
-            s.slot_base = (uint32_t)sbase[k];
-            s.cap = (uint32_t)cap[k];
-            hseg[k] = s;
+            segs[k].slot_base = (uint32_t)sbase[k];
+            segs[k].cap = (uint32_t)cap[k];
+            hseg[k] = segs[k];
             if (!B.replay) {
-                s.src = it.slice;
-                s.n = it.n_slice;
-                s.point_base = spbase[k];
-                s.block_base = sbbase[k];
-                hsl[k] = s;
+                slsegs[k].slot_base = (uint32_t)sbase[k];
+                slsegs[k].cap = (uint32_t)cap[k];
+                hsl[k] = slsegs[k];
             }
         }
 
@@ -275,7 +310,10 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             sa.rec_slot = B.replay ? (uint32_t*)E.rec.p : nullptr;
             sa.seg_status = (unsigned*)(dmeta + L.segstat);
             sa.blocks = (uint32_t)blocks;
+            sa.tile_blocks = (uint32_t)tile_blocks;
             if (!ops->splat(sa, vdp, B.payload, st)) return fail(PGPU_ERR_UNSUPPORTED, "splat variant");
+            CUDA_TRY(cudaGetLastError());
+            if (!ops->splat_tile(sa, vdp, B.payload, st)) return fail(PGPU_ERR_UNSUPPORTED, "tile splat variant");
             CUDA_TRY(cudaGetLastError());
             if (timed) CUDA_TRY(cudaEventRecord(E.ev[1], st));
 

@@ -1,5 +1,7 @@
 // Kernels that do not depend on the number of position dimensions: first-touch
 // marking, the prefix popcount that numbers the vertices, compaction and the blur.
+#include <algorithm>
+
 #include "lattice_ops.h"
 
 namespace pgpu {
@@ -118,6 +120,38 @@ void launch_segment_counts(const uint32_t* bitmap, const uint32_t* offs, uint32_
 // ---------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------
+static uint32_t pow2_at_least(uint32_t x) {
+    uint32_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+void segment_geometry(Segment& s, const PointSource& slice_src, bool tiled, uint32_t* splat,
+                      uint32_t* tile, uint32_t* slice) {
+    const uint32_t W = (uint32_t)s.src.width, H = (uint32_t)s.src.height, F = (uint32_t)s.src.frames;
+    const uint64_t n = (uint64_t)W * H * F;
+    if (tiled) {
+        // rows of 32 pixels (a warp) stacked into 32x32 tiles; a point list (one row) in
+        // runs of kTilePixels
+        s.tile_w = (H == 1 && F == 1) ? (uint32_t)kTilePixels : std::min<uint32_t>(32u, pow2_at_least(W));
+        s.tile_h = (uint32_t)kTilePixels / s.tile_w;
+        s.tiles_x = (W + s.tile_w - 1) / s.tile_w;
+        s.tiles_y = (H + s.tile_h - 1) / s.tile_h;
+        *tile = s.tiles_x * s.tiles_y * F;
+        *splat = 0;
+    } else {
+        s.tile_w = s.tile_h = s.tiles_x = s.tiles_y = 0;
+        *tile = 0;
+        *splat = (uint32_t)((n + kSplatThreads - 1) / kSplatThreads);
+    }
+    const uint32_t Ws = (uint32_t)slice_src.width, Hs = (uint32_t)slice_src.height,
+                   Fs = (uint32_t)slice_src.frames;
+    s.slice_tw = (Hs == 1 && Fs == 1) ? (uint32_t)kSliceThreads : std::min<uint32_t>(32u, pow2_at_least(Ws));
+    s.slice_th = (uint32_t)kSliceThreads / s.slice_tw;
+    s.stiles_x = (Ws + s.slice_tw - 1) / s.slice_tw;
+    s.stiles_y = (Hs + s.slice_th - 1) / s.slice_th;
+    *slice = s.stiles_x * s.stiles_y * Fs;
+}
 const DimOps* dim_ops(int d) {
     switch (d) {
     case 1: return dim_ops_1();

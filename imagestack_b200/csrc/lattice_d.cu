@@ -1,6 +1,8 @@
 // Per-dimension instantiation of the splat, neighbour and slice kernels.  This file is
 // compiled once for each d in 1..16 with -DPGPU_D=d, so the sixteen variants build in
 // parallel and each keeps its per-point arrays in registers.
+#include <atomic>
+
 #include "lattice_ops.h"
 
 #ifndef PGPU_D
@@ -31,6 +33,49 @@ bool splat(const SplatArgs& a, int vdp, int payload, cudaStream_t st) {
     case 2: f64 ? splat_t<2, double>(a, st) : splat_t<2, float>(a, st); return true;
     case 4: f64 ? splat_t<4, double>(a, st) : splat_t<4, float>(a, st); return true;
     case 8: f64 ? splat_t<8, double>(a, st) : splat_t<8, float>(a, st); return true;
+    }
+    return false;
+}
+
+// The tile splat's shared-memory limit is an attribute of each kernel on each device; it
+// is set once per device (a bit per device ordinal), outside any stream capture.
+std::atomic<uint64_t> g_tile_prepared{0};
+
+template <int VDP>
+bool prepare_tile_t() {
+    if constexpr (key_words(D) == 1)
+        return cudaFuncSetAttribute(splat_tile_kernel<D, VDP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)tile_smem_bytes(D, VDP)) == cudaSuccess;
+    return true;
+}
+
+bool prepare() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    const uint64_t bit = 1ull << (dev & 63);
+    if (g_tile_prepared.load() & bit) return true;
+    if (!prepare_tile_t<2>() || !prepare_tile_t<4>() || !prepare_tile_t<8>()) return false;
+    g_tile_prepared.fetch_or(bit);
+    return true;
+}
+
+template <int VDP>
+bool splat_tile_t(const SplatArgs& a, cudaStream_t st) {
+    if constexpr (key_words(D) == 1) {
+        if (!a.tile_blocks) return true;
+        splat_tile_kernel<D, VDP><<<a.tile_blocks, kTileThreads, tile_smem_bytes(D, VDP), st>>>(a);
+        return true;
+    } else {
+        return a.tile_blocks == 0;
+    }
+}
+
+bool splat_tile(const SplatArgs& a, int vdp, int payload, cudaStream_t st) {
+    if (payload == kPayloadF64) return a.tile_blocks == 0;
+    switch (vdp) {
+    case 2: return splat_tile_t<2>(a, st);
+    case 4: return splat_tile_t<4>(a, st);
+    case 8: return splat_tile_t<8>(a, st);
     }
     return false;
 }
@@ -68,7 +113,7 @@ bool slice(const SliceArgs& a, int vdp, int payload, bool homog, cudaStream_t st
     return false;
 }
 
-const DimOps kOps = {splat, neighbours, slice};
+const DimOps kOps = {splat, splat_tile, prepare, neighbours, slice};
 
 }  // namespace
 

@@ -60,26 +60,44 @@ struct OutView {
 // Each lattice owns a contiguous range of the shared hash-slot array and of the point
 // numbering; its points are numbered after the previous lattice's, so first-touch order,
 // and with it the vertex numbering, stays per-lattice insertion order.
+//
+// Blocks of three launches cover a segment, each launch with its own block numbering:
+//   direct splat  kSplatThreads consecutive points per block (splat_base; no blocks when
+//                 the segment uses the tile splat)
+//   tile splat    one tile_w x tile_h tile of one frame per block, tiles_x x tiles_y tiles
+//                 per frame (tile_base; no blocks when tile_w == 0)
+//   slice         one slice_tw x slice_th tile of one frame per block (slice_tw * slice_th
+//                 == kSliceThreads), stiles_x x stiles_y tiles per frame (block_base)
 struct Segment {
     PointSource src;       // its points
     OutView out;           // where its slice goes
     uint32_t n;            // points
     uint32_t point_base;   // first point in the batch numbering
-    uint32_t block_base;   // first block of the segment in splat / slice launches
+    uint32_t block_base;   // first block of the segment in the slice launch
     uint32_t slot_base;    // first slot in the shared hash-slot array
     uint32_t cap;          // slots
+    uint32_t splat_base;   // first block in the direct splat launch
+    uint32_t tile_base;    // first block in the tile splat launch
+    uint32_t tile_w, tile_h, tiles_x, tiles_y;     // tile splat geometry (tile_w 0: direct)
+    uint32_t slice_tw, slice_th, stiles_x, stiles_y;   // slice geometry
     uint32_t pad_;
 };
 
-// Segment of block b: the last one whose block_base <= b (segments are in block order).
-__device__ __forceinline__ int segment_of_block(const Segment* segs, int nseg, uint32_t b) {
+// Segment of block b of a launch whose per-segment first blocks are the field Base: the
+// last segment whose Base <= b (segments are in block order; a segment with no blocks in
+// this launch shares its Base with the next one and is never picked for a block).
+template <uint32_t Segment::*Base>
+__device__ __forceinline__ int segment_by(const Segment* segs, int nseg, uint32_t b) {
     int lo = 0, hi = nseg - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(&segs[mid].block_base) <= b) lo = mid;
+        if (__ldg(&(segs[mid].*Base)) <= b) lo = mid;
         else hi = mid - 1;
     }
     return lo;
+}
+__device__ __forceinline__ int segment_of_block(const Segment* segs, int nseg, uint32_t b) {
+    return segment_by<&Segment::block_base>(segs, nseg, b);
 }
 
 // Segment of slot s: the last k with slot_base[k] <= s (slot_base has nseg + 1 entries).
@@ -114,7 +132,8 @@ struct SplatArgs {
     uint32_t* ft;          // cap_total first-touch entries, all ones
     uint32_t* rec_slot;    // optional [r][n_total] slot of every (point, remainder)
     unsigned* seg_status;  // one status word per segment
-    uint32_t blocks;       // splat blocks of the batch
+    uint32_t blocks;       // direct splat blocks of the batch
+    uint32_t tile_blocks;  // tile splat blocks of the batch
 };
 
 struct CompactArgs {
@@ -300,10 +319,10 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
     __shared__ unsigned char s_coord[(D + 1) * kSplatThreads];
     __shared__ uint4 s_key[kKeysInSmem ? (D + 1) * kSplatThreads : 1];
     __shared__ Segment sg;
-    const int kseg = segment_of_block(a.segs, a.nseg, blockIdx.x);
+    const int kseg = segment_by<&Segment::splat_base>(a.segs, a.nseg, blockIdx.x);
     load_segment(a.segs + kseg, sg);
     const unsigned lane = threadIdx.x & 31u;
-    const uint32_t i = (blockIdx.x - sg.block_base) * (uint32_t)kSplatThreads + threadIdx.x;
+    const uint32_t i = (blockIdx.x - sg.splat_base) * (uint32_t)kSplatThreads + threadIdx.x;
     const bool valid = i < sg.n;
     const unsigned active = __ballot_sync(0xFFFFFFFFu, valid);
     if (!valid) return;
@@ -393,6 +412,207 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
         if (s >= 0) atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
         if (a.rec_slot)
             a.rec_slot[(size_t)r * a.n_total + gi] = s >= 0 ? sg.slot_base + (uint32_t)s : 0xFFFFFFFFu;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// tile splat: one block per 2D tile of kTilePixels pixels of one frame
+// ---------------------------------------------------------------------------------
+// Neighbouring pixels land on the same lattice vertices: on the 4K d=5 bilateral a 32x32
+// tile's 6144 (point, remainder) entries touch about 370 distinct vertices, while a
+// direct splat's block of 256 consecutive pixels of a row touches 470 of 1536.  The tile
+// splat therefore inserts and sums every entry into a hash table of the block's own in
+// shared memory (phase A), then adds each distinct vertex to the global table once: one
+// insert, one row reduction and one first-touch minimum per (tile, vertex) instead of one
+// row reduction per (point, remainder) (phase B), and finally writes the replay record
+// from the shared-memory slot of each entry (phase C).  A shared-memory slot's first
+// touch is the smallest entry that reached it, so the global minimum over tiles is the
+// reference's first insertion as before; the vertex set, keys and records are the same as
+// the direct splat's, only the order of the FP32 additions differs.  An entry whose probe
+// finds no free local slot within kTileProbe goes straight to the global table, as in the
+// direct splat, so no tile can overflow.  One-word keys only (d <= 7), FP32 accumulators.
+constexpr int kTileThreads = 256;
+constexpr int kTilePixels = 1024;       // 4 pixels per thread
+constexpr int kTileSlots = 1024;        // shared-memory hash slots per block
+constexpr int kTileProbe = 64;
+__host__ __device__ constexpr int tile_min_blocks(int d) { return d <= 5 ? 3 : 2; }
+
+// dynamic shared memory of a tile splat block: keys, rows, first touches (then global
+// slots), the local slot of every (pixel, remainder), the simplex scratch
+__host__ __device__ constexpr size_t tile_smem_bytes(int d, int vdp) {
+    return (size_t)kTileSlots * 16 + (size_t)kTileSlots * vdp * 4 + (size_t)kTileSlots * 4 +
+           (size_t)(d + 1) * kTilePixels * 2 + (size_t)(d + 1) * kTileThreads * 4 +
+           (size_t)(d + 1) * kTileThreads + 16;
+}
+
+// find-or-insert of a one-word key in the block's table; -1 when no slot within the probe
+// limit is free (the caller then uses the global table)
+__device__ __forceinline__ int tile_insert(uint4* t_key, const uint4& k, uint32_t h) {
+    const uint4 empty = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+    uint32_t l = h >> (32 - 10);   // kTileSlots == 1024
+    static_assert(kTileSlots == 1024, "home slot uses the top 10 hash bits");
+#pragma unroll 1
+    for (int probe = 0; probe < kTileProbe; ++probe) {
+        uint4 w = t_key[l];
+        if (is_empty_word(w)) w = atomicCAS_block(&t_key[l], empty, k);
+        if (is_empty_word(w) || words_equal(w, k)) return (int)l;
+        l = (l + 1) & (kTileSlots - 1);
+    }
+    return -1;
+}
+
+template <int D, int VDP>
+__global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_kernel(SplatArgs a) {
+    static_assert(key_words(D) == 1, "the tile splat handles one-word keys (d <= 7)");
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    uint4* t_key = reinterpret_cast<uint4*>(tile_smem);
+    float* t_row = reinterpret_cast<float*>(t_key + kTileSlots);
+    uint32_t* t_ft = reinterpret_cast<uint32_t*>(t_row + kTileSlots * VDP);
+    uint16_t* t_loc = reinterpret_cast<uint16_t*>(t_ft + kTileSlots);
+    float* s_delta = reinterpret_cast<float*>(t_loc + (D + 1) * kTilePixels);
+    unsigned char* s_coord = reinterpret_cast<unsigned char*>(s_delta + (D + 1) * kTileThreads);
+    __shared__ Segment sg;
+    const int kseg = segment_by<&Segment::tile_base>(a.segs, a.nseg, blockIdx.x);
+    for (int l = threadIdx.x; l < kTileSlots; l += kTileThreads) {
+        t_key[l] = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+        t_ft[l] = 0xFFFFFFFFu;
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) t_row[l * VDP + k] = 0.0f;
+    }
+    load_segment(a.segs + kseg, sg);   // ends with a barrier
+
+    unsigned* status = a.seg_status + kseg;
+    const TableView table{a.key0 + sg.slot_base, a.keyn + sg.slot_base, sg.cap, a.cap_total};
+    float* vals = reinterpret_cast<float*>(a.vals) + (size_t)sg.slot_base * VDP;
+    uint32_t* ft = a.ft + sg.slot_base;
+    const uint32_t b = blockIdx.x - sg.tile_base;
+    const uint32_t per_frame = sg.tiles_x * sg.tiles_y;
+    const uint32_t f = b / per_frame, bt = b - f * per_frame;
+    const uint32_t ty = bt / sg.tiles_x, tx = bt - ty * sg.tiles_x;
+    const uint32_t x0 = tx * sg.tile_w, y0 = ty * sg.tile_h;
+    const uint32_t W = (uint32_t)sg.src.width, H = (uint32_t)sg.src.height;
+    const unsigned lane = threadIdx.x & 31u;
+    const SimplexScratch scr{s_delta + threadIdx.x, s_coord + threadIdx.x, kTileThreads};
+
+    // Phase A: every entry into the block's table.  Lanes of a warp are consecutive pixels
+    // of one tile row (ascending point numbers), grouped by key as in the direct splat; the
+    // group's leader inserts and records the first touch, every lane adds its own row.
+#pragma unroll 1
+    for (int k = 0; k < kTilePixels / kTileThreads; ++k) {
+        const uint32_t p = threadIdx.x + (uint32_t)k * kTileThreads;
+        const uint32_t px = x0 + p % sg.tile_w, py = y0 + p / sg.tile_w;
+        const bool valid = px < W && py < H;
+        const unsigned active = __ballot_sync(0xFFFFFFFFu, valid);
+        if (valid) {
+            const uint32_t i = (f * H + py) * W + px;
+            float pp[D], v[VDP];
+            load_point<D, VDP>(sg.src, i, pp, v);
+            Simplex<D> sx;
+            compute_simplex<D>(pp, a.lc, sx, status, scr);
+            const uint32_t gi = sg.point_base + i;
+            const uint32_t e0 = gi * (uint32_t)(D + 1);
+            Key<1> key;
+            first_key<D>(sx, key);
+#pragma unroll
+            for (int r = 0; r <= D; ++r) {
+                if (r > 0) key_step<D>(key, scr.coord[(D - (r - 1)) * scr.stride]);
+                const uint32_t hk = key_hash<1>(key);
+                unsigned pr = __match_any_sync(active, hk);
+                {
+                    const unsigned ld = __ffs(pr) - 1;
+                    bool same = __shfl_sync(active, key.w[0].x, ld) == key.w[0].x;
+                    same &= __shfl_sync(active, key.w[0].y, ld) == key.w[0].y;
+                    same &= __shfl_sync(active, key.w[0].z, ld) == key.w[0].z;
+                    same &= __shfl_sync(active, key.w[0].w, ld) == key.w[0].w;
+                    if (!__all_sync(active, same)) {
+                        pr = __match_any_sync(active, ((unsigned long long)key.w[0].y << 32) | key.w[0].x);
+                        pr &= __match_any_sync(active, ((unsigned long long)key.w[0].w << 32) | key.w[0].z);
+                    }
+                }
+                const unsigned leader = __ffs(pr) - 1;
+                int l = -1;
+                if (lane == leader) {
+                    l = tile_insert(t_key, key.w[0], hk);
+                    if (l >= 0) atomicMin(&t_ft[l], e0 + (uint32_t)r);
+                }
+                l = __shfl_sync(active, l, leader);
+                float c[VDP];
+#pragma unroll
+                for (int q = 0; q < VDP; ++q) c[q] = __fmul_rn(sx.bary[r], v[q]);
+                if (l >= 0) {
+#pragma unroll
+                    for (int q = 0; q < VDP; ++q) atomicAdd(&t_row[l * VDP + q], c[q]);
+                    t_loc[r * kTilePixels + p] = (uint16_t)l;
+                } else {
+                    // the block's table is full around this key: the global table directly
+                    int s = -1;
+                    if (lane == leader) {
+                        const uint32_t home = home_slot(hk, table.cap);
+                        s = table_insert<1>(table, key, home, __ldcg(&table.key0[home]), status);
+                        if (s >= 0) atomicMin(&ft[s], e0 + (uint32_t)r);
+                    }
+                    s = __shfl_sync(pr, s, leader);
+                    if (s >= 0) atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
+                    if (a.rec_slot)
+                        a.rec_slot[(size_t)r * a.n_total + gi] =
+                            s >= 0 ? sg.slot_base + (uint32_t)s : 0xFFFFFFFFu;
+                    t_loc[r * kTilePixels + p] = 0xFFFFu;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Phase B: each distinct vertex of the tile into the global table once; the home-slot
+    // loads of all of a thread's occupied local slots are issued before any is resolved.
+    constexpr int kPer = kTileSlots / kTileThreads;
+    uint4 kw[kPer];
+    uint32_t home[kPer];
+    uint4 first[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        kw[j] = t_key[threadIdx.x + j * kTileThreads];
+        home[j] = 0;
+        first[j] = make_uint4(0u, 0u, 0u, 0u);
+        if (!is_empty_word(kw[j])) {
+            Key<1> kk;
+            kk.w[0] = kw[j];
+            home[j] = home_slot(key_hash<1>(kk), table.cap);
+            first[j] = __ldcg(&table.key0[home[j]]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int l = threadIdx.x + j * kTileThreads;
+        if (is_empty_word(kw[j])) continue;
+        Key<1> kk;
+        kk.w[0] = kw[j];
+        const int s = table_insert<1>(table, kk, home[j], first[j], status);
+        if (s >= 0) {
+            atomicMin(&ft[s], t_ft[l]);
+            float row[VDP];
+#pragma unroll
+            for (int q = 0; q < VDP; ++q) row[q] = t_row[l * VDP + q];
+            atomic_add_row<VDP>(vals + (size_t)s * VDP, row);
+        }
+        t_ft[l] = s >= 0 ? sg.slot_base + (uint32_t)s : 0xFFFFFFFFu;   // now the global slot
+    }
+    if (!a.rec_slot) return;
+    __syncthreads();
+
+    // Phase C: the replay record, from each entry's local slot
+#pragma unroll 1
+    for (int k = 0; k < kTilePixels / kTileThreads; ++k) {
+        const uint32_t p = threadIdx.x + (uint32_t)k * kTileThreads;
+        const uint32_t px = x0 + p % sg.tile_w, py = y0 + p / sg.tile_w;
+        if (px >= W || py >= H) continue;
+        const uint32_t gi = sg.point_base + (f * H + py) * W + px;
+#pragma unroll
+        for (int r = 0; r <= D; ++r) {
+            const uint32_t l = t_loc[r * kTilePixels + p];
+            if (l != 0xFFFFu) a.rec_slot[(size_t)r * a.n_total + gi] = t_ft[l];
+        }
     }
 }
 
@@ -681,8 +901,16 @@ __global__ void __launch_bounds__(kSliceThreads, slice_min_blocks(D)) slice_kern
     __shared__ Segment sg;
     const int kseg = segment_of_block(a.segs, a.nseg, blockIdx.x);
     load_segment(a.segs + kseg, sg);
-    const uint32_t i = (blockIdx.x - sg.block_base) * (uint32_t)kSliceThreads + threadIdx.x;
-    if (i >= sg.n) return;
+    // a block is a slice_tw x slice_th tile of one frame: neighbouring pixels gather the
+    // same vertex rows, which then come from L1
+    const uint32_t b = blockIdx.x - sg.block_base;
+    const uint32_t per_frame = sg.stiles_x * sg.stiles_y;
+    const uint32_t fr = b / per_frame, bt = b - fr * per_frame;
+    const uint32_t ty = bt / sg.stiles_x, tx = bt - ty * sg.stiles_x;
+    const uint32_t px = tx * sg.slice_tw + threadIdx.x % sg.slice_tw;
+    const uint32_t py = ty * sg.slice_th + threadIdx.x / sg.slice_tw;
+    if (px >= (uint32_t)sg.src.width || py >= (uint32_t)sg.src.height) return;
+    const uint32_t i = (fr * (uint32_t)sg.src.height + py) * (uint32_t)sg.src.width + px;
     unsigned* status = a.seg_status + kseg;
     // A splat that overflowed the table is rerun by the host with more slots; its
     // output may be the caller's input image (in-place filtering), so write nothing.

@@ -16,6 +16,12 @@ inline int accum_bytes(int payload) { return payload == kPayloadF64 ? 8 : 4; }
 // kernels whose code depends on the number of position dimensions d
 struct DimOps {
     bool (*splat)(const SplatArgs&, int vdp, int payload, cudaStream_t);
+    // the tile splat over the segments with tile_w > 0 (a.tile_blocks blocks); false when
+    // this d or payload has no tile splat (multi-word keys, FP64 accumulators)
+    bool (*splat_tile)(const SplatArgs&, int vdp, int payload, cudaStream_t);
+    // one-time per-device set-up of the tile splat's kernels (their shared-memory limit);
+    // called outside any stream capture, before the first launch
+    bool (*prepare)();
     void (*neighbours)(const NbrArgs&, uint32_t vmax, int sms, cudaStream_t);
     bool (*slice)(const SliceArgs&, int vdp, int payload, bool homog, cudaStream_t);
 };
@@ -29,6 +35,12 @@ PGPU_DECLARE_DIM(13) PGPU_DECLARE_DIM(14) PGPU_DECLARE_DIM(15) PGPU_DECLARE_DIM(
 #undef PGPU_DECLARE_DIM
 
 const DimOps* dim_ops(int d);
+
+// Launch geometry of one segment (its src, the splat points, and slice_src, the points
+// sliced, are set): the direct-splat blocks or, when `tiled`, the tile-splat tiles, and
+// the slice tiles.  Returns the blocks of each launch through *splat, *tile and *slice.
+void segment_geometry(Segment& s, const PointSource& slice_src, bool tiled, uint32_t* splat,
+                      uint32_t* tile, uint32_t* slice);
 
 void launch_mark(const uint32_t* ft, uint32_t cap, uint32_t* bitmap, int sms, cudaStream_t st);
 // per-segment vertex counts from the first-touch bitmap and its prefix popcount

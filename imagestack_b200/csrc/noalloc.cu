@@ -170,6 +170,8 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     seg.out.normalize = 1;
     seg.n = n;
     seg.cap = cap;
+    uint32_t splat_blocks = 0, tile_blocks = 0, slice_blocks = 0;
+    segment_geometry(seg, src, false, &splat_blocks, &tile_blocks, &slice_blocks);
     const uint32_t slot_bounds[2] = {0u, cap};
     CUDA_TRY(cudaMemcpyAsync(base + kOffSeg, &seg, sizeof(seg), cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(base + kOffSlotBase, slot_bounds, sizeof(slot_bounds),
@@ -189,7 +191,8 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     sa.ft = (uint32_t*)(base + kOffFt);
     sa.rec_slot = (uint32_t*)(base + kOffRec);
     sa.seg_status = dstatus;
-    sa.blocks = (n + kSplatThreads - 1) / kSplatThreads;
+    sa.blocks = splat_blocks;
+    sa.tile_blocks = 0;
     if (!ops->splat(sa, vdp, kPayloadF32, st)) return fail(PGPU_ERR_UNSUPPORTED, "splat variant");
     CUDA_TRY(cudaGetLastError());
 
@@ -262,7 +265,7 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     sl.svals = base + kOffSval;
     sl.vd = vd;
     sl.seg_status = dstatus;
-    sl.blocks = (n + kSliceThreads - 1) / kSliceThreads;
+    sl.blocks = slice_blocks;
     if (!ops->slice(sl, vdp, kPayloadF32, false, st)) return fail(PGPU_ERR_UNSUPPORTED, "slice variant");
     CUDA_TRY(cudaGetLastError());
 

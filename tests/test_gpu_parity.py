@@ -307,3 +307,42 @@ def test_full_size_d16_gauss_transform_matches_reference_digests(gpu):
     assert float((np.abs(a - b) / scale).max()) <= RTOL_FP32
     np.testing.assert_allclose(d["splat"].astype(np.float64).sum(0), g["sum_splat"], rtol=1e-5, atol=1e-2)
     np.testing.assert_allclose(d["blur"].astype(np.float64).sum(0), g["sum_blur"], rtol=1e-5, atol=1e-2)
+
+
+@pytest.mark.parametrize("mode", ["direct", "tile"])
+def test_both_splat_kernels_bit_exact(gpu, monkeypatch, mode):
+    """The direct splat (one point per thread, global table) and the tile splat (a
+    shared-memory table per tile of points, then one global insert per distinct vertex)
+    give the same keys, vertex order and replay records, bit for bit, and the same values
+    within the FP32 tolerance (only their summation order differs)."""
+    monkeypatch.setenv("PGPU_SPLAT", mode)
+    g = golden("gt_config1_512")
+    p, v = config1_points()
+    d = gpu.lattice_dump(p, v)
+    assert d["keys"].shape[0] == int(g["vertices"])
+    assert sha(d["keys"]) == str(g["keys_sha256"])
+    assert sha(d["replay_vtx"]) == str(g["replay_vtx_sha256"])
+    assert sha(d["replay_w"]) == str(g["replay_w_sha256"])
+    assert rel_err(d["out"][g["rows"]], g["out_rows"]) <= RTOL_FP32
+    check_dump(gpu.lattice_dump(golden("lattice_rgb_d5")["pos"], golden("lattice_rgb_d5")["val"]),
+               golden("lattice_rgb_d5"))
+
+
+@pytest.mark.parametrize("mode", ["direct", "tile"])
+@pytest.mark.parametrize("w,h,c,ss,sr", [
+    (333, 217, 3, 6.0, 0.1),    # tiles cut by both image edges
+    (1000, 31, 1, 4.0, 0.2),    # fewer rows than a tile
+    (17, 700, 3, 3.0, 0.15),    # narrower than a tile row
+    (640, 480, 3, 2.0, 0.05),   # a sparse lattice: the tile tables overflow into the global one
+])
+def test_both_splat_kernels_match_the_oracle_on_images(gpu, monkeypatch, mode, w, h, c, ss, sr):
+    """Bilateral filtering of images whose sizes do not divide into tiles, by each splat
+    kernel, against the C oracle."""
+    monkeypatch.setenv("PGPU_SPLAT", mode)
+    img = synth.image(w, h, c, rects=12, seed=w + h)
+    out = img.copy()
+    gpu.Bilateral.apply(out, ss, ss, 0.0, sr)
+    pos, val = oracle.bilateral_points(img, img, ss, sr)
+    ref = oracle.oracle_lattice(pos, val).out
+    norm = (ref[:, :c] / ref[:, c:c + 1]).reshape(h, w, c).transpose(2, 0, 1)
+    assert rel_err(out, norm) <= RTOL_FP32
