@@ -68,7 +68,7 @@ void Engine::shutdown() {
     hmeta = nullptr;
     hmeta_bytes = 0;
     for (DevBuf* b : {&key0, &keyn, &tvals, &ft, &slot2vtx, &bitmap, &offs, &partials, &vkey0, &vkeyn,
-                      &vv0, &vv1, &nbr, &vf32, &vtx2slot, &sval, &rec, &grid, &tags, &dstat, &meta, &img_a, &img_b,
+                      &vv0, &vv1, &nbr, &vf32, &vtx2slot, &sval, &rec, &grid, &tags, &vlist, &dstat, &meta, &img_a, &img_b,
                       &img_c, &img_d})
         b->release();
 }
@@ -146,6 +146,10 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     // 25.8 -> 20.5 ms).
     const bool use_tags = kw > 1;
     const bool graph = B.use_graph && !dumps;
+    // Vertices are numbered in the reference's first-insertion order only for parity dumps
+    // (first touches, a bitmap and its prefix popcount); otherwise in the order the splat
+    // created them, which gives the same filtered values with less work.
+    const bool exact_order = dumps;
 
     // points and first-touch entries, lattice after lattice
     uint64_t n_total = 0, ns_total = 0;
@@ -250,10 +254,13 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         if (cap_total > 0x7FFFFF00ull) return fail(PGPU_ERR_CAPACITY, "batch needs more than 2^31 hash slots");
 
         if ((rc = E.key0.ensure(cap_total * 16)) || (rc = E.keyn.ensure((kw - 1) * cap_total * 16)) ||
-            (rc = E.tvals.ensure(cap_total * vdp * accb)) || (rc = E.ft.ensure(cap_total * 4)) ||
-            (rc = E.slot2vtx.ensure(cap_total * 4)) || (rc = E.bitmap.ensure((size_t)nwords * 4)) ||
-            (rc = E.offs.ensure((size_t)nwords * 4)) ||
-            (rc = E.partials.ensure((size_t)scan_parts(nwords) * 4 + 16)) ||
+            (rc = E.tvals.ensure(cap_total * vdp * accb)) ||
+            (rc = E.slot2vtx.ensure(cap_total * 4)) ||
+            (exact_order && (rc = E.ft.ensure(cap_total * 4))) ||
+            (exact_order && (rc = E.bitmap.ensure((size_t)nwords * 4))) ||
+            (exact_order && (rc = E.offs.ensure((size_t)nwords * 4))) ||
+            (exact_order && (rc = E.partials.ensure((size_t)scan_parts(nwords) * 4 + 16))) ||
+            (!exact_order && (rc = E.vlist.ensure(cap_total * 4))) ||
             (rc = E.vkey0.ensure(cap_total * 16)) || (rc = E.vkeyn.ensure((kw - 1) * cap_total * 16)) ||
             (rc = E.vv0.ensure(cap_total * vdp * payb)) || (rc = E.vv1.ensure(cap_total * vdp * payb)) ||
             (rc = E.nbr.ensure((size_t)(d + 1) * cap_total * 8)) ||
@@ -292,8 +299,10 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             CUDA_TRY(cudaMemsetAsync(dmeta, 0, L.slotbase, st));
             CUDA_TRY(cudaMemsetAsync(E.key0.p, 0xFF, cap_total * 16, st));
             CUDA_TRY(cudaMemsetAsync(E.tvals.p, 0, cap_total * vdp * accb, st));
-            CUDA_TRY(cudaMemsetAsync(E.ft.p, 0xFF, cap_total * 4, st));
-            CUDA_TRY(cudaMemsetAsync(E.bitmap.p, 0, (size_t)nwords * 4, st));
+            if (exact_order) {
+                CUDA_TRY(cudaMemsetAsync(E.ft.p, 0xFF, cap_total * 4, st));
+                CUDA_TRY(cudaMemsetAsync(E.bitmap.p, 0, (size_t)nwords * 4, st));
+            }
             if (use_tags) CUDA_TRY(cudaMemsetAsync(E.tags.p, 0, cap_total, st));
             if (timed) CUDA_TRY(cudaEventRecord(E.ev[0], st));
 
@@ -306,7 +315,10 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             sa.keyn = (uint4*)E.keyn.p;
             sa.cap_total = (uint32_t)cap_total;
             sa.vals = E.tvals.p;
-            sa.ft = (uint32_t*)E.ft.p;
+            sa.ft = exact_order ? (uint32_t*)E.ft.p : nullptr;
+            sa.vlist = exact_order ? nullptr : (uint32_t*)E.vlist.p;
+            sa.vcount = dM;
+            sa.seg_counts = (uint32_t*)(dmeta + L.counts);
             sa.rec_slot = B.replay ? (uint32_t*)E.rec.p : nullptr;
             sa.seg_status = (unsigned*)(dmeta + L.segstat);
             sa.blocks = (uint32_t)blocks;
@@ -317,12 +329,14 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             CUDA_TRY(cudaGetLastError());
             if (timed) CUDA_TRY(cudaEventRecord(E.ev[1], st));
 
-            launch_mark((const uint32_t*)E.ft.p, (uint32_t)cap_total, (uint32_t*)E.bitmap.p, E.sms, st);
-            launch_scan((const uint32_t*)E.bitmap.p, nwords, (uint32_t*)E.partials.p,
-                        (uint32_t*)E.offs.p, dM, st);
-            launch_segment_counts((const uint32_t*)E.bitmap.p, (const uint32_t*)E.offs.p, nwords, dM,
-                                  (const uint32_t*)(dmeta + L.entry), nseg,
-                                  (uint32_t*)(dmeta + L.counts), st);
+            if (exact_order) {
+                launch_mark((const uint32_t*)E.ft.p, (uint32_t)cap_total, (uint32_t*)E.bitmap.p, E.sms, st);
+                launch_scan((const uint32_t*)E.bitmap.p, nwords, (uint32_t*)E.partials.p,
+                            (uint32_t*)E.offs.p, dM, st);
+                launch_segment_counts((const uint32_t*)E.bitmap.p, (const uint32_t*)E.offs.p, nwords, dM,
+                                      (const uint32_t*)(dmeta + L.entry), nseg,
+                                      (uint32_t*)(dmeta + L.counts), st);
+            }
             CompactArgs ca;
             memset(&ca, 0, sizeof(ca));
             ca.table = TableView{(uint4*)E.key0.p, (uint4*)E.keyn.p, (uint32_t)cap_total, (uint32_t)cap_total};
@@ -339,6 +353,8 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             ca.vvals = homog ? E.vf32.p : E.vv0.p;
             ca.wc = vd - 1;
             ca.tags = use_tags ? (uint8_t*)E.tags.p : nullptr;
+            ca.vlist = exact_order ? nullptr : (const uint32_t*)E.vlist.p;
+            ca.nverts = dM;
             if (!launch_assign(ca, kw, vdp, B.payload, homog, E.sms, st))
                 return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
             CUDA_TRY(cudaGetLastError());

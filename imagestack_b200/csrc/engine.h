@@ -63,6 +63,7 @@ struct Engine {
     DevBuf rec;        // slot of every (point, remainder), [r][n], recorded by the splat
     DevBuf grid;       // the dense grid of the grid method
     DevBuf tags;       // one tag byte per hash slot (compaction -> neighbour lookups)
+    DevBuf vlist;      // slots in the order the splat created them (the vertex list)
     DevBuf dstat;
     // batch metadata: statuses, counts, segment tables (device copy of hmeta)
     DevBuf meta;

@@ -131,9 +131,9 @@ void segment_geometry(Segment& s, const PointSource& slice_src, bool tiled, uint
     const uint32_t W = (uint32_t)s.src.width, H = (uint32_t)s.src.height, F = (uint32_t)s.src.frames;
     const uint64_t n = (uint64_t)W * H * F;
     if (tiled) {
-        // rows of 32 pixels (a warp) stacked into 32x32 tiles; a point list (one row) in
-        // runs of kTilePixels
-        s.tile_w = (H == 1 && F == 1) ? (uint32_t)kTilePixels : std::min<uint32_t>(32u, pow2_at_least(W));
+        // 16x16 tiles (a warp is two rows of 16 pixels); a point list (one row) in runs
+        // of kTilePixels
+        s.tile_w = (H == 1 && F == 1) ? (uint32_t)kTilePixels : std::min<uint32_t>(16u, pow2_at_least(W));
         s.tile_h = (uint32_t)kTilePixels / s.tile_w;
         s.tiles_x = (W + s.tile_w - 1) / s.tile_w;
         s.tiles_y = (H + s.tile_h - 1) / s.tile_h;
@@ -205,7 +205,10 @@ void launch_scan(const uint32_t* bitmap, uint32_t nwords, uint32_t* partials, ui
 
 template <int KW, int VDP, typename Acc, typename P, bool HOMOG>
 static void assign_t(const CompactArgs& a, int sms, cudaStream_t st) {
-    assign_kernel<KW, VDP, Acc, P, HOMOG><<<grid_for(a.table.cap, 256, sms), 256, 0, st>>>(a);
+    if (a.vlist)
+        assign_list_kernel<KW, VDP, Acc, P, HOMOG><<<grid_for(a.table.cap, 256, sms), 256, 0, st>>>(a);
+    else
+        assign_kernel<KW, VDP, Acc, P, HOMOG><<<grid_for(a.table.cap, 256, sms), 256, 0, st>>>(a);
 }
 
 template <int KW, int VDP>

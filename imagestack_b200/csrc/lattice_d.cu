@@ -84,22 +84,20 @@ void neighbours(const NbrArgs& a, uint32_t vmax, int sms, cudaStream_t st) {
     neighbours_kernel<D><<<grid_cap(vmax, 256, sms), 256, 0, st>>>(a);
 }
 
-template <int VDP, typename A, bool HOMOG>
+template <int VDP, typename A>
 void slice_t(const SliceArgs& a, cudaStream_t st) {
-    if (a.blocks) slice_kernel<D, VDP, A, HOMOG><<<a.blocks, kSliceThreads, 0, st>>>(a);
+    if (a.blocks) slice_kernel<D, VDP, A><<<a.blocks, kSliceThreads, 0, st>>>(a);
 }
 
-// the slice reads the last blur pass's rows: FP64 for the FP64 lattice, FP32 otherwise;
-// homogeneous rows exist only for the 16-bit payloads
+// the slice reads the last blur pass's rows, plain (not homogeneous) products: FP64 for
+// the FP64 lattice, FP32 otherwise; homogeneous lattices exist only for 16-bit payloads
 template <int VDP>
 bool slice_p(const SliceArgs& a, int payload, bool homog, cudaStream_t st) {
     switch (payload) {
-    case kPayloadF32: slice_t<VDP, float, false>(a, st); return !homog;
+    case kPayloadF32: slice_t<VDP, float>(a, st); return !homog;
     case kPayloadF16:
-    case kPayloadBF16:
-        homog ? slice_t<VDP, float, true>(a, st) : slice_t<VDP, float, false>(a, st);
-        return true;
-    case kPayloadF64: slice_t<VDP, double, false>(a, st); return !homog;
+    case kPayloadBF16: slice_t<VDP, float>(a, st); return true;
+    case kPayloadF64: slice_t<VDP, double>(a, st); return !homog;
     }
     return false;
 }

@@ -143,10 +143,11 @@ __device__ __forceinline__ uint32_t home_slot(uint32_t h, uint32_t cap) { return
 
 // Insert-or-find during the splat, starting at slot `home` whose word 0 the caller has
 // already loaded into `first` (so the loads of several keys can be in flight at once);
-// returns the slot or -1 (status bit set).
+// returns the slot or -1 (status bit set).  *inserted, when given, is set when this call
+// created the slot.
 template <int KW>
 __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home, uint4 first,
-                            unsigned* status) {
+                            unsigned* status, bool* inserted = nullptr) {
     const uint4 empty = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
     uint32_t s = home;
     for (int probe = 0; probe < kMaxProbe; ++probe) {
@@ -157,6 +158,7 @@ __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home,
             uint4 desired = (KW == 1) ? k.w[0] : with_state(k.w[0], kStatePending);
             w = atomicCAS(&t.key0[s], empty, desired);
             if (is_empty_word(w)) {
+                if (inserted) *inserted = true;
                 if (KW > 1) {
 #pragma unroll
                     for (int i = 1; i < KW; ++i) __stcg(&t.keyn[(size_t)(i - 1) * t.stride + s], k.w[i]);

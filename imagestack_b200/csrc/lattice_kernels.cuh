@@ -129,12 +129,50 @@ struct SplatArgs {
     uint4* keyn;
     uint32_t cap_total;
     void* vals;            // cap_total * VDP accumulators (float or double), zeroed
-    uint32_t* ft;          // cap_total first-touch entries, all ones
+    uint32_t* ft;          // cap_total first-touch entries, all ones; null: not tracked
     uint32_t* rec_slot;    // optional [r][n_total] slot of every (point, remainder)
     unsigned* seg_status;  // one status word per segment
     uint32_t blocks;       // direct splat blocks of the batch
     uint32_t tile_blocks;  // tile splat blocks of the batch
+    // optional vertex list: every slot the splat creates is appended to vlist (vcount
+    // entries, zeroed), and counted in its segment's seg_counts entry (zeroed)
+    uint32_t* vlist;
+    uint32_t* vcount;
+    uint32_t* seg_counts;
 };
+
+// Appends of one block to the batch's vertex list: slots go to the block's shared-memory
+// list first; after a barrier one thread reserves the block's range of the global list
+// with one atomic (and adds the count to the segment's), and the block copies its slots.
+// A block that creates more than kBlockListCap slots appends the rest one by one.
+constexpr uint32_t kBlockListCap = 512;
+struct BlockList {
+    uint32_t* slots;   // shared memory, kBlockListCap entries
+    uint32_t* count;   // shared memory, zeroed before the block's first append
+    uint32_t* base;    // shared memory
+};
+__device__ __forceinline__ void block_list_append(const BlockList& L, const SplatArgs& a, int kseg,
+                                                  uint32_t slot) {
+    const uint32_t j = atomicAdd(L.count, 1u);
+    if (j < kBlockListCap) {
+        L.slots[j] = slot;
+    } else {
+        a.vlist[atomicAdd(a.vcount, 1u)] = slot;
+        atomicAdd(a.seg_counts + kseg, 1u);
+    }
+}
+// called by the whole block, after a barrier that follows the last append
+__device__ __forceinline__ void block_list_flush(const BlockList& L, const SplatArgs& a, int kseg) {
+    const uint32_t n = min(*L.count, kBlockListCap);
+    if (n == 0) return;
+    if (threadIdx.x == 0) {
+        *L.base = atomicAdd(a.vcount, n);
+        atomicAdd(a.seg_counts + kseg, n);
+    }
+    __syncthreads();
+    const uint32_t base = *L.base;
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) a.vlist[base + j] = L.slots[j];
+}
 
 struct CompactArgs {
     TableView table;
@@ -151,6 +189,8 @@ struct CompactArgs {
     void* vvals;           // vertex values (payload type)
     int wc;                // homogeneous weight channel (homogeneous rows only)
     uint8_t* tags = nullptr;   // optional slot tags (zeroed), written for occupied slots
+    const uint32_t* vlist = nullptr;    // the splat's vertex list (list order), or null:
+    const uint32_t* nverts = nullptr;   // first-touch order through ft and the bitmap
 };
 
 struct NbrArgs {
@@ -318,15 +358,18 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
     __shared__ float s_delta[(D + 1) * kSplatThreads];
     __shared__ unsigned char s_coord[(D + 1) * kSplatThreads];
     __shared__ uint4 s_key[kKeysInSmem ? (D + 1) * kSplatThreads : 1];
+    __shared__ uint32_t s_new[kBlockListCap];   // slots this block created
+    __shared__ uint32_t s_new_count, s_new_base;
     __shared__ Segment sg;
     const int kseg = segment_by<&Segment::splat_base>(a.segs, a.nseg, blockIdx.x);
+    if (threadIdx.x == 0) s_new_count = 0;
     load_segment(a.segs + kseg, sg);
+    const BlockList blist{s_new, &s_new_count, &s_new_base};
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t i = (blockIdx.x - sg.splat_base) * (uint32_t)kSplatThreads + threadIdx.x;
     const bool valid = i < sg.n;
     const unsigned active = __ballot_sync(0xFFFFFFFFu, valid);
-    if (!valid) return;
-
+    if (valid) {
     unsigned* status = a.seg_status + kseg;
     const TableView table{a.key0 + sg.slot_base, a.keyn + sg.slot_base, sg.cap, a.cap_total};
     float p[D], v[VDP];
@@ -337,7 +380,7 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
     const uint32_t gi = sg.point_base + i;   // point number in the batch
     const uint32_t e0 = gi * (uint32_t)(D + 1);
     Acc* vals = reinterpret_cast<Acc*>(a.vals) + (size_t)sg.slot_base * VDP;
-    uint32_t* ft = a.ft + sg.slot_base;
+    uint32_t* ft = a.ft ? a.ft + sg.slot_base : nullptr;
 
     // Phase 1: group the lanes that share each vertex key: lanes with equal hashes,
     // confirmed against the group leader's key (a hash collision inside the warp falls
@@ -405,60 +448,110 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
                 pack_key<D>(kc, kr);
             }
             const uint4 w0 = kAhead ? first[r] : __ldcg(&table.key0[home[r]]);
-            s = table_insert<KW>(table, kr, home[r], w0, status);
-            if (s >= 0) atomicMin(&ft[s], e0 + (uint32_t)r);
+            bool created = false;
+            s = table_insert<KW>(table, kr, home[r], w0, status, &created);
+            if (s >= 0 && ft) atomicMin(&ft[s], e0 + (uint32_t)r);
+            if (created && a.vlist) block_list_append(blist, a, kseg, sg.slot_base + (uint32_t)s);
         }
         s = __shfl_sync(active, s, leader);
         if (s >= 0) atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
         if (a.rec_slot)
             a.rec_slot[(size_t)r * a.n_total + gi] = s >= 0 ? sg.slot_base + (uint32_t)s : 0xFFFFFFFFu;
     }
+    }
+    if (!a.vlist) return;
+    __syncthreads();
+    block_list_flush(blist, a, kseg);
 }
 
 // ---------------------------------------------------------------------------------
 // tile splat: one block per 2D tile of kTilePixels pixels of one frame
 // ---------------------------------------------------------------------------------
-// Neighbouring pixels land on the same lattice vertices: on the 4K d=5 bilateral a 32x32
-// tile's 6144 (point, remainder) entries touch about 370 distinct vertices, while a
-// direct splat's block of 256 consecutive pixels of a row touches 470 of 1536.  The tile
-// splat therefore inserts and sums every entry into a hash table of the block's own in
-// shared memory (phase A), then adds each distinct vertex to the global table once: one
-// insert, one row reduction and one first-touch minimum per (tile, vertex) instead of one
-// row reduction per (point, remainder) (phase B), and finally writes the replay record
-// from the shared-memory slot of each entry (phase C).  A shared-memory slot's first
-// touch is the smallest entry that reached it, so the global minimum over tiles is the
-// reference's first insertion as before; the vertex set, keys and records are the same as
-// the direct splat's, only the order of the FP32 additions differs.  An entry whose probe
-// finds no free local slot within kTileProbe goes straight to the global table, as in the
-// direct splat, so no tile can overflow.  One-word keys only (d <= 7), FP32 accumulators.
+// Neighbouring pixels land on the same lattice vertices (on the 4K d=5 bilateral a 16x16
+// tile's 1536 (point, remainder) entries touch about 155 distinct vertices), while the
+// direct splat pays one dependent probe of the global table, a trip to L2 or DRAM, per
+// lane group.  The tile splat resolves every entry's key in a hash table of the block's
+// own in shared memory instead (phase A), inserts each distinct vertex of the tile into
+// the global table once (phase B), and then every lane adds its rows to the global slots
+// with fire-and-forget vector reductions and writes its replay record (phase C).  A local
+// slot's first touch is the smallest entry that reached it, so the global minimum over
+// tiles is the reference's first insertion; the vertex set, keys and records equal the
+// direct splat's, only the order of the FP32 additions differs.  An entry whose probe finds
+// no free local slot within kTileProbe goes to the global table directly, so no tile can
+// overflow.  One-word keys (d <= 7), FP32 accumulators.
 constexpr int kTileThreads = 256;
-constexpr int kTilePixels = 1024;       // 4 pixels per thread
+constexpr int kTilePixels = 256;        // one pixel per thread
 constexpr int kTileSlots = 1024;        // shared-memory hash slots per block
 constexpr int kTileProbe = 64;
-__host__ __device__ constexpr int tile_min_blocks(int d) { return d <= 5 ? 3 : 2; }
-
-// dynamic shared memory of a tile splat block: keys, rows, first touches (then global
-// slots), the local slot of every (pixel, remainder), the simplex scratch
-__host__ __device__ constexpr size_t tile_smem_bytes(int d, int vdp) {
-    return (size_t)kTileSlots * 16 + (size_t)kTileSlots * vdp * 4 + (size_t)kTileSlots * 4 +
-           (size_t)(d + 1) * kTilePixels * 2 + (size_t)(d + 1) * kTileThreads * 4 +
-           (size_t)(d + 1) * kTileThreads + 16;
+#ifndef PGPU_TILE_MIN_BLOCKS_D5
+#define PGPU_TILE_MIN_BLOCKS_D5 5
+#endif
+__host__ __device__ constexpr int tile_min_blocks(int d) {
+    return d <= 5 ? PGPU_TILE_MIN_BLOCKS_D5 : d <= 6 ? 4 : 3;
 }
 
-// find-or-insert of a one-word key in the block's table; -1 when no slot within the probe
-// limit is free (the caller then uses the global table)
-__device__ __forceinline__ int tile_insert(uint4* t_key, const uint4& k, uint32_t h) {
+// dynamic shared memory of a tile splat block: keys, first touches (then global slots),
+// the list of occupied slots, the slots the block creates, and the simplex scratch
+__host__ __device__ constexpr size_t tile_smem_bytes(int d, int vdp) {
+    return (size_t)kTileSlots * 16 + (size_t)kTileSlots * 4 + (size_t)kTileSlots * 2 +
+           (size_t)kBlockListCap * 4 + (size_t)(d + 1) * kTileThreads * 4 + (size_t)(d + 1) * kTileThreads +
+           16 + 0 * (size_t)vdp;
+}
+
+// find-or-insert of a one-word key in the block's table; a new key's slot is appended to
+// the block's list of occupied slots.  -1 when no slot within the probe limit is free (the
+// caller then uses the global table).
+__device__ __forceinline__ int tile_insert(uint4* t_key, uint16_t* t_list, uint32_t* t_count,
+                                           const uint4& k, uint32_t h) {
     const uint4 empty = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
-    uint32_t l = h >> (32 - 10);   // kTileSlots == 1024
     static_assert(kTileSlots == 1024, "home slot uses the top 10 hash bits");
+    uint32_t l = h >> (32 - 10);
 #pragma unroll 1
     for (int probe = 0; probe < kTileProbe; ++probe) {
         uint4 w = t_key[l];
-        if (is_empty_word(w)) w = atomicCAS_block(&t_key[l], empty, k);
-        if (is_empty_word(w) || words_equal(w, k)) return (int)l;
+        if (is_empty_word(w)) {
+            w = atomicCAS_block(&t_key[l], empty, k);
+            if (is_empty_word(w)) {
+                t_list[atomicAdd(t_count, 1u)] = (uint16_t)l;
+                return (int)l;
+            }
+        }
+        if (words_equal(w, k)) return (int)l;
         l = (l + 1) & (kTileSlots - 1);
     }
     return -1;
+}
+
+// point (x, y, t) of a source: positions and values as load_point
+template <int D, int VDP>
+__device__ __forceinline__ void load_point_xyt(const PointSource& s, uint32_t x, uint32_t y, uint32_t t,
+                                               float (&p)[D], float (&v)[VDP]) {
+    const long long off_p = (long long)t * s.pos.tstride + (long long)y * s.pos.ystride + x;
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+        if (k < s.pos_channels)
+            p[k] = __fmul_rn(__ldg(s.pos.base + off_p + (long long)k * s.pos.cstride), s.pos_scale[k]);
+    int c = s.pos_channels;
+    if (s.coord_mask & 1) { float f = __fmul_rn((float)x, s.coord_scale[0]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    if (s.coord_mask & 2) { float f = __fmul_rn((float)y, s.coord_scale[1]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    if (s.coord_mask & 4) { float f = __fmul_rn((float)t, s.coord_scale[2]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    const long long off_v = (long long)t * s.val.tstride + (long long)y * s.val.ystride + x;
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) {
+        float f = 0.0f;
+        if (k < s.val_channels) f = __ldg(s.val.base + off_v + (long long)k * s.val.cstride);
+        else if (k == s.val_channels && s.homogeneous) f = 1.0f;
+        v[k] = f;
+    }
 }
 
 template <int D, int VDP>
@@ -466,153 +559,109 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
     static_assert(key_words(D) == 1, "the tile splat handles one-word keys (d <= 7)");
     extern __shared__ __align__(16) unsigned char tile_smem[];
     uint4* t_key = reinterpret_cast<uint4*>(tile_smem);
-    float* t_row = reinterpret_cast<float*>(t_key + kTileSlots);
-    uint32_t* t_ft = reinterpret_cast<uint32_t*>(t_row + kTileSlots * VDP);
-    uint16_t* t_loc = reinterpret_cast<uint16_t*>(t_ft + kTileSlots);
-    float* s_delta = reinterpret_cast<float*>(t_loc + (D + 1) * kTilePixels);
+    uint32_t* t_ft = reinterpret_cast<uint32_t*>(t_key + kTileSlots);
+    uint16_t* t_list = reinterpret_cast<uint16_t*>(t_ft + kTileSlots);
+    uint32_t* s_new = reinterpret_cast<uint32_t*>(t_list + kTileSlots);
+    float* s_delta = reinterpret_cast<float*>(s_new + kBlockListCap);
     unsigned char* s_coord = reinterpret_cast<unsigned char*>(s_delta + (D + 1) * kTileThreads);
     __shared__ Segment sg;
+    __shared__ uint32_t t_count, s_new_count, s_new_base;
     const int kseg = segment_by<&Segment::tile_base>(a.segs, a.nseg, blockIdx.x);
     for (int l = threadIdx.x; l < kTileSlots; l += kTileThreads) {
         t_key[l] = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
         t_ft[l] = 0xFFFFFFFFu;
-#pragma unroll
-        for (int k = 0; k < VDP; ++k) t_row[l * VDP + k] = 0.0f;
     }
+    if (threadIdx.x == 0) t_count = 0, s_new_count = 0;
     load_segment(a.segs + kseg, sg);   // ends with a barrier
+    const BlockList blist{s_new, &s_new_count, &s_new_base};
 
     unsigned* status = a.seg_status + kseg;
     const TableView table{a.key0 + sg.slot_base, a.keyn + sg.slot_base, sg.cap, a.cap_total};
     float* vals = reinterpret_cast<float*>(a.vals) + (size_t)sg.slot_base * VDP;
-    uint32_t* ft = a.ft + sg.slot_base;
+    uint32_t* ft = a.ft ? a.ft + sg.slot_base : nullptr;
     const uint32_t b = blockIdx.x - sg.tile_base;
     const uint32_t per_frame = sg.tiles_x * sg.tiles_y;
     const uint32_t f = b / per_frame, bt = b - f * per_frame;
     const uint32_t ty = bt / sg.tiles_x, tx = bt - ty * sg.tiles_x;
-    const uint32_t x0 = tx * sg.tile_w, y0 = ty * sg.tile_h;
+    const uint32_t px = tx * sg.tile_w + threadIdx.x % sg.tile_w;
+    const uint32_t py = ty * sg.tile_h + threadIdx.x / sg.tile_w;
     const uint32_t W = (uint32_t)sg.src.width, H = (uint32_t)sg.src.height;
-    const unsigned lane = threadIdx.x & 31u;
+    const bool valid = px < W && py < H;
     const SimplexScratch scr{s_delta + threadIdx.x, s_coord + threadIdx.x, kTileThreads};
 
-    // Phase A: every entry into the block's table.  Lanes of a warp are consecutive pixels
-    // of one tile row (ascending point numbers), grouped by key as in the direct splat; the
-    // group's leader inserts and records the first touch, every lane adds its own row.
-#pragma unroll 1
-    for (int k = 0; k < kTilePixels / kTileThreads; ++k) {
-        const uint32_t p = threadIdx.x + (uint32_t)k * kTileThreads;
-        const uint32_t px = x0 + p % sg.tile_w, py = y0 + p / sg.tile_w;
-        const bool valid = px < W && py < H;
-        const unsigned active = __ballot_sync(0xFFFFFFFFu, valid);
-        if (valid) {
-            const uint32_t i = (f * H + py) * W + px;
-            float pp[D], v[VDP];
-            load_point<D, VDP>(sg.src, i, pp, v);
-            Simplex<D> sx;
-            compute_simplex<D>(pp, a.lc, sx, status, scr);
-            const uint32_t gi = sg.point_base + i;
-            const uint32_t e0 = gi * (uint32_t)(D + 1);
-            Key<1> key;
-            first_key<D>(sx, key);
+    // Phase A: this pixel's simplex and the local slot of each of its d+1 vertices.
+    // loc[r] >= 0: local slot; -1: not placed; <= -2: global slot -(loc + 2), taken directly
+    // because the local table was full around the key.
+    float v[VDP];
+    float bary[D + 1];
+    int loc[D + 1];
+    uint32_t gi = 0;
 #pragma unroll
-            for (int r = 0; r <= D; ++r) {
-                if (r > 0) key_step<D>(key, scr.coord[(D - (r - 1)) * scr.stride]);
-                const uint32_t hk = key_hash<1>(key);
-                unsigned pr = __match_any_sync(active, hk);
-                {
-                    const unsigned ld = __ffs(pr) - 1;
-                    bool same = __shfl_sync(active, key.w[0].x, ld) == key.w[0].x;
-                    same &= __shfl_sync(active, key.w[0].y, ld) == key.w[0].y;
-                    same &= __shfl_sync(active, key.w[0].z, ld) == key.w[0].z;
-                    same &= __shfl_sync(active, key.w[0].w, ld) == key.w[0].w;
-                    if (!__all_sync(active, same)) {
-                        pr = __match_any_sync(active, ((unsigned long long)key.w[0].y << 32) | key.w[0].x);
-                        pr &= __match_any_sync(active, ((unsigned long long)key.w[0].w << 32) | key.w[0].z);
-                    }
-                }
-                const unsigned leader = __ffs(pr) - 1;
-                int l = -1;
-                if (lane == leader) {
-                    l = tile_insert(t_key, key.w[0], hk);
-                    if (l >= 0) atomicMin(&t_ft[l], e0 + (uint32_t)r);
-                }
-                l = __shfl_sync(active, l, leader);
-                float c[VDP];
+    for (int r = 0; r <= D; ++r) loc[r] = -1;
+    if (valid) {
+        float pp[D];
+        load_point_xyt<D, VDP>(sg.src, px, py, f, pp, v);
+        Simplex<D> sx;
+        compute_simplex<D>(pp, a.lc, sx, status, scr);
+        gi = sg.point_base + (f * H + py) * W + px;
+        const uint32_t e0 = gi * (uint32_t)(D + 1);
+        Key<1> key;
+        first_key<D>(sx, key);
 #pragma unroll
-                for (int q = 0; q < VDP; ++q) c[q] = __fmul_rn(sx.bary[r], v[q]);
-                if (l >= 0) {
-#pragma unroll
-                    for (int q = 0; q < VDP; ++q) atomicAdd(&t_row[l * VDP + q], c[q]);
-                    t_loc[r * kTilePixels + p] = (uint16_t)l;
-                } else {
-                    // the block's table is full around this key: the global table directly
-                    int s = -1;
-                    if (lane == leader) {
-                        const uint32_t home = home_slot(hk, table.cap);
-                        s = table_insert<1>(table, key, home, __ldcg(&table.key0[home]), status);
-                        if (s >= 0) atomicMin(&ft[s], e0 + (uint32_t)r);
-                    }
-                    s = __shfl_sync(pr, s, leader);
-                    if (s >= 0) atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
-                    if (a.rec_slot)
-                        a.rec_slot[(size_t)r * a.n_total + gi] =
-                            s >= 0 ? sg.slot_base + (uint32_t)s : 0xFFFFFFFFu;
-                    t_loc[r * kTilePixels + p] = 0xFFFFu;
+        for (int r = 0; r <= D; ++r) {
+            if (r > 0) key_step<D>(key, scr.coord[(D - (r - 1)) * scr.stride]);
+            bary[r] = sx.bary[r];
+            const uint32_t hk = key_hash<1>(key);
+            const int l = tile_insert(t_key, t_list, &t_count, key.w[0], hk);
+            if (l >= 0) {
+                if (ft) atomicMin(&t_ft[l], e0 + (uint32_t)r);
+                loc[r] = l;
+            } else {
+                const uint32_t home = home_slot(hk, table.cap);
+                bool created = false;
+                const int s = table_insert<1>(table, key, home, __ldcg(&table.key0[home]), status, &created);
+                if (s >= 0) {
+                    if (ft) atomicMin(&ft[s], e0 + (uint32_t)r);
+                    if (created && a.vlist) block_list_append(blist, a, kseg, sg.slot_base + (uint32_t)s);
+                    loc[r] = -(s + 2);
                 }
             }
         }
-        __syncwarp();
     }
     __syncthreads();
 
-    // Phase B: each distinct vertex of the tile into the global table once; the home-slot
-    // loads of all of a thread's occupied local slots are issued before any is resolved.
-    constexpr int kPer = kTileSlots / kTileThreads;
-    uint4 kw[kPer];
-    uint32_t home[kPer];
-    uint4 first[kPer];
-#pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-        kw[j] = t_key[threadIdx.x + j * kTileThreads];
-        home[j] = 0;
-        first[j] = make_uint4(0u, 0u, 0u, 0u);
-        if (!is_empty_word(kw[j])) {
-            Key<1> kk;
-            kk.w[0] = kw[j];
-            home[j] = home_slot(key_hash<1>(kk), table.cap);
-            first[j] = __ldcg(&table.key0[home[j]]);
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-        const int l = threadIdx.x + j * kTileThreads;
-        if (is_empty_word(kw[j])) continue;
-        Key<1> kk;
-        kk.w[0] = kw[j];
-        const int s = table_insert<1>(table, kk, home[j], first[j], status);
-        if (s >= 0) {
-            atomicMin(&ft[s], t_ft[l]);
-            float row[VDP];
-#pragma unroll
-            for (int q = 0; q < VDP; ++q) row[q] = t_row[l * VDP + q];
-            atomic_add_row<VDP>(vals + (size_t)s * VDP, row);
-        }
-        t_ft[l] = s >= 0 ? sg.slot_base + (uint32_t)s : 0xFFFFFFFFu;   // now the global slot
-    }
-    if (!a.rec_slot) return;
-    __syncthreads();
-
-    // Phase C: the replay record, from each entry's local slot
+    // Phase B: each distinct vertex of the tile (the list of occupied local slots) into the
+    // global table once
+    const uint32_t count = t_count;
 #pragma unroll 1
-    for (int k = 0; k < kTilePixels / kTileThreads; ++k) {
-        const uint32_t p = threadIdx.x + (uint32_t)k * kTileThreads;
-        const uint32_t px = x0 + p % sg.tile_w, py = y0 + p / sg.tile_w;
-        if (px >= W || py >= H) continue;
-        const uint32_t gi = sg.point_base + (f * H + py) * W + px;
+    for (uint32_t j = threadIdx.x; j < count; j += kTileThreads) {
+        const int l = t_list[j];
+        Key<1> kk;
+        kk.w[0] = t_key[l];
+        const uint32_t h = home_slot(key_hash<1>(kk), table.cap);
+        bool created = false;
+        const int s = table_insert<1>(table, kk, h, __ldcg(&table.key0[h]), status, &created);
+        if (s >= 0 && ft) atomicMin(&ft[s], t_ft[l]);
+        if (created && a.vlist) block_list_append(blist, a, kseg, sg.slot_base + (uint32_t)s);
+        t_ft[l] = s >= 0 ? (uint32_t)s : 0xFFFFFFFFu;   // now the global slot (segment-relative)
+    }
+    __syncthreads();
+    if (a.vlist) block_list_flush(blist, a, kseg);
+
+    // Phase C: every lane's rows into its vertices' global rows, and the replay record
+    if (!valid) return;
 #pragma unroll
-        for (int r = 0; r <= D; ++r) {
-            const uint32_t l = t_loc[r * kTilePixels + p];
-            if (l != 0xFFFFu) a.rec_slot[(size_t)r * a.n_total + gi] = t_ft[l];
+    for (int r = 0; r <= D; ++r) {
+        const int l = loc[r];
+        const uint32_t s = l >= 0 ? t_ft[l] : l <= -2 ? (uint32_t)(-(l + 2)) : 0xFFFFFFFFu;
+        if (s != 0xFFFFFFFFu) {
+            float c[VDP];
+#pragma unroll
+            for (int q = 0; q < VDP; ++q) c[q] = __fmul_rn(bary[r], v[q]);
+            atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
         }
+        if (a.rec_slot)
+            a.rec_slot[(size_t)r * a.n_total + gi] = s != 0xFFFFFFFFu ? sg.slot_base + s : 0xFFFFFFFFu;
     }
 }
 
@@ -643,53 +692,58 @@ __device__ __forceinline__ void write_tag(const CompactArgs& a, uint32_t s) {
     a.tags[s] = slot_tag(key_hash<KW>(k));
 }
 
+// vertex `vtx` of slot s: the index maps, its key and its row in vertex order
 template <int KW, int VDP, typename Acc, typename P, bool HOMOG>
-__global__ void assign_kernel(CompactArgs a) {
+__device__ __forceinline__ void assign_vertex(const CompactArgs& a, uint32_t s, uint32_t vtx) {
     const Acc* tvals = reinterpret_cast<const Acc*>(a.tvals);
     P* vvals = reinterpret_cast<P*>(a.vvals);
+    a.slot2vtx[s] = vtx;
+    a.vtx2slot[vtx] = s;
+    a.vkey0[vtx] = a.table.key0[s];
+#pragma unroll
+    for (int k = 1; k < KW; ++k)
+        a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.stride + s];
+    if (a.tags) write_tag<KW>(a, s);
     if constexpr (HOMOG) {
-        for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.table.cap;
-             s += gridDim.x * blockDim.x) {
-            const uint32_t f = a.ft[s];
-            if (f == 0xFFFFFFFFu) continue;
-            const uint32_t w = f >> 5;
-            const uint32_t vtx = a.offs[w] + __popc(a.bitmap[w] & ((1u << (f & 31u)) - 1u));
-            a.slot2vtx[s] = vtx;
-            a.vtx2slot[vtx] = s;
-            a.vkey0[vtx] = a.table.key0[s];
+        Acc wt = tvals[(size_t)s * VDP];
 #pragma unroll
-            for (int k = 1; k < KW; ++k)
-                a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.stride + s];
-            if (a.tags) write_tag<KW>(a, s);
-            Acc wt = tvals[(size_t)s * VDP];
+        for (int k = 0; k < VDP; ++k) if (k == a.wc) wt = tvals[(size_t)s * VDP + k];
 #pragma unroll
-            for (int k = 0; k < VDP; ++k) if (k == a.wc) wt = tvals[(size_t)s * VDP + k];
-#pragma unroll
-            for (int k = 0; k < VDP; ++k) {
-                const Acc t = tvals[(size_t)s * VDP + k];
-                const Acc m = (k == a.wc) ? wt : (k < a.wc && wt != (Acc)0) ? t / wt : (Acc)0;
-                Payload<P>::store(vvals + (size_t)vtx * VDP + k, m);
-            }
+        for (int k = 0; k < VDP; ++k) {
+            const Acc t = tvals[(size_t)s * VDP + k];
+            const Acc m = (k == a.wc) ? wt : (k < a.wc && wt != (Acc)0) ? t / wt : (Acc)0;
+            Payload<P>::store(vvals + (size_t)vtx * VDP + k, m);
         }
-        return;
+    } else {
+#pragma unroll
+        for (int k = 0; k < VDP; ++k)
+            Payload<P>::store(vvals + (size_t)vtx * VDP + k, tvals[(size_t)s * VDP + k]);
     }
+}
+
+// Vertices in the reference's order (parity dumps): every occupied slot's index is the
+// rank of its first touch among all first touches (the bitmap's prefix popcount).
+template <int KW, int VDP, typename Acc, typename P, bool HOMOG>
+__global__ void assign_kernel(CompactArgs a) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.table.cap;
          s += gridDim.x * blockDim.x) {
         const uint32_t f = a.ft[s];
         if (f == 0xFFFFFFFFu) continue;
         const uint32_t w = f >> 5;
         const uint32_t vtx = a.offs[w] + __popc(a.bitmap[w] & ((1u << (f & 31u)) - 1u));
-        a.slot2vtx[s] = vtx;
-        a.vtx2slot[vtx] = s;
-        a.vkey0[vtx] = a.table.key0[s];
-#pragma unroll
-        for (int k = 1; k < KW; ++k)
-            a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.stride + s];
-        if (a.tags) write_tag<KW>(a, s);
-#pragma unroll
-        for (int k = 0; k < VDP; ++k)
-            Payload<P>::store(vvals + (size_t)vtx * VDP + k, tvals[(size_t)s * VDP + k]);
+        assign_vertex<KW, VDP, Acc, P, HOMOG>(a, s, vtx);
     }
+}
+
+// Vertices in the order the splat created them (its vertex list): the filtered values do
+// not depend on how vertices are numbered, so lattices that need no dump skip the
+// first-touch bookkeeping; the list keeps tiles' vertices together, as the reference's
+// first-insertion order keeps a scanline's.
+template <int KW, int VDP, typename Acc, typename P, bool HOMOG>
+__global__ void assign_list_kernel(CompactArgs a) {
+    const uint32_t m = *a.nverts;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x)
+        assign_vertex<KW, VDP, Acc, P, HOMOG>(a, __ldg(a.vlist + v), v);
 }
 
 // ---------------------------------------------------------------------------------
@@ -876,6 +930,17 @@ __global__ void blur_kernel(BlurArgs a) {
         } else {
             blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, out);
         }
+        // The last pass writes the slice's rows; homogeneous rows (m_0.., w) go back to
+        // plain products (w*m_0.., w), so the slice is the same kernel for every payload.
+        if constexpr (HOMOG) {
+            if (a.dst_map) {
+                A w = out[0];
+#pragma unroll
+                for (int k = 0; k < VDP; ++k) if (k == a.wc) w = out[k];
+#pragma unroll
+                for (int k = 0; k < VDP; ++k) if (k < a.wc) out[k] = out[k] * w;
+            }
+        }
         const size_t row = a.dst_map ? (size_t)__ldg(a.dst_map + vtx) : (size_t)vtx;
         store_row<VDP, PD, A>(dst, row, out);
     }
@@ -893,7 +958,7 @@ __host__ __device__ constexpr int slice_min_blocks(int d) { return d <= 8 ? 6 : 
 // from the splat's record of this very point (the reference's replay slice,
 // src/Permutohedral.h:418-427); without it the keys are looked up (re-elevation slice at
 // other positions, :405-407), and a vertex the splat never created contributes zero.
-template <int D, int VDP, typename A, bool HOMOG>
+template <int D, int VDP, typename A>
 __global__ void __launch_bounds__(kSliceThreads, slice_min_blocks(D)) slice_kernel(SliceArgs a) {
     constexpr int KW = key_words(D);
     __shared__ float s_delta[(D + 1) * kSliceThreads];
@@ -936,33 +1001,13 @@ __global__ void __launch_bounds__(kSliceThreads, slice_min_blocks(D)) slice_kern
 #pragma unroll
         for (int r = 0; r <= D; ++r)
             rows[r] = __ldg(reinterpret_cast<const float4*>(sv) + (sl[r] >= 0 ? sl[r] : 0));
-        // homogeneous rows with the weight in the last lane (vd == 4, the bilateral's
-        // RGB + 1) take the weight from a fixed lane
-        const bool wlast = a.vd == VDP;
 #pragma unroll
         for (int r = 0; r <= D; ++r) {
             if (sl[r] < 0) continue;
             const float w = sx.bary[r];
             const A row[4] = {rows[r].x, rows[r].y, rows[r].z, rows[r].w};
-            if constexpr (HOMOG) {   // row (m_0.., w): accumulate (w*m_k, w)
-                if (wlast) {
-                    const A bw = (A)w * row[VDP - 1];
 #pragma unroll
-                    for (int k = 0; k < VDP - 1; ++k) acc[k] = acc_add(acc[k], bw * row[k]);
-                    acc[VDP - 1] = acc_add(acc[VDP - 1], bw);
-                    continue;
-                }
-                A wt = row[0];
-#pragma unroll
-                for (int k = 0; k < VDP; ++k) if (k == a.vd - 1) wt = row[k];
-                const A bw = (A)w * wt;
-#pragma unroll
-                for (int k = 0; k < VDP; ++k)
-                    acc[k] = acc_add(acc[k], (k == a.vd - 1) ? bw : bw * row[k]);
-            } else {
-#pragma unroll
-                for (int k = 0; k < VDP; ++k) acc[k] = acc_add(acc[k], (A)w * row[k]);
-            }
+            for (int k = 0; k < VDP; ++k) acc[k] = acc_add(acc[k], (A)w * row[k]);
         }
     } else {
     Key<KW> key;
@@ -987,18 +1032,8 @@ __global__ void __launch_bounds__(kSliceThreads, slice_min_blocks(D)) slice_kern
             A row[VDP];
 #pragma unroll
             for (int k = 0; k < VDP; ++k) row[k] = __ldg(sv + (size_t)s * VDP + k);
-            if constexpr (HOMOG) {   // row (m_0.., w): accumulate (w*m_k, w)
-                A wt = row[0];
 #pragma unroll
-                for (int k = 0; k < VDP; ++k) if (k == a.vd - 1) wt = row[k];
-                const A bw = (A)w * wt;
-#pragma unroll
-                for (int k = 0; k < VDP; ++k)
-                    acc[k] = acc_add(acc[k], (k == a.vd - 1) ? bw : bw * row[k]);
-            } else {
-#pragma unroll
-                for (int k = 0; k < VDP; ++k) acc[k] = acc_add(acc[k], (A)w * row[k]);
-            }
+            for (int k = 0; k < VDP; ++k) acc[k] = acc_add(acc[k], (A)w * row[k]);
         }
     }
     }
@@ -1010,15 +1045,11 @@ __global__ void __launch_bounds__(kSliceThreads, slice_min_blocks(D)) slice_kern
     A wsum = acc[0];
 #pragma unroll
     for (int j = 0; j < VDP; ++j) if (j == a.vd - 1) wsum = acc[j];
-    // a 16-bit payload's result is normalised with one reciprocal (its error budget is
-    // 1e-3); FP32 and FP64 divide per channel, as src/GaussTransform.cpp:673-676 does
-    const A inv = (A)1 / wsum;
+    // normalised per channel, as src/GaussTransform.cpp:673-676 divides
 #pragma unroll
     for (int k = 0; k < VDP; ++k) {
         if (k < ov.channels) {
-            float r;
-            if (ov.normalize) r = HOMOG ? (float)(acc[k] * inv) : (float)(acc[k] / wsum);
-            else r = (float)acc[k];
+            const float r = ov.normalize ? (float)(acc[k] / wsum) : (float)acc[k];
             o[(long long)k * ov.cstride] = r;
         }
     }

@@ -193,6 +193,9 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     sa.seg_status = dstatus;
     sa.blocks = splat_blocks;
     sa.tile_blocks = 0;
+    sa.vlist = nullptr;   // vertices numbered by first touch (mark, scan, assign below)
+    sa.vcount = nullptr;
+    sa.seg_counts = nullptr;
     if (!ops->splat(sa, vdp, kPayloadF32, st)) return fail(PGPU_ERR_UNSUPPORTED, "splat variant");
     CUDA_TRY(cudaGetLastError());
 
