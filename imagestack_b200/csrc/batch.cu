@@ -68,7 +68,7 @@ void Engine::shutdown() {
     hmeta = nullptr;
     hmeta_bytes = 0;
     for (DevBuf* b : {&key0, &keyn, &tvals, &ft, &slot2vtx, &bitmap, &offs, &partials, &vkey0, &vkeyn,
-                      &vv0, &vv1, &nbr, &vf32, &vtx2slot, &sval, &rec, &grid, &tags, &vlist, &dstat, &meta, &img_a, &img_b,
+                      &vv0, &vv1, &nbr, &vf32, &vtx2slot, &sval, &rec, &recw, &grid, &tags, &vlist, &dstat, &meta, &img_a, &img_b,
                       &img_c, &img_d})
         b->release();
 }
@@ -150,6 +150,10 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     // (first touches, a bitmap and its prefix popcount); otherwise in the order the splat
     // created them, which gives the same filtered values with less work.
     const bool exact_order = dumps;
+    // The replay slice reads weights the splat recorded beside the slots, as the
+    // reference's replay does, instead of recomputing every point's simplex (parity dumps
+    // recompute them: they report the weights the slice sees).
+    const bool replay_w = B.replay && !dumps;
 
     // points and first-touch entries, lattice after lattice
     uint64_t n_total = 0, ns_total = 0;
@@ -267,7 +271,8 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             (homog && (rc = E.vf32.ensure(cap_total * vdp * 4))) ||
             (rc = E.vtx2slot.ensure(cap_total * 4)) || (rc = E.sval.ensure(cap_total * vdp * accb)) ||
             (use_tags && (rc = E.tags.ensure(cap_total))) ||
-            (B.replay && (rc = E.rec.ensure((size_t)entries * 4))))
+            (B.replay && (rc = E.rec.ensure((size_t)entries * 4))) ||
+            (replay_w && (rc = E.recw.ensure((size_t)entries * 4))))
             return rc;
 
         // per-lattice descriptors, staged in pinned memory and uploaded by the first copy
@@ -320,6 +325,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             sa.vcount = dM;
             sa.seg_counts = (uint32_t*)(dmeta + L.counts);
             sa.rec_slot = B.replay ? (uint32_t*)E.rec.p : nullptr;
+            sa.rec_w = replay_w ? (float*)E.recw.p : nullptr;
             sa.seg_status = (unsigned*)(dmeta + L.segstat);
             sa.blocks = (uint32_t)blocks;
             sa.tile_blocks = (uint32_t)tile_blocks;
@@ -355,6 +361,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             ca.tags = use_tags ? (uint8_t*)E.tags.p : nullptr;
             ca.vlist = exact_order ? nullptr : (const uint32_t*)E.vlist.p;
             ca.nverts = dM;
+            ca.index_in_key = index_in_key(d) ? 1 : 0;   // the neighbour lookups expect it
             if (!launch_assign(ca, kw, vdp, B.payload, homog, E.sms, st))
                 return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
             CUDA_TRY(cudaGetLastError());
@@ -414,6 +421,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             sl.cap_total = (uint32_t)cap_total;
             sl.slot2vtx = (const uint32_t*)E.slot2vtx.p;
             sl.rec_slot = B.replay ? (const uint32_t*)E.rec.p : nullptr;
+            sl.rec_w_in = replay_w ? (const float*)E.recw.p : nullptr;
             sl.svals = E.sval.p;
             sl.vd = vd;
             sl.rec_vtx = B.rec_vtx;

@@ -61,6 +61,7 @@ struct Engine {
     DevBuf vtx2slot;   // slot of each vertex
     DevBuf sval;       // filtered rows in slot space, arithmetic type, read by the slice
     DevBuf rec;        // slot of every (point, remainder), [r][n], recorded by the splat
+    DevBuf recw;       // its barycentric weight, [r][n], recorded by the splat
     DevBuf grid;       // the dense grid of the grid method
     DevBuf tags;       // one tag byte per hash slot (compaction -> neighbour lookups)
     DevBuf vlist;      // slots in the order the splat created them (the vertex list)

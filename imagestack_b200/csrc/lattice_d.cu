@@ -86,7 +86,11 @@ void neighbours(const NbrArgs& a, uint32_t vmax, int sms, cudaStream_t st) {
 
 template <int VDP, typename A>
 void slice_t(const SliceArgs& a, cudaStream_t st) {
-    if (a.blocks) slice_kernel<D, VDP, A><<<a.blocks, kSliceThreads, 0, st>>>(a);
+    if (!a.blocks) return;
+    if (a.rec_slot && a.rec_w_in && !a.rec_vtx)
+        slice_replay_kernel<D, VDP, A><<<a.blocks, kSliceThreads, 0, st>>>(a);
+    else
+        slice_kernel<D, VDP, A><<<a.blocks, kSliceThreads, 0, st>>>(a);
 }
 
 // the slice reads the last blur pass's rows, plain (not homogeneous) products: FP64 for

@@ -193,15 +193,27 @@ __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home,
     return -1;
 }
 
+// For d <= 6 a one-word key leaves lanes 6 and 7 (the state lane) free of coordinates;
+// the compaction stores the vertex's index there, so a neighbour lookup returns the index
+// with the key.  Keys are then compared on lanes 0..5 only.
+__host__ __device__ constexpr bool index_in_key(int d) { return d <= 6; }
+
+template <int D>
+__device__ __forceinline__ bool key_match(const uint4& w, const uint4& k) {
+    if constexpr (index_in_key(D)) return w.x == k.x && w.y == k.y && w.z == k.z;
+    else return key_words(D) == 1 ? words_equal(w, k) : prefix_equal(w, k);
+}
+
 // Lookup in a table that no thread modifies any more (after the splat); -1 if absent.
-template <int KW>
-__device__ __forceinline__ int table_find(const TableView& t, const Key<KW>& k, uint32_t h) {
+template <int D>
+__device__ __forceinline__ int table_find(const TableView& t, const Key<key_words(D)>& k, uint32_t h) {
+    constexpr int KW = key_words(D);
     uint32_t s = home_slot(h, t.cap);
     for (int probe = 0; probe < kMaxProbe; ++probe) {
         uint4 w = __ldg(&t.key0[s]);
         if (is_empty_word(w)) return -1;
         if (KW == 1) {
-            if (words_equal(w, k.w[0])) return (int)s;
+            if (key_match<D>(w, k.w[0])) return (int)s;
         } else if (prefix_equal(w, k.w[0])) {
             bool same = true;
 #pragma unroll
@@ -209,6 +221,20 @@ __device__ __forceinline__ int table_find(const TableView& t, const Key<KW>& k, 
                 same = same && words_equal(__ldg(&t.keyn[(size_t)(i - 1) * t.stride + s]), k.w[i]);
             if (same) return (int)s;
         }
+        s = (s + 1 == t.cap) ? 0u : s + 1;
+    }
+    return -1;
+}
+
+// The vertex index of a key after the compaction, for d <= 6 (index_in_key); -1 if absent.
+template <int D>
+__device__ __forceinline__ int table_find_index(const TableView& t, const Key<1>& k, uint32_t h) {
+    static_assert(index_in_key(D), "the vertex index lives in the key word for d <= 6 only");
+    uint32_t s = home_slot(h, t.cap);
+    for (int probe = 0; probe < kMaxProbe; ++probe) {
+        const uint4 w = __ldg(&t.key0[s]);
+        if (is_empty_word(w)) return -1;
+        if (key_match<D>(w, k.w[0])) return (int)w.w;
         s = (s + 1 == t.cap) ? 0u : s + 1;
     }
     return -1;

@@ -131,6 +131,7 @@ struct SplatArgs {
     void* vals;            // cap_total * VDP accumulators (float or double), zeroed
     uint32_t* ft;          // cap_total first-touch entries, all ones; null: not tracked
     uint32_t* rec_slot;    // optional [r][n_total] slot of every (point, remainder)
+    float* rec_w;          // optional [r][n_total] barycentric weight of every (point, remainder)
     unsigned* seg_status;  // one status word per segment
     uint32_t blocks;       // direct splat blocks of the batch
     uint32_t tile_blocks;  // tile splat blocks of the batch
@@ -191,6 +192,7 @@ struct CompactArgs {
     uint8_t* tags = nullptr;   // optional slot tags (zeroed), written for occupied slots
     const uint32_t* vlist = nullptr;    // the splat's vertex list (list order), or null:
     const uint32_t* nverts = nullptr;   // first-touch order through ft and the bitmap
+    int index_in_key = 0;   // store each vertex's index in its key word (d <= 6)
 };
 
 struct NbrArgs {
@@ -233,6 +235,7 @@ struct SliceArgs {
     uint32_t cap_total;
     const uint32_t* slot2vtx;   // parity dumps only
     const uint32_t* rec_slot;   // slots recorded by the splat, [r][n_total]; null: look up
+    const float* rec_w_in;      // weights recorded by the splat, [r][n_total] (replay gather)
     const void* svals;          // filtered rows in slot space (float, or double)
     int vd;
     int* rec_vtx;               // optional (point, remainder) vertex indices (dumps)
@@ -457,6 +460,7 @@ __global__ void __launch_bounds__(kSplatThreads, splat_min_blocks(D)) splat_kern
         if (s >= 0) atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
         if (a.rec_slot)
             a.rec_slot[(size_t)r * a.n_total + gi] = s >= 0 ? sg.slot_base + (uint32_t)s : 0xFFFFFFFFu;
+        if (a.rec_w) a.rec_w[(size_t)r * a.n_total + gi] = sx.bary[r];
     }
     }
     if (!a.vlist) return;
@@ -662,6 +666,7 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
         }
         if (a.rec_slot)
             a.rec_slot[(size_t)r * a.n_total + gi] = s != 0xFFFFFFFFu ? sg.slot_base + s : 0xFFFFFFFFu;
+        if (a.rec_w) a.rec_w[(size_t)r * a.n_total + gi] = bary[r];
     }
 }
 
@@ -699,7 +704,9 @@ __device__ __forceinline__ void assign_vertex(const CompactArgs& a, uint32_t s, 
     P* vvals = reinterpret_cast<P*>(a.vvals);
     a.slot2vtx[s] = vtx;
     a.vtx2slot[vtx] = s;
-    a.vkey0[vtx] = a.table.key0[s];
+    const uint4 k0 = a.table.key0[s];
+    a.vkey0[vtx] = k0;
+    if (KW == 1 && a.index_in_key) a.table.key0[s] = make_uint4(k0.x, k0.y, k0.z, vtx);
 #pragma unroll
     for (int k = 1; k < KW; ++k)
         a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.stride + s];
@@ -749,7 +756,56 @@ __global__ void assign_list_kernel(CompactArgs a) {
 // ---------------------------------------------------------------------------------
 // neighbours: n1 = key + 1 except n1[j] = key[j] - d; n2 = key - 1 except n2[j] = key[j] + d
 // (for j == d every stored coordinate moves by one), src/Permutohedral.h:446-451.
+// Both are formed in packed form: stored lanes are int16 + 0x8000 mod 2^16, so adding a
+// per-lane 16-bit step (__vadd2) wraps exactly like the reference's short keys.
 // ---------------------------------------------------------------------------------
+// the packed step of axis j (sign +1: n1, -1: n2) for word w of a d-dimensional key
+template <int D>
+__device__ __forceinline__ uint32_t axis_step(int j, int sign, int w, int h) {
+    uint32_t inc = 0;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        const int lane = 2 * h + half;
+        const int c = w == 0 ? lane : 7 + (w - 1) * 8 + lane;   // coordinate in this lane
+        const bool stored = (w == 0 ? lane < 7 : true) && c < D;
+        if (stored) {
+            const int step = sign * ((c == j) ? -D : 1);
+            inc |= ((uint32_t)(uint16_t)step) << (16 * half);
+        }
+    }
+    return inc;
+}
+
+template <int D>
+__device__ __forceinline__ void neighbour_key(const Key<key_words(D)>& k, int j, int sign,
+                                              Key<key_words(D)>& out) {
+    constexpr int KW = key_words(D);
+#pragma unroll
+    for (int w = 0; w < KW; ++w) {
+        uint4 q = k.w[w];
+        if (w == 0) q.w &= 0xFFFFu;   // a clean state lane (it may hold the vertex index)
+        out.w[w].x = __vadd2(q.x, axis_step<D>(j, sign, w, 0));
+        out.w[w].y = __vadd2(q.y, axis_step<D>(j, sign, w, 1));
+        out.w[w].z = __vadd2(q.z, axis_step<D>(j, sign, w, 2));
+        out.w[w].w = __vadd2(q.w, axis_step<D>(j, sign, w, 3));
+    }
+}
+
+template <int D>
+__device__ __forceinline__ int neighbour_index(const NbrArgs& a, const TableView& table, uint32_t base,
+                                               const Key<key_words(D)>& k) {
+    constexpr int KW = key_words(D);
+    const uint32_t h = key_hash<KW>(k);
+    if constexpr (index_in_key(D)) {
+        return table_find_index<D>(table, k, h);
+    } else {
+        // tagged lookups exist for multi-word keys only (the host sets tags for those)
+        const int s = (KW > 1 && a.tags) ? table_find_tagged<KW>(table, a.tags + base, k, h)
+                                         : table_find<D>(table, k, h);
+        return s >= 0 ? (int)__ldg(a.slot2vtx + base + s) : -1;
+    }
+}
+
 template <int D>
 __global__ void neighbours_kernel(NbrArgs a) {
     constexpr int KW = key_words(D);
@@ -757,8 +813,7 @@ __global__ void neighbours_kernel(NbrArgs a) {
     for (uint32_t vtx = blockIdx.x * blockDim.x + threadIdx.x; vtx < m;
          vtx += gridDim.x * blockDim.x) {
         // neighbours are looked up in the vertex's own lattice only
-        const uint32_t slot = __ldg(a.vtx2slot + vtx);
-        const int kseg = a.nseg > 1 ? segment_of_slot(a.seg_slot_base, a.nseg, slot) : 0;
+        const int kseg = a.nseg > 1 ? segment_of_slot(a.seg_slot_base, a.nseg, __ldg(a.vtx2slot + vtx)) : 0;
         const uint32_t base = __ldg(a.seg_slot_base + kseg);
         const TableView table{a.key0 + base, a.keyn + base, __ldg(a.seg_slot_base + kseg + 1) - base,
                               a.cap_total};
@@ -766,31 +821,14 @@ __global__ void neighbours_kernel(NbrArgs a) {
         key.w[0] = a.vkey0[vtx];
 #pragma unroll
         for (int k = 1; k < KW; ++k) key.w[k] = a.vkeyn[(size_t)(k - 1) * a.vcap + vtx];
-        int kc[D];
-        unpack_key<D>(key, kc);
-#pragma unroll 1
-        for (int j = 0; j <= D; ++j) {
-            int n1[D], n2[D];
 #pragma unroll
-            for (int c = 0; c < D; ++c) {
-                n1[c] = (int)(short)(kc[c] + ((c == j) ? -D : 1));
-                n2[c] = (int)(short)(kc[c] + ((c == j) ? D : -1));
-            }
+        for (int j = 0; j <= D; ++j) {
             Key<KW> k1, k2;
-            pack_key<D>(n1, k1);
-            pack_key<D>(n2, k2);
-            // tagged lookups exist for multi-word keys only (the host sets tags for those)
-            int s1, s2;
-            if (KW > 1 && a.tags) {
-                s1 = table_find_tagged<KW>(table, a.tags + base, k1, key_hash<KW>(k1));
-                s2 = table_find_tagged<KW>(table, a.tags + base, k2, key_hash<KW>(k2));
-            } else {
-                s1 = table_find<KW>(table, k1, key_hash<KW>(k1));
-                s2 = table_find<KW>(table, k2, key_hash<KW>(k2));
-            }
-            a.nbr[(size_t)j * a.vcap + vtx] =
-                make_int2(s1 >= 0 ? (int)__ldg(a.slot2vtx + base + s1) : -1,
-                          s2 >= 0 ? (int)__ldg(a.slot2vtx + base + s2) : -1);
+            neighbour_key<D>(key, j, +1, k1);
+            neighbour_key<D>(key, j, -1, k2);
+            const int u1 = neighbour_index<D>(a, table, base, k1);
+            const int u2 = neighbour_index<D>(a, table, base, k2);
+            a.nbr[(size_t)j * a.vcap + vtx] = make_int2(u1, u2);
         }
     }
 }
@@ -1020,7 +1058,7 @@ __global__ void __launch_bounds__(kSliceThreads, slice_min_blocks(D)) slice_kern
         } else {
             if (r > 0) key_step<D>(key, scr.coord[(D - (r - 1)) * scr.stride]);
             const TableView table{a.key0 + sg.slot_base, a.keyn + sg.slot_base, sg.cap, a.cap_total};
-            const int ls = table_find<KW>(table, key, key_hash<KW>(key));
+            const int ls = table_find<D>(table, key, key_hash<KW>(key));
             s = ls >= 0 ? (int)sg.slot_base + ls : -1;
         }
         const float w = sx.bary[r];
@@ -1051,6 +1089,71 @@ __global__ void __launch_bounds__(kSliceThreads, slice_min_blocks(D)) slice_kern
         if (k < ov.channels) {
             const float r = ov.normalize ? (float)(acc[k] / wsum) : (float)acc[k];
             o[(long long)k * ov.cstride] = r;
+        }
+    }
+}
+
+// Replay slice from the splat's records of slots and weights (src/Permutohedral.h:418-427:
+// the reference replays its recorded offsets and weights the same way): a gather of d+1 rows
+// per point with no simplex to recompute.  A block is a slice_tw x slice_th tile of one frame.
+template <int D, int VDP, typename A>
+__global__ void __launch_bounds__(kSliceThreads) slice_replay_kernel(SliceArgs a) {
+    __shared__ Segment sg;
+    const int kseg = segment_of_block(a.segs, a.nseg, blockIdx.x);
+    load_segment(a.segs + kseg, sg);
+    const uint32_t b = blockIdx.x - sg.block_base;
+    const uint32_t per_frame = sg.stiles_x * sg.stiles_y;
+    const uint32_t fr = b / per_frame, bt = b - fr * per_frame;
+    const uint32_t ty = bt / sg.stiles_x, tx = bt - ty * sg.stiles_x;
+    const uint32_t px = tx * sg.slice_tw + threadIdx.x % sg.slice_tw;
+    const uint32_t py = ty * sg.slice_th + threadIdx.x / sg.slice_tw;
+    const uint32_t W = (uint32_t)sg.src.width, H = (uint32_t)sg.src.height;
+    if (px >= W || py >= H) return;
+    // an image whose splat overflowed its table is rerun by the host; write nothing
+    if (__ldcg(a.seg_status + kseg) & (kStatusProbeLimit | kStatusSpinLimit | kStatusKeyRange)) return;
+    const uint32_t gi = sg.point_base + (fr * H + py) * W + px;
+    const A* sv = reinterpret_cast<const A*>(a.svals);
+    int sl[D + 1];
+    float w[D + 1];
+#pragma unroll
+    for (int r = 0; r <= D; ++r) {
+        sl[r] = (int)__ldcs(a.rec_slot + (size_t)r * a.n_total + gi);
+        w[r] = __ldcs(a.rec_w_in + (size_t)r * a.n_total + gi);
+    }
+    A acc[VDP];
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) acc[k] = (A)0;
+    if constexpr (VDP == 4 && sizeof(A) == 4) {
+        float4 rows[D + 1];
+#pragma unroll
+        for (int r = 0; r <= D; ++r)   // a point the splat could not place reads row 0, unused
+            rows[r] = __ldg(reinterpret_cast<const float4*>(sv) + (sl[r] >= 0 ? sl[r] : 0));
+#pragma unroll
+        for (int r = 0; r <= D; ++r) {
+            if (sl[r] < 0) continue;
+            acc[0] = acc_add(acc[0], w[r] * rows[r].x);
+            acc[1] = acc_add(acc[1], w[r] * rows[r].y);
+            acc[2] = acc_add(acc[2], w[r] * rows[r].z);
+            acc[3] = acc_add(acc[3], w[r] * rows[r].w);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r <= D; ++r) {
+            if (sl[r] < 0) continue;
+#pragma unroll
+            for (int k = 0; k < VDP; ++k) acc[k] = acc_add(acc[k], (A)w[r] * __ldg(sv + (size_t)sl[r] * VDP + k));
+        }
+    }
+    const OutView& ov = sg.out;
+    float* o = ov.base + (long long)fr * ov.tstride + (long long)py * ov.ystride + px;
+    A wsum = acc[0];
+#pragma unroll
+    for (int j = 0; j < VDP; ++j) if (j == a.vd - 1) wsum = acc[j];
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) {
+        if (k < ov.channels) {
+            const float r = ov.normalize ? (float)(acc[k] / wsum) : (float)acc[k];
+            __stcs(o + (long long)k * ov.cstride, r);
         }
     }
 }

@@ -193,6 +193,7 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     sa.seg_status = dstatus;
     sa.blocks = splat_blocks;
     sa.tile_blocks = 0;
+    sa.rec_w = nullptr;   // the slice recomputes the weights
     sa.vlist = nullptr;   // vertices numbered by first touch (mark, scan, assign below)
     sa.vcount = nullptr;
     sa.seg_counts = nullptr;
@@ -217,6 +218,7 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
     ca.tvals = base + kOffTvals;
     ca.vvals = base + kOffVv0;
     ca.wc = vd - 1;
+    ca.index_in_key = index_in_key(d) ? 1 : 0;   // the neighbour lookups expect it
     if (!launch_assign(ca, 1, vdp, kPayloadF32, false, sms, st))
         return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
 
