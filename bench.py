@@ -44,7 +44,7 @@ def workload(payload):
 
 
 L2_BYTES = 126 * 1024 * 1024
-KERNELS_PER_LATTICE = 9   # splat, mark, 3 scan phases, counts, assign, neighbours, slice
+KERNELS_PER_LATTICE = 4   # tile splat, list assign, neighbours, replay slice (+ the blur's)
 TUNE_TRIALS = 4           # candidate settings the batch autotuner tries per batch shape
 D = 5
 
@@ -62,9 +62,34 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def stage_bytes(N, M, d=D, C=3, p=4, vdp=4, blur_passes=3):
+    """Algorithmic bytes of each lattice stage for N points and M vertices: what each stage's
+    kernels must move as they are built, every input read once and every output written
+    once (a row is vdp values of p bytes; the splat's sums and the slice's rows are FP32).
+      splat       image N*C*4 read; replay record N*(d+1)*(4 slot + 4 weight) written;
+                  table M*(16 key + 4*vdp row) written once
+      compaction  vertex list M*4, key M*16 and row M*4*vdp read; key M*16, row M*p*vdp,
+                  both index maps M*8 and the index in the key word M*16 written
+      neighbours  key M*16 read, one table slot M*16 per lookup (2(d+1) lookups), the
+                  pairs M*8*(d+1) written
+      blur        per pass: rows M*p*vdp read and written, neighbour pairs M*8 per axis
+                  (2 axes per fused pass); the last pass writes FP32 rows M*4*vdp through
+                  the vertex->slot map M*4
+      slice       replay record N*(d+1)*8 and the FP32 rows M*4*vdp read, N*C*4 written"""
+    axes = d + 1
+    splat = N * C * 4 + N * axes * 8 + M * (16 + 4 * vdp)
+    compact = M * (4 + 16 + 4 * vdp) + M * (16 + p * vdp + 8 + 16)
+    neighbours = M * 16 + 2 * axes * M * 16 + axes * M * 8
+    per_pass_axes = axes / blur_passes
+    blur = blur_passes * (2 * M * p * vdp + per_pass_axes * M * 8) + M * (4 * vdp - p * vdp + 4)
+    slice_ = N * axes * 8 + M * 4 * vdp + N * C * 4
+    return {"splat": int(splat), "compact": int(compact), "neighbours": int(neighbours),
+            "blur": int(blur), "slice": int(slice_)}
+
+
 def ncu_traffic():
-    """Per-launch DRAM bytes of the kernels from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "ncu_traffic_4k_bilateral.txt")
+    """DRAM bytes of each stage for one 3840x2160 frame, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_bilateral_4k_frame.txt")
     out = {}
     if os.path.exists(path):
         for line in open(path):
@@ -605,22 +630,26 @@ def run_ours(args):
         plain_stages = {k: round(statistics.mean(s[k] for s in plain_stage), 4)
                         for k in ("ms_splat", "ms_compact", "ms_neighbours", "ms_blur",
                                   "ms_slice", "ms_total")}
-        # Algorithmic bytes per launch (all frames of the batch; M = measured vertices of the
-        # batch, C = 3 colour channels, Cp = 3 position source channels, vd = 4, p = payload
-        # bytes, 4 for the splat's FP32 accumulators):
-        #   splat  N*4*(Cp + C) read + M*(2d + vd*4) written (one key, one row per vertex)
-        #   blur   (d+1) * 2 * M*vd*p (each axis reads and writes the rows once)
-        #   slice  N*(d+1)*8 (replay record) + M*vd*p (rows read once) + N*4*C written
-        vd, C, Cp = 4, 3, 3
+        # Algorithmic bytes of each stage (stage_bytes: formulas that follow the kernels),
+        # for all frames of the batch and M = the measured vertices of the batch
         p = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[args.payload]
         N = FRAMES_PER_STEP * n
-        splat_bytes = N * 4 * (Cp + C) + M * (2 * D + vd * 4)
-        blur_bytes = (D + 1) * 2 * M * vd * p
-        slice_bytes = N * (D + 1) * 8 + M * vd * p + N * 4 * C
+        passes = blur_launches(D, bool(stage[-1]["blur_pairs"]))
+        sb = stage_bytes(N, M, p=p, blur_passes=passes)
+        splat_bytes = sb["splat"]
         achieved = splat_bytes / (splat_ms / 1e3) / 1e9
-        total_bytes = splat_bytes + blur_bytes + slice_bytes
+        total_bytes = sum(sb.values())
         lattice_ms = statistics.mean(s["ms_total"] for s in stage)
-        traffic = ncu_traffic().get("splat_dram_bytes")
+        traffic = ncu_traffic()
+        stage_ms_key = {"splat": "ms_splat", "compact": "ms_compact", "neighbours": "ms_neighbours",
+                        "blur": "ms_blur", "slice": "ms_slice"}
+        roofline_stages = {}
+        for k, b in sb.items():
+            ms = stages[stage_ms_key[k]]
+            ach = b / (ms / 1e3) / 1e9 if ms > 0 else None
+            roofline_stages[k] = {"bytes": b, "ms": ms, "achieved_gbs": round(ach, 1) if ach else None,
+                                  "frac": round(ach / hbm, 4) if ach else None,
+                                  "traffic_per_frame": traffic.get(k + "_dram_bytes")}
         # the splat's atomic roofline: one float4 RED per (point, remainder) against the
         # measured RED rate at scattered rows of an L2-resident table (16 MB: the L2 atomic
         # units' ceiling), and, for reference, of a table as large as the batch's
@@ -664,20 +693,23 @@ def run_ours(args):
                                     "denominator": "max(|fp64|, 1e-2 x max|fp64|)"},
             "roofline": {"kernel": "splat", "bound": "hbm", "achieved": round(achieved, 2),
                          "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4), "traffic": traffic,
+                         "frac": round(achieved / hbm, 4),
+                         "traffic": (traffic["splat_dram_bytes"] * FRAMES_PER_STEP
+                                     if "splat_dram_bytes" in traffic else None),
                          "algorithmic_bytes": splat_bytes,
-                         "note": "latency bound on L2 probes and atomics; see profiles/"},
+                         "note": "issue bound: the per-point simplex, keys and hashes, plus one "
+                                 "float4 L2 reduction per (point, vertex); see profiles/"},
             "roofline_atomics": atomics,
-            "roofline_pipeline": {"bytes": {"splat": splat_bytes, "blur": blur_bytes,
-                                            "slice": slice_bytes},
-                                  "ms": round(lattice_ms, 4),
+            "roofline_blur": dict(roofline_stages["blur"], peak=hbm, unit="GB/s"),
+            "roofline_slice": dict(roofline_stages["slice"], peak=hbm, unit="GB/s"),
+            "roofline_stages": roofline_stages,
+            "roofline_pipeline": {"bytes": sb, "ms": round(lattice_ms, 4),
                                   "achieved": round(total_bytes / (lattice_ms / 1e3) / 1e9, 2),
                                   "peak": hbm, "unit": "GB/s",
                                   "frac": round(total_bytes / (lattice_ms / 1e3) / 1e9 / hbm, 4)},
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s",
                     "h2d_bytes_per_step": px_step * 3 * 4, "d2h_bytes_per_step": px_step * 3 * 4},
-            "gpu_launches": args.steps * (KERNELS_PER_LATTICE +
-                                          blur_launches(D, bool(stage[-1]["blur_pairs"]))),
+            "gpu_launches": args.steps * (KERNELS_PER_LATTICE + passes),
             "autotuned": {"load_factor": round(stage[-1]["load_factor"], 3),
                           "blur_pairs": bool(stage[-1]["blur_pairs"])},
             "stages_ms": stages, "vertices": M, "capacity": stage[-1]["capacity"],

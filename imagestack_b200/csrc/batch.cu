@@ -385,6 +385,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             na.nverts = dM;
             na.nbr = (int2*)E.nbr.p;
             na.tags = use_tags ? (const uint8_t*)E.tags.p : nullptr;
+            na.seg_status = (const unsigned*)(dmeta + L.segstat);
             ops->neighbours(na, (uint32_t)cap_total, E.sms, st);
             CUDA_TRY(cudaGetLastError());
             if (timed) CUDA_TRY(cudaEventRecord(E.ev[3], st));

@@ -16,7 +16,7 @@
 namespace pgpu {
 
 constexpr int kMaxD = 16;      // position dimensions supported by the kernels
-constexpr int kMaxProbe = 1 << 14;
+constexpr int kMaxProbe = 1 << 12;   // a probe this long means the table is full
 constexpr int kMaxSpin = 1 << 20;
 
 // status bits written by the kernels (atomicOr into the job's status word)
@@ -151,6 +151,9 @@ __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home,
     const uint4 empty = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
     uint32_t s = home;
     for (int probe = 0; probe < kMaxProbe; ++probe) {
+        // A probe this long means a table (nearly) full: if the lattice has overflowed
+        // already, give up at once, so a table sized too small fails fast and is rerun.
+        if ((probe & 255) == 255 && (__ldcg(status) & kStatusProbeLimit)) return -1;
         uint4 w = probe == 0 ? first : __ldcg(&t.key0[s]);
         if (maybe_empty(w)) {
             // An empty slot, or a read that raced with the slot's one-time fill: the
@@ -196,7 +199,10 @@ __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home,
 // For d <= 6 a one-word key leaves lanes 6 and 7 (the state lane) free of coordinates;
 // the compaction stores the vertex's index there, so a neighbour lookup returns the index
 // with the key.  Keys are then compared on lanes 0..5 only.
-__host__ __device__ constexpr bool index_in_key(int d) { return d <= 6; }
+#ifndef PGPU_INDEX_IN_KEY_MAX_D
+#define PGPU_INDEX_IN_KEY_MAX_D 6
+#endif
+__host__ __device__ constexpr bool index_in_key(int d) { return d <= PGPU_INDEX_IN_KEY_MAX_D; }
 
 template <int D>
 __device__ __forceinline__ bool key_match(const uint4& w, const uint4& k) {

@@ -223,6 +223,7 @@ extern "C" int pgpu_bilateral_noalloc(const float* d_in, float* d_out, int width
         return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
 
     NbrArgs na;
+    na.seg_status = dstatus;
     na.key0 = key0;
     na.keyn = key0;
     na.cap_total = cap;
