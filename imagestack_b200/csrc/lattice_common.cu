@@ -128,6 +128,10 @@ static uint32_t pow2_at_least(uint32_t x) {
 
 void segment_geometry(Segment& s, const PointSource& slice_src, bool tiled, uint32_t* splat,
                       uint32_t* tile, uint32_t* slice) {
+    const PointSource& q = s.src;
+    s.src.pos_is_val = q.pos.base == q.val.base && q.pos.ystride == q.val.ystride &&
+                       q.pos.tstride == q.val.tstride && q.pos.cstride == q.val.cstride &&
+                       q.pos_channels == q.val_channels;
     const uint32_t W = (uint32_t)s.src.width, H = (uint32_t)s.src.height, F = (uint32_t)s.src.frames;
     const uint64_t n = (uint64_t)W * H * F;
     if (tiled) {

@@ -280,12 +280,6 @@ struct LatticeConsts {
     float inv_d1;      // 1.0f/(d+1), computed on the host
 };
 
-// gcc on x86-64 converts float to short through a 32-bit cvttss2si, which yields
-// INT_MIN for NaN and out-of-range values; the result is then truncated to 16 bits.
-__device__ __forceinline__ int x86_float_to_int(float f) {
-    return (fabsf(f) < 2147483648.0f) ? __float2int_rz(f) : (int)0x80000000;
-}
-
 template <int D>
 struct Simplex {
     int g[D + 1];      // greedy[] after the hyperplane correction (int16 values)
@@ -322,11 +316,16 @@ __device__ __forceinline__ void compute_simplex(const float (&p)[D], const Latti
 #pragma unroll
     for (int i = 0; i <= D; ++i) {
         float v = __fmul_rn(e[i], scale);
-        float up = __fmul_rn(ceilf(v), dp1);
+        // ceilf(v)*(d+1) is floorf(v)*(d+1) + (d+1) exactly (small integers times d+1)
+        // unless v is an integer, where the reference's up == down; then down + (d+1) is
+        // never the nearer one, so the pick is the same down
         float down = __fmul_rn(floorf(v), dp1);
+        float up = __fadd_rn(down, dp1);
         float pick = (__fsub_rn(up, e[i]) < __fsub_rn(e[i], down)) ? up : down;
         out_of_range |= !(fabsf(pick) <= 32767.0f);
-        int gi = (int)(short)x86_float_to_int(pick);
+        // in range the reference's conversion (float -> int -> short) is the plain
+        // truncating one; out of range the call fails (flagged below)
+        int gi = __float2int_rz(pick);
         sx.g[i] = gi;
         sum += gi;
     }

@@ -47,6 +47,7 @@ struct PointSource {
     PlanarView val;
     int val_channels;
     int homogeneous;
+    int pos_is_val;            // the position channels are the value channels (bilateral)
 };
 
 struct OutView {
@@ -534,11 +535,32 @@ __device__ __forceinline__ int tile_insert(uint4* t_key, uint16_t* t_list, uint3
 template <int D, int VDP>
 __device__ __forceinline__ void load_point_xyt(const PointSource& s, uint32_t x, uint32_t y, uint32_t t,
                                                float (&p)[D], float (&v)[VDP]) {
-    const long long off_p = (long long)t * s.pos.tstride + (long long)y * s.pos.ystride + x;
+    const long long off_v = (long long)t * s.val.tstride + (long long)y * s.val.ystride + x;
+    if (s.pos_is_val) {   // one load per channel: the bilateral's guide is its image
 #pragma unroll
-    for (int k = 0; k < D; ++k)
-        if (k < s.pos_channels)
-            p[k] = __fmul_rn(__ldg(s.pos.base + off_p + (long long)k * s.pos.cstride), s.pos_scale[k]);
+        for (int k = 0; k < VDP; ++k) {
+            float f = 0.0f;
+            if (k < s.val_channels) f = __ldg(s.val.base + off_v + (long long)k * s.val.cstride);
+            else if (k == s.val_channels && s.homogeneous) f = 1.0f;
+            v[k] = f;
+        }
+#pragma unroll
+        for (int k = 0; k < D && k < VDP; ++k)
+            if (k < s.pos_channels) p[k] = __fmul_rn(v[k], s.pos_scale[k]);
+    } else {
+        const long long off_p = (long long)t * s.pos.tstride + (long long)y * s.pos.ystride + x;
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+            if (k < s.pos_channels)
+                p[k] = __fmul_rn(__ldg(s.pos.base + off_p + (long long)k * s.pos.cstride), s.pos_scale[k]);
+#pragma unroll
+        for (int k = 0; k < VDP; ++k) {
+            float f = 0.0f;
+            if (k < s.val_channels) f = __ldg(s.val.base + off_v + (long long)k * s.val.cstride);
+            else if (k == s.val_channels && s.homogeneous) f = 1.0f;
+            v[k] = f;
+        }
+    }
     int c = s.pos_channels;
     if (s.coord_mask & 1) { float f = __fmul_rn((float)x, s.coord_scale[0]);
 #pragma unroll
@@ -552,14 +574,6 @@ __device__ __forceinline__ void load_point_xyt(const PointSource& s, uint32_t x,
 #pragma unroll
         for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
         ++c; }
-    const long long off_v = (long long)t * s.val.tstride + (long long)y * s.val.ystride + x;
-#pragma unroll
-    for (int k = 0; k < VDP; ++k) {
-        float f = 0.0f;
-        if (k < s.val_channels) f = __ldg(s.val.base + off_v + (long long)k * s.val.cstride);
-        else if (k == s.val_channels && s.homogeneous) f = 1.0f;
-        v[k] = f;
-    }
 }
 
 template <int D, int VDP>
