@@ -443,7 +443,43 @@ def mixed_batch(ib, synth, torch, dev, steps):
             "max_rel_err_fp16_vs_fp64": err}
 
 
-def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0, workers=2, max_batch=32):
+def served_saturation(ib, synth, torch, count=4000, workers=2, max_batch=32):
+    """The server at saturation: `count` requests of the served stream's mix (24 pooled
+    images, bilateral RGB and grey joint bilateral, sides 64..2048) submitted at once."""
+    import numpy as np
+    sides = synth.log_uniform_int(SEED, 31, 48, 64, 2048)
+    rng = np.random.default_rng(SEED + 1)
+    pool = []
+    for k in range(24):
+        w, h = int(sides[2 * k]), int(sides[2 * k + 1])
+        rgb = synth.image(w, h, 3, rects=8, seed=700 + k)
+        if k % 2 == 0:
+            img, ref, kind = torch.from_numpy(rgb).pin_memory(), None, ib.REQ_BILATERAL
+        else:
+            img = torch.from_numpy(synth.luminance(rgb)).pin_memory()
+            ref = torch.from_numpy(synth.luminance(synth.image(w, h, 3, rects=8, seed=900 + k))).pin_memory()
+            kind = ib.REQ_JOINT_BILATERAL
+        pool.append((kind, img.numpy(), None if ref is None else ref.numpy(),
+                     torch.empty_like(img).pin_memory().numpy(),
+                     float(4 + 28 * rng.random()), float(0.05 + 0.25 * rng.random())))
+    with ib.Server(workers=workers, max_batch=max_batch, payload="fp16", memory_budget=40 << 30) as srv:
+        for kind, img, ref, out, ss, sr in pool:   # warm-up: every shape once
+            srv.wait(srv.submit(kind, img, out, ref=ref, filter_width=ss, color_sigma=sr))
+        srv.reset_stats()
+        tickets = []
+        for j in range(count):
+            kind, img, ref, out, ss, sr = pool[j % 24]
+            tickets.append(srv.submit(kind, img, out, ref=ref, filter_width=ss, color_sigma=sr))
+        for t in tickets:
+            srv.wait(t)
+        st = srv.stats()
+    return {"requests": int(st["completed"]), "failed": int(st["failed"]),
+            "throughput_req_s": round(st["req_per_s"], 1), "throughput_mpix_s": round(st["mpix_per_s"], 1),
+            "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2), "workers": workers,
+            "note": "every request of the same pooled image writes the same output buffer"}
+
+
+def served_stream(ib, synth, torch, seconds=60.0, rate0=50.0, rate1=2000.0, workers=2, max_batch=32):
     """The served stream: Poisson arrivals ramped rate0 -> rate1 req/s over `seconds`;
     half bilateral RGB (d=5), half joint bilateral of a grey image on a grey guide (d=3);
     sides log-uniform 64..2048, sigmas as the mixed batch; FP16 payload, 40 GB budget.
@@ -511,19 +547,6 @@ def served_stream(ib, synth, torch, seconds=6.0, rate0=50.0, rate1=2000.0, worke
             "max_ms": round(st["max_ms"], 3), "throughput_mpix_s": round(st["mpix_per_s"], 2),
             "throughput_req_s": round(st["req_per_s"], 1), "batches": int(st["batches"]),
             "payload": "fp16", "workers": workers, "max_batch": max_batch, "memory_budget_gib": 40}
-
-
-def served_stream_fresh():
-    """The served stream in a process of its own, so that it starts from a clean device
-    (no workspaces, graphs or pool state left by the batch measurements)."""
-    code = ("import sys,json; sys.path.insert(0,%r); import torch; import bench; "
-            "import imagestack_b200 as ib; from imagestack_b200 import synth; "
-            "print(json.dumps(bench.served_stream(ib, synth, torch)))" % ROOT)
-    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
-    try:
-        return json.loads(r.stdout.strip().splitlines()[-1])
-    except Exception:
-        return {"error": (r.stderr or r.stdout)[-300:]}
 
 
 def run_ours(args):
@@ -722,7 +745,8 @@ def run_ours(args):
             line["gauss_transform_d16"] = gauss_transform_d16(ib, synth, torch, dev)
         if world == 1 and not args.quick:
             line["mixed_batch"] = mixed_batch(ib, synth, torch, dev, steps=6)
-            line["served"] = served_stream_fresh()
+            line["served"] = served_stream(ib, synth, torch)
+            line["served_saturation"] = served_saturation(ib, synth, torch)
             line["p50_ms"] = line["served"]["p50_ms"]
             line["p99_ms"] = line["served"]["p99_ms"]
         if world == 1 and not args.no_cpu_baseline:

@@ -47,6 +47,35 @@ static thread_local cudaStream_t t_call_stream = nullptr;
 void set_call_stream(cudaStream_t st) { t_call_stream = st; }
 cudaStream_t call_stream() { return t_call_stream; }
 
+// The library's own stream-ordered memory pool of each device.  It keeps the memory that
+// buffers give back (release threshold: unlimited), so a workspace that grows under load
+// (the server's workers) is served from the pool instead of new driver allocations, and
+// the device's default pool, which the host application may use, is left as it is.
+static std::mutex g_pool_mu;
+static std::map<int, cudaMemPool_t> g_pools;
+
+static cudaMemPool_t device_pool() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) return it->second;
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pools[dev] = pool;
+    return pool;
+}
+
 // Every call is synchronous, so when a buffer grows (at the start of a call) no earlier
 // work still uses the old block, whichever stream it ran on.
 int DevBuf::ensure(size_t need) {
@@ -57,7 +86,9 @@ int DevBuf::ensure(size_t need) {
     p = nullptr;
     bytes = 0;
     const size_t nb = need + need / 2;
-    if (cudaMallocAsync(&p, nb, st) != cudaSuccess) {
+    cudaMemPool_t pool = device_pool();
+    const cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, nb, pool, st) : cudaMallocAsync(&p, nb, st);
+    if (e != cudaSuccess) {
         cudaGetLastError();
         p = nullptr;
         return fail(PGPU_ERR_MEMORY, "device allocation of %zu bytes failed", nb);

@@ -61,10 +61,6 @@ public:
     size_t worker_cap = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    // One worker's lattices on the device at a time: overlapping lattices of several
-    // workers compete for L2 and run slower together than one after the other.  Uploads
-    // and downloads of the other workers overlap them.
-    std::mutex device_mu;
     std::deque<Req*> queue;
     std::unordered_map<long long, Req*> reqs;
     std::vector<std::thread> threads;
@@ -217,11 +213,9 @@ public:
             }
             it.n = q->n;
         }
-        CUDA_TRY(cudaStreamSynchronize(st));   // this batch's uploads, outside the device lock
-        {
-            std::lock_guard<std::mutex> dev(device_mu);
-            if ((rc = run_batch(E, B, st))) return rc;
-        }
+        // The lattices follow the uploads on this worker's stream; the other workers'
+        // copies and lattices run on theirs at the same time.
+        if ((rc = run_batch(E, B, st))) return rc;
         for (size_t k = 0; k < batch.size(); ++k)
             if ((rc = copy_view(dout[k], batch[k]->r.out, batch[k]->out_channels, cudaMemcpyDeviceToHost, st)))
                 return rc;
