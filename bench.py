@@ -45,7 +45,7 @@ def workload(payload):
 
 L2_BYTES = 126 * 1024 * 1024
 KERNELS_PER_LATTICE = 4   # tile splat, list assign, neighbours, replay slice (+ the blur's)
-TUNE_TRIALS = 4           # candidate settings the batch autotuner tries per batch shape
+TUNE_TRIALS = 5           # candidate settings the batch autotuner tries per batch shape
 D = 5
 
 
@@ -734,7 +734,10 @@ def run_ours(args):
                     "h2d_bytes_per_step": px_step * 3 * 4, "d2h_bytes_per_step": px_step * 3 * 4},
             "gpu_launches": args.steps * (KERNELS_PER_LATTICE + passes),
             "autotuned": {"load_factor": round(stage[-1]["load_factor"], 3),
-                          "blur_pairs": bool(stage[-1]["blur_pairs"])},
+                          "blur_pairs": bool(stage[-1]["blur_pairs"]),
+                          "splat": "tile" if stage[-1]["tiled"] else "direct",
+                          "candidates": "load factor 0.5/0.35/0.7, blur axes in pairs or one "
+                                        "per pass (FP32), tile or direct splat"},
             "stages_ms": stages, "vertices": M, "capacity": stage[-1]["capacity"],
             "clocks": clk.summary(),
         }

@@ -60,7 +60,7 @@ class Stats(C.Structure):
                 ("d", C.c_int), ("vd", C.c_int), ("payload", C.c_int), ("retries", C.c_int),
                 ("ms_splat", C.c_float), ("ms_compact", C.c_float), ("ms_neighbours", C.c_float),
                 ("ms_blur", C.c_float), ("ms_slice", C.c_float), ("ms_total", C.c_float),
-                ("load_factor", C.c_float), ("blur_pairs", C.c_int)]
+                ("load_factor", C.c_float), ("blur_pairs", C.c_int), ("tiled", C.c_int)]
 
 
 from .tmpfile import load_tmp, save_tmp  # noqa: E402,F401  (ImageStack .tmp files)

@@ -211,9 +211,10 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     constexpr double kTileRatioMax = 0.8;
     const char* mode = std::getenv("PGPU_SPLAT");
     const int forced = !mode ? 0 : !strcmp(mode, "direct") ? 1 : !strcmp(mode, "tile") ? 2 : 0;
-    const bool tile_ok = kw == 1 && B.payload != kPayloadF64 && forced != 1;
+    const bool tile_ok = kw == 1 && B.payload != kPayloadF64 && forced != 1 && (forced == 2 || B.splat == 0);
     std::vector<Segment> segs(nseg), slsegs(B.replay ? 0 : nseg);
     uint64_t blocks = 0, tile_blocks = 0, slice_blocks = 0;
+    int tiled_count = 0;
     for (int k = 0; k < nseg; ++k) {
         const BatchItem& it = B.items[k];
         Segment& sgm = segs[k];
@@ -225,6 +226,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         const bool tiled = tile_ok && (forced == 2 || (density[k] <= kTileRatioMax && it.n >= 256));
         uint32_t nb_splat = 0, nb_tile = 0, nb_slice = 0;
         segment_geometry(sgm, B.replay ? it.splat : it.slice, tiled, &nb_splat, &nb_tile, &nb_slice);
+        tiled_count += tiled ? 1 : 0;
         sgm.splat_base = (uint32_t)blocks;
         sgm.tile_base = (uint32_t)tile_blocks;
         sgm.block_base = (uint32_t)slice_blocks;
@@ -445,6 +447,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
                      E.tvals.p, E.nbr.p, E.rec.p, E.meta.p, (void*)E.hmeta, E.sval.p);
             std::string gk(key);
             gk += B.blur_pairs ? ":p" : ":s";
+            gk += tile_blocks ? ":t" + std::to_string(tile_blocks) : ":d";
             for (int k = 0; k < nseg; ++k) gk += ":" + std::to_string(cap[k]) + "/" + std::to_string(B.items[k].n);
             auto it = E.graphs.find(gk);
             if (it == E.graphs.end()) {
@@ -522,6 +525,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         s.retries = pass;
         s.load_factor = load;
         s.blur_pairs = B.blur_pairs ? 1 : 0;
+        s.tiled = tiled_count;
         if (!graph) {
             cudaEventElapsedTime(&s.ms_splat, E.ev[0], E.ev[1]);
             cudaEventElapsedTime(&s.ms_compact, E.ev[1], E.ev[2]);
@@ -538,16 +542,20 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
 // Every image of a batch is filtered in place, so an image whose range overflowed cannot
 // simply be rerun with its whole batch: the others are finished.  Only the overflowed
 // ones go again, as a smaller batch with larger ranges.  The statistics cover all passes.
-// Autotuner candidates: hash-table load factor and blur pairing.  The first calls of a
-// batch shape try them in turn; later calls of the shape use the fastest by the lattice's
-// device time.  Keys, vertex order and FP32/FP64 results do not depend on the choice; a
+// Autotuner candidates: hash-table load factor, blur pairing and the splat kernel (the
+// tile splat wherever the learned vertex density allows it, or the direct splat for every
+// image).  The first calls of a batch shape try them in turn; later calls of the shape use
+// the fastest by the lattice's device time.  Keys, vertex order and FP32/FP64 results do not depend on the choice; a
 // 16-bit payload tries fused pairs only, because one axis per pass rounds its rows to 16
 // bits between axes, which the pair keeps in FP32 registers.
 struct TuneCandidate {
     float load;
     bool pairs;
+    int splat;   // BatchJob::splat
 };
-constexpr TuneCandidate kTune[] = {{0.5f, true}, {0.35f, true}, {0.7f, true}, {0.5f, false}};
+// the last candidate (one axis per pass) only for FP32/FP64 payloads
+constexpr TuneCandidate kTune[] = {{0.5f, true, 0}, {0.35f, true, 0}, {0.7f, true, 0},
+                                   {0.5f, true, 1}, {0.5f, false, 0}};
 constexpr int kTuneCount = (int)(sizeof(kTune) / sizeof(kTune[0]));
 
 static std::string tune_key(const BatchJob& B) {
@@ -569,10 +577,11 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
     if (B.autotune && !B.rec_vtx && !B.dump_splat) {
         if (E.tuning.size() > 1024) E.tuning.clear();
         tune = &E.tuning[tune_key(B)];
-        tune->count = (B.payload == kPayloadF16 || B.payload == kPayloadBF16) ? 3 : kTuneCount;
+        tune->count = (B.payload == kPayloadF16 || B.payload == kPayloadBF16) ? kTuneCount - 1 : kTuneCount;
         cand = tune->trials < tune->count ? tune->trials : tune->best;
         cur.load = kTune[cand].load;
         cur.blur_pairs = kTune[cand].pairs;
+        cur.splat = kTune[cand].splat;
     }
     std::vector<uint64_t> caps;
     pgpu_stats sum;
@@ -595,6 +604,7 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
         if (failed.empty()) {
             sum.load_factor = s.load_factor;
             sum.blur_pairs = s.blur_pairs;
+            sum.tiled = s.tiled;
             set_stats(sum);
             if (tune && tune->trials < tune->count) {
                 tune->ms[tune->trials++] = sum.ms_total;

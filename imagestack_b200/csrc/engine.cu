@@ -591,6 +591,7 @@ int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int 
                 sum.capacity = std::max(sum.capacity, s.capacity);
                 sum.d = s.d, sum.vd = s.vd, sum.payload = s.payload;
                 sum.load_factor = s.load_factor, sum.blur_pairs = s.blur_pairs;
+                sum.tiled += s.tiled;
                 sum.retries += s.retries;
                 sum.ms_splat += s.ms_splat, sum.ms_compact += s.ms_compact;
                 sum.ms_neighbours += s.ms_neighbours, sum.ms_blur += s.ms_blur;

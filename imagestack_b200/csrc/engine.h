@@ -127,6 +127,7 @@ struct BatchJob {
     bool use_graph = false;   // capture / replay the launch sequence as a CUDA graph
     bool autotune = false;    // pick load factor and blur pairing per batch shape
     bool blur_pairs = true;   // blur two axes per launch
+    int splat = 0;            // 0: the tile splat where vertices are shared, 1: direct only
     std::vector<BatchItem> items;
     // parity dumps (single-item jobs)
     int* rec_vtx = nullptr;

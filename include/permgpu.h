@@ -76,6 +76,7 @@ typedef struct pgpu_stats {
     float ms_splat, ms_compact, ms_neighbours, ms_blur, ms_slice, ms_total;
     float load_factor;     /* hash-table load factor used */
     int blur_pairs;        /* 1: blur axes fused in pairs, 0: one axis per pass */
+    int tiled;             /* images splatted by the tile splat (the others: direct) */
 } pgpu_stats;
 
 /* Fill *opt with the defaults. */
@@ -124,8 +125,9 @@ int pgpu_bilateral(pgpu_image *im, float filter_width, float filter_height,
  * opt->flags & PGPU_FLAG_AUTOTUNE lets the first calls of each batch shape (the number
  * of images, the point count to a power of two, d, the payload) try candidate settings
  * — hash-table load factor 0.5, 0.35 or 0.7, blur axes fused in pairs or (FP32/FP64
- * payloads only) one per pass — and keeps the fastest for later calls of that shape
- * (opt->load_factor is then unused); results do not depend on the choice. */
+ * payloads only) one per pass, the tile splat where it applies or the direct splat for
+ * every image — and keeps the fastest for later calls of that shape (opt->load_factor is
+ * then unused); results do not depend on the choice. */
 #define PGPU_FLAG_GRAPH 1
 #define PGPU_FLAG_AUTOTUNE 2
 int pgpu_bilateral_batch(pgpu_image *ims, int count, const float *filter_width,

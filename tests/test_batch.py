@@ -99,9 +99,9 @@ def test_batch_on_device_with_graph_replay(gpu):
 @pytest.mark.gpu
 @pytest.mark.parametrize("graph", [False, True])
 def test_autotuned_batch_tries_candidates_then_keeps_one(gpu, graph):
-    """With autotune the first four calls of a batch shape try (load factor, blur pairing)
-    candidates and later calls keep the fastest; every call's results equal the
-    single-image path."""
+    """With autotune the first five calls of a batch shape try (load factor, blur pairing,
+    splat kernel) candidates and later calls keep the fastest; every call's results equal
+    the single-image path."""
     import torch
     imgs, ss, sr = uneven_batch(10 + int(graph), seed=12)
     expect = []
@@ -110,16 +110,17 @@ def test_autotuned_batch_tries_candidates_then_keeps_one(gpu, graph):
         gpu.Bilateral.apply(e, s, s, 0.0, r)
         expect.append(e)
     seen = []
-    for call in range(6):
+    for call in range(7):
         dev = [torch.from_numpy(im.copy()).cuda() for im in imgs]
         gpu.bilateral_batch(dev, ss, sr, graph=graph, autotune=True)
         st = gpu.last_stats()
-        seen.append((round(st["load_factor"], 2), st["blur_pairs"]))
+        seen.append((round(st["load_factor"], 2), st["blur_pairs"], st["tiled"] > 0))
         torch.cuda.synchronize()
         for d, e in zip(dev, expect):
             assert rel_err(d.cpu().numpy(), e) <= RTOL_FP32
-    assert seen[:4] == [(0.5, 1), (0.35, 1), (0.7, 1), (0.5, 0)]
-    assert seen[4] == seen[5] and seen[4] in seen[:4]
+    assert [x[:2] for x in seen[:5]] == [(0.5, 1), (0.35, 1), (0.7, 1), (0.5, 1), (0.5, 0)]
+    assert seen[3][2] is False                  # the direct-splat candidate
+    assert seen[5] == seen[6] and seen[5] in seen[:5]
 
 
 @pytest.mark.gpu
@@ -130,14 +131,14 @@ def test_autotuned_fp16_batch_keeps_blur_pairs(gpu):
     ref = [im.copy() for im in imgs]
     gpu.bilateral_batch(ref, ss, sr, payload="fp64")
     seen = []
-    for call in range(5):
+    for call in range(6):
         out = [im.copy() for im in imgs]
         gpu.bilateral_batch(out, ss, sr, payload="fp16", autotune=True)
         st = gpu.last_stats()
         seen.append((round(st["load_factor"], 2), st["blur_pairs"]))
         assert max(rel_err(o, r, floor_frac=1e-2) for o, r in zip(out, ref)) <= 1e-3
     assert all(p == 1 for _, p in seen)
-    assert [l for l, _ in seen[:3]] == [0.5, 0.35, 0.7] and seen[3] == seen[4]
+    assert [l for l, _ in seen[:4]] == [0.5, 0.35, 0.7, 0.5] and seen[4] in seen[:4]
 
 
 @pytest.mark.gpu
