@@ -68,7 +68,7 @@ void Engine::shutdown() {
     hmeta = nullptr;
     hmeta_bytes = 0;
     for (DevBuf* b : {&key0, &keyn, &tvals, &ft, &slot2vtx, &bitmap, &offs, &partials, &vkey0, &vkeyn,
-                      &vv0, &vv1, &nbr, &vf32, &vtx2slot, &sval, &rec, &recw, &grid, &tags, &vlist, &dstat, &meta, &img_a, &img_b,
+                      &vv0, &vv1, &nbr, &vf32, &vtx2slot, &sval, &rec, &recw, &grid, &grid2, &tags, &vlist, &dstat, &meta, &img_a, &img_b,
                       &img_c, &img_d})
         b->release();
 }

@@ -62,7 +62,7 @@ struct Engine {
     DevBuf sval;       // filtered rows in slot space, arithmetic type, read by the slice
     DevBuf rec;        // slot of every (point, remainder), [r][n], recorded by the splat
     DevBuf recw;       // its barycentric weight, [r][n], recorded by the splat
-    DevBuf grid;       // the dense grid of the grid method
+    DevBuf grid, grid2;   // the dense grid of the grid method, and its blur's second buffer
     DevBuf tags;       // one tag byte per hash slot (compaction -> neighbour lookups)
     DevBuf vlist;      // slots in the order the splat created them (the vertex list)
     DevBuf dstat;

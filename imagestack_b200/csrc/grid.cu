@@ -9,9 +9,9 @@
 //            order-preserving integer atomics: exact in any order)
 //   splat    one thread per point; FP32 atomics into the corners (the reference adds in
 //            point order, so sums agree to rounding)
-//   blur     one launch per dimension; one thread per grid row and value channel runs the
-//            reference's in-place recurrence (src/DenseGrid.h:199-236) with its exact
-//            arithmetic, including the last cell's double-precision step
+//   blur     one launch per dimension, one thread per grid value: the reference's two
+//            in-place passes (src/DenseGrid.h:199-236) evaluated out of place, cell by cell,
+//            with their exact arithmetic, including the last cell's double-precision step
 //   slice    one thread per point; the corners gathered in the reference's order
 #include <cuda_runtime.h>
 
@@ -124,7 +124,9 @@ __device__ __forceinline__ bool grid_corner(const GridArgs& g, const int (&I)[D]
     return ok;
 }
 
-template <int D>
+// VD: value channels when they fill a vector atomic (2: grey + weight, 4: RGB + weight;
+// a cell's values are then 8- or 16-byte aligned), else 0 (one float atomic per value)
+template <int D, int VD>
 __global__ void __launch_bounds__(kGridThreads) grid_splat_kernel(PointSource src, uint32_t n, GridArgs g) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -137,41 +139,63 @@ __global__ void __launch_bounds__(kGridThreads) grid_splat_kernel(PointSource sr
         float w;
         long long off;
         if (!grid_corner<D>(g, I, F, Fi, corner, w, off)) continue;
+        if constexpr (VD == 2) {
+            atomicAdd(reinterpret_cast<float2*>(g.grid + off), make_float2(__fmul_rn(w, v[0]), __fmul_rn(w, v[1])));
+        } else if constexpr (VD == 4) {
+            atomicAdd(reinterpret_cast<float4*>(g.grid + off),
+                      make_float4(__fmul_rn(w, v[0]), __fmul_rn(w, v[1]), __fmul_rn(w, v[2]), __fmul_rn(w, v[3])));
+        } else {
 #pragma unroll
-        for (int k = 0; k < kGridMaxVd; ++k)
-            if (k < g.vd) atomicAdd(g.grid + off + k, __fmul_rn(w, v[k]));
-    }
-}
-
-// DenseGrid::blur_ (src/DenseGrid.h:186-238) along dimension j: rows x vd threads, each
-// running taps/2 in-place [1 2 1]/4 passes over its row with zero boundaries.
-__global__ void __launch_bounds__(kGridThreads) grid_blur_kernel(GridArgs g, int d, int j, long long rows) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= rows * g.vd) return;
-    const int k = (int)(t % g.vd);
-    long long rem = t / g.vd, start = k;
-    for (int i = 0; i < d; ++i) {
-        if (i == j) continue;
-        start += (rem % g.sizes[i]) * g.stride[i];
-        rem /= g.sizes[i];
-    }
-    float* row = g.grid + start;
-    const long long s = g.stride[j];
-    const int len = g.sizes[j];
-    for (int it = 0; it < kGridTaps / 2; ++it) {
-        float t1 = __fdiv_rn(row[0], 2.0f);                            // rowPtr[k]/2
-        for (int x = 0; x < len - 1; ++x) {
-            const float t2 = __fmul_rn(0.5f, __fadd_rn(row[x * s], row[(x + 1) * s]));
-            row[x * s] = __fmul_rn(0.5f, __fadd_rn(t1, t2));
-            t1 = t2;
+            for (int k = 0; k < kGridMaxVd; ++k)
+                if (k < g.vd) atomicAdd(g.grid + off + k, __fmul_rn(w, v[k]));
         }
-        // the last cell: 0.5*(tmp1 + 0.5*rowPtr[k]) evaluates in double (double literals)
-        const long long last = (long long)(len - 1) * s;
-        row[last] = (float)__dmul_rn(0.5, __dadd_rn((double)t1, __dmul_rn(0.5, (double)row[last])));
     }
 }
 
-template <int D>
+// The two [1 2 1]/4 passes of DenseGrid::blur_ (src/DenseGrid.h:186-238) along dimension j
+// (taps 5: taps/2 passes).  The reference walks each row in place, but every value a pass
+// writes depends only on values from before that pass (row[x] is overwritten after both
+// row[x] and row[x+1] were read, and the running tmp carries 0.5*(old[x-1] + old[x])), so
+// each cell is computed independently here, out of place, with the same single-precision
+// operations in the same order:
+//   x = 0:           0.5*(old[0]/2 + 0.5*(old[0] + old[1]))
+//   0 < x < len-1:   0.5*(0.5*(old[x-1] + old[x]) + 0.5*(old[x] + old[x+1]))
+//   x = len-1:       0.5*(tmp + 0.5*old[len-1]) in double (the reference's double literals),
+//                    tmp = 0.5*(old[len-2] + old[len-1]) in single, or old[0]/2 when len == 1
+// The second pass at x needs the first pass at x-1, x and x+1, which each thread evaluates
+// from the five values around x.  One thread per grid value; consecutive threads are
+// consecutive values, so every access is coalesced whatever the dimension.
+__device__ __forceinline__ float grid_pass_value(float left, float here, float right, uint32_t x, uint32_t len) {
+    const float t1 = x == 0 ? __fdiv_rn(here, 2.0f) : __fmul_rn(0.5f, __fadd_rn(left, here));
+    if (x == len - 1) return (float)__dmul_rn(0.5, __dadd_rn((double)t1, __dmul_rn(0.5, (double)here)));
+    return __fmul_rn(0.5f, __fadd_rn(t1, __fmul_rn(0.5f, __fadd_rn(here, right))));
+}
+
+__global__ void __launch_bounds__(kGridThreads) grid_blur_kernel(GridArgs g, int j, const float* src,
+                                                                 float* dst, uint32_t total) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;   // grids hold < 2^30 values
+    if (t >= total) return;
+    const uint32_t s = (uint32_t)g.stride[j];
+    const uint32_t len = (uint32_t)g.sizes[j];
+    const uint32_t x = (t / s) % len;
+    // old values at x-2 .. x+2 (those outside the row are never used)
+    float o[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int xx = (int)x + k - 2;
+        o[k] = (xx >= 0 && xx < (int)len) ? src[(int64_t)t + (int64_t)(k - 2) * s] : 0.0f;
+    }
+    // first pass at x-1, x, x+1, then the second pass at x
+    float p1[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int xx = (int)x + k - 1;
+        p1[k] = (xx >= 0 && xx < (int)len) ? grid_pass_value(o[k], o[k + 1], o[k + 2], (uint32_t)xx, len) : 0.0f;
+    }
+    dst[t] = grid_pass_value(p1[0], p1[1], p1[2], x, len);
+}
+
+template <int D, int VD>
 __global__ void __launch_bounds__(kGridThreads) grid_slice_kernel(PointSource src, uint32_t n, GridArgs g,
                                                                   OutView out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -188,9 +212,20 @@ __global__ void __launch_bounds__(kGridThreads) grid_slice_kernel(PointSource sr
         float w;
         long long off;
         if (!grid_corner<D>(g, I, F, Fi, corner, w, off)) continue;
+        float c[kGridMaxVd];
+        if constexpr (VD == 2) {
+            const float2 q = __ldg(reinterpret_cast<const float2*>(g.grid + off));
+            c[0] = q.x, c[1] = q.y;
+        } else if constexpr (VD == 4) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(g.grid + off));
+            c[0] = q.x, c[1] = q.y, c[2] = q.z, c[3] = q.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < kGridMaxVd; ++k) c[k] = k < g.vd ? g.grid[off + k] : 0.0f;
+        }
 #pragma unroll
         for (int k = 0; k < kGridMaxVd; ++k)
-            if (k < g.vd) acc[k] = __fadd_rn(acc[k], __fmul_rn(w, g.grid[off + k]));
+            if (k < g.vd) acc[k] = __fadd_rn(acc[k], __fmul_rn(w, c[k]));
     }
     const uint32_t wdt = (uint32_t)src.width, hgt = (uint32_t)src.height;
     const uint32_t x = i % wdt, q = i / wdt, y = q % hgt, t = q / hgt;
@@ -212,11 +247,19 @@ void launch_minmax(const PointSource& s, uint32_t n, float sf, unsigned* mm, int
 }
 template <int D>
 void launch_splat(const PointSource& s, uint32_t n, const GridArgs& g, cudaStream_t st) {
-    if (n) grid_splat_kernel<D><<<(n + kGridThreads - 1) / kGridThreads, kGridThreads, 0, st>>>(s, n, g);
+    if (!n) return;
+    const unsigned blocks = (n + kGridThreads - 1) / kGridThreads;
+    if (g.vd == 2) grid_splat_kernel<D, 2><<<blocks, kGridThreads, 0, st>>>(s, n, g);
+    else if (g.vd == 4) grid_splat_kernel<D, 4><<<blocks, kGridThreads, 0, st>>>(s, n, g);
+    else grid_splat_kernel<D, 0><<<blocks, kGridThreads, 0, st>>>(s, n, g);
 }
 template <int D>
 void launch_slice(const PointSource& s, uint32_t n, const GridArgs& g, const OutView& o, cudaStream_t st) {
-    if (n) grid_slice_kernel<D><<<(n + kGridThreads - 1) / kGridThreads, kGridThreads, 0, st>>>(s, n, g, o);
+    if (!n) return;
+    const unsigned blocks = (n + kGridThreads - 1) / kGridThreads;
+    if (g.vd == 2) grid_slice_kernel<D, 2><<<blocks, kGridThreads, 0, st>>>(s, n, g, o);
+    else if (g.vd == 4) grid_slice_kernel<D, 4><<<blocks, kGridThreads, 0, st>>>(s, n, g, o);
+    else grid_slice_kernel<D, 0><<<blocks, kGridThreads, 0, st>>>(s, n, g, o);
 }
 
 #define PGPU_GRID_DISPATCH(d, call)          \
@@ -270,19 +313,24 @@ int run_grid(Engine& E, const LatticeJob& J, cudaStream_t st) {
             return fail(PGPU_ERR_CAPACITY, "the grid would need more than %lld cells", kGridMaxCells);
     }
     const long long cells = g.stride[d];
-    if ((rc = E.grid.ensure((size_t)cells * sizeof(float)))) return rc;
+    if ((rc = E.grid.ensure((size_t)cells * sizeof(float))) ||
+        (rc = E.grid2.ensure((size_t)cells * sizeof(float))))
+        return rc;
     g.grid = (float*)E.grid.p;
     CUDA_TRY(cudaMemsetAsync(g.grid, 0, (size_t)cells * sizeof(float), st));
     CUDA_TRY(cudaEventRecord(E.ev[1], st));
     PGPU_GRID_DISPATCH(d, launch_splat<DD>(J.splat, J.n, g, st));
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaEventRecord(E.ev[3], st));
-    for (int j = 0; j < d; ++j) {
-        const long long rows = cells / ((long long)vd * g.sizes[j]);
-        const long long threads = rows * vd;
-        grid_blur_kernel<<<(unsigned)((threads + kGridThreads - 1) / kGridThreads), kGridThreads, 0, st>>>(
-            g, d, j, rows);
-    }
+    // one launch per dimension (both of its passes), ping-ponging between the grid and a
+    // second buffer
+    static_assert(kGridTaps / 2 == 2, "grid_blur_kernel fuses exactly two passes");
+    float* bufs[2] = {g.grid, (float*)E.grid2.p};
+    int cur = 0;
+    const unsigned blur_blocks = (unsigned)((cells + kGridThreads - 1) / kGridThreads);
+    for (int j = 0; j < d; ++j, cur ^= 1)
+        grid_blur_kernel<<<blur_blocks, kGridThreads, 0, st>>>(g, j, bufs[cur], bufs[cur ^ 1], (uint32_t)cells);
+    g.grid = bufs[cur];
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaEventRecord(E.ev[4], st));
     PGPU_GRID_DISPATCH(d, launch_slice<DD>(sl, nsl, g, J.out, st));
