@@ -237,3 +237,30 @@ def test_full_mixed_batch_matches_the_oracle_and_fp16_the_fp64_lattice(gpu):
         gpu.Bilateral.apply(ref, ss[k], ss[k], 0.0, sr[k], payload="fp64")
         torch.cuda.synchronize()
         assert rel_err(half[k].cpu().numpy(), ref.cpu().numpy(), floor_frac=1e-2) <= 1e-3, k
+
+
+@pytest.mark.gpu
+def test_host_batch_of_large_images_one_per_chunk_with_an_overflow_rerun(gpu):
+    """Images of at least 2^22 pixels are chunks of their own, each uploaded, filtered and
+    downloaded on the overlapping streams.  Every image equals the single-image path,
+    including a noisy one whose first table overflows (its shape is new, so its table size
+    is guessed) and is rerun in the middle of the pipeline.  Odd heights on purpose."""
+    import torch
+    rng = np.random.default_rng(77)
+    sizes = [(2304, 1830), (2111, 2003), (2560, 1640)]
+    imgs = [synth.image(w, h, 3, rects=12, seed=60 + k) for k, (w, h) in enumerate(sizes)]
+    imgs[1] = rng.random((3, 2003, 2111), dtype=np.float32)        # sparse: overflows once
+    ss, sr = [12.0, 2.0, 16.0], [0.1, 0.05, 0.12]
+    results = []
+    for rep in range(2):   # the first call meets the noisy image's shape for the first time
+        keep = [torch.from_numpy(im.copy()).pin_memory() for im in imgs]
+        gpu.bilateral_batch([t.numpy() for t in keep], ss, sr)
+        results.append([t.numpy().copy() for t in keep])
+    expect = []
+    for im, s, r in zip(imgs, ss, sr):
+        e = im.copy()
+        gpu.Bilateral.apply(e, s, s, 0.0, r)
+        expect.append(e)
+    for work in results:
+        for w, e in zip(work, expect):
+            assert rel_err(w, e) <= RTOL_FP32
