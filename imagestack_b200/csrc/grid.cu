@@ -105,51 +105,140 @@ __device__ __forceinline__ void grid_cell(const GridArgs& g, const float (&p)[D]
     }
 }
 
-// Corner `corner` of the cell: its weight (the reference's product order) and offset; a
-// corner past the grid's last cell has weight exactly 0 (the point lies on the last
-// plane), and is skipped.
+// The cell's base offset, and which of its upper corners lie inside the grid (bit j: the
+// corners one step up along dimension j); false if the cell itself is outside.  A corner
+// past the grid's last cell has weight exactly 0 (the point lies on the last plane) and is
+// skipped, as DenseGrid::query's bounds checks do.
 template <int D>
-__device__ __forceinline__ bool grid_corner(const GridArgs& g, const int (&I)[D], const float (&F)[D],
-                                            const float (&Fi)[D], int corner, float& w, long long& off) {
-    w = 1.0f;
-    off = 0;
+__device__ __forceinline__ bool grid_base(const GridArgs& g, const int (&I)[D], long long& base, unsigned& hi_ok) {
+    base = 0;
+    hi_ok = 0;
     bool ok = true;
 #pragma unroll
     for (int j = 0; j < D; ++j) {
-        const int ij = I[j] + ((corner >> j) & 1);
-        ok = ok && ij >= 0 && ij < g.sizes[j];
-        off += (long long)ij * g.stride[j];
-        w = __fmul_rn(w, ((corner >> j) & 1) ? F[j] : Fi[j]);
+        ok = ok && I[j] >= 0 && I[j] < g.sizes[j];
+        base += (long long)I[j] * g.stride[j];
+        if (I[j] + 1 < g.sizes[j]) hi_ok |= 1u << j;
     }
     return ok;
 }
 
-// VD: value channels when they fill a vector atomic (2: grey + weight, 4: RGB + weight;
-// a cell's values are then 8- or 16-byte aligned), else 0 (one float atomic per value)
-template <int D, int VD>
-__global__ void __launch_bounds__(kGridThreads) grid_splat_kernel(PointSource src, uint32_t n, GridArgs g) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float p[D], v[kGridMaxVd];
-    load_point<D, kGridMaxVd>(src, i, p, v);
-    int I[D];
-    float F[D], Fi[D];
-    grid_cell<D>(g, p, I, F, Fi);
-    for (int corner = 0; corner < (1 << D); ++corner) {
-        float w;
-        long long off;
-        if (!grid_corner<D>(g, I, F, Fi, corner, w, off)) continue;
-        if constexpr (VD == 2) {
-            atomicAdd(reinterpret_cast<float2*>(g.grid + off), make_float2(__fmul_rn(w, v[0]), __fmul_rn(w, v[1])));
-        } else if constexpr (VD == 4) {
-            atomicAdd(reinterpret_cast<float4*>(g.grid + off),
-                      make_float4(__fmul_rn(w, v[0]), __fmul_rn(w, v[1]), __fmul_rn(w, v[2]), __fmul_rn(w, v[3])));
+// Corner `corner` of the cell (unrolled by the caller): its weight in the reference's
+// product order and its offset from the cell's base.
+template <int D>
+__device__ __forceinline__ float grid_corner_weight(const GridArgs& g, const float (&F)[D], const float (&Fi)[D],
+                                                    int corner, long long base, long long& off) {
+    float w = 1.0f;
+    off = base;
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        const bool up = (corner >> j) & 1;
+        w = __fmul_rn(w, up ? F[j] : Fi[j]);
+        if (up) off += g.stride[j];
+    }
+    return w;
+}
+
+// Blocks of the splat and slice: tiles of (bw * kp) x (kGridThreads/bw) pixels of one frame
+// (bw = 32 for images, kGridThreads for point lists of one row; kp consecutive pixels of a
+// row per thread), so a thread finds its pixels without dividing.
+struct PixelTiles {
+    unsigned bw;
+    dim3 grid;
+};
+PixelTiles pixel_tiles(const PointSource& s, unsigned kp) {
+    PixelTiles t;
+    t.bw = s.height == 1 ? (unsigned)kGridThreads : 32u;
+    const unsigned bh = kGridThreads / t.bw, w = t.bw * kp;
+    t.grid = dim3(((unsigned)s.width + w - 1) / w, ((unsigned)s.height + bh - 1) / bh, (unsigned)s.frames);
+    return t;
+}
+
+// the splat's atomic of one corner: VD values of a cell are 8- or 16-byte aligned when VD is
+// 2 or 4, so one vector atomic adds them; otherwise one float atomic per value
+template <int VD>
+__device__ __forceinline__ void grid_add(const GridArgs& g, long long off, const float* c) {
+    if constexpr (VD == 2) {
+        atomicAdd(reinterpret_cast<float2*>(g.grid + off), make_float2(c[0], c[1]));
+    } else if constexpr (VD == 4) {
+        atomicAdd(reinterpret_cast<float4*>(g.grid + off), make_float4(c[0], c[1], c[2], c[3]));
+    } else {
+#pragma unroll
+        for (int k = 0; k < kGridMaxVd; ++k)
+            if (k < g.vd) atomicAdd(g.grid + off + k, c[k]);
+    }
+}
+
+// KP consecutive pixels of a row per thread.  With KP > 1 (small grids: the 2^D corners x
+// VD values fit in registers) a run of pixels that fall into the same cell is summed in
+// registers first and sent as one set of corner atomics: neighbouring pixels share cells,
+// and the splat is bound by the atomics' rate (4K grey d=3: 66 M float2 atomics).  The sums
+// differ from the reference's point-by-point additions only in rounding order.
+template <int D, int VD, int KP>
+__global__ void __launch_bounds__(kGridThreads) grid_splat_kernel(PointSource src, unsigned bw, GridArgs g) {
+    constexpr int NC = 1 << D;
+    constexpr int NV = VD > 0 ? VD : kGridMaxVd;
+    const uint32_t x0 = (blockIdx.x * bw + threadIdx.x % bw) * KP;
+    const uint32_t y = blockIdx.y * (kGridThreads / bw) + threadIdx.x / bw;
+    if (x0 >= (uint32_t)src.width || y >= (uint32_t)src.height) return;
+    float acc[KP > 1 ? NC : 1][NV];
+    long long run_base = -1;
+    unsigned run_hi = 0;
+    auto flush = [&]() {
+        if (run_base < 0) return;
+#pragma unroll
+        for (int corner = 0; corner < NC; ++corner) {
+            if (corner & ~run_hi) continue;
+            long long off = run_base;
+#pragma unroll
+            for (int j = 0; j < D; ++j)
+                if ((corner >> j) & 1) off += g.stride[j];
+            grid_add<VD>(g, off, acc[KP > 1 ? corner : 0]);
+        }
+    };
+#pragma unroll
+    for (int kp = 0; kp < KP; ++kp) {
+        const uint32_t x = x0 + kp;
+        if (x >= (uint32_t)src.width) break;
+        float p[D], v[kGridMaxVd];
+        load_point_xyt<D, kGridMaxVd>(src, x, y, blockIdx.z, p, v);
+        int I[D];
+        float F[D], Fi[D];
+        grid_cell<D>(g, p, I, F, Fi);
+        long long base;
+        unsigned hi_ok;
+        if (!grid_base<D>(g, I, base, hi_ok)) continue;
+        if constexpr (KP > 1) {
+            if (base != run_base) {   // a new cell: send the run so far, start a new one
+                flush();
+                run_base = base;
+                run_hi = hi_ok;
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int k = 0; k < NV; ++k) acc[c][k] = 0.0f;
+            }
+#pragma unroll
+            for (int corner = 0; corner < NC; ++corner) {
+                long long off;
+                const float w = grid_corner_weight<D>(g, F, Fi, corner, base, off);
+#pragma unroll
+                for (int k = 0; k < NV; ++k) acc[corner][k] = __fadd_rn(acc[corner][k], __fmul_rn(w, v[k]));
+            }
         } else {
 #pragma unroll
-            for (int k = 0; k < kGridMaxVd; ++k)
-                if (k < g.vd) atomicAdd(g.grid + off + k, __fmul_rn(w, v[k]));
+            for (int corner = 0; corner < NC; ++corner) {
+                if (corner & ~hi_ok) continue;
+                long long off;
+                const float w = grid_corner_weight<D>(g, F, Fi, corner, base, off);
+                float c[NV];
+#pragma unroll
+                for (int k = 0; k < NV; ++k) c[k] = __fmul_rn(w, v[k]);
+                grid_add<VD>(g, off, c);
+            }
         }
     }
+    if constexpr (KP > 1) flush();
 }
 
 // The two [1 2 1]/4 passes of DenseGrid::blur_ (src/DenseGrid.h:186-238) along dimension j
@@ -196,22 +285,27 @@ __global__ void __launch_bounds__(kGridThreads) grid_blur_kernel(GridArgs g, int
 }
 
 template <int D, int VD>
-__global__ void __launch_bounds__(kGridThreads) grid_slice_kernel(PointSource src, uint32_t n, GridArgs g,
+__global__ void __launch_bounds__(kGridThreads) grid_slice_kernel(PointSource src, unsigned bw, GridArgs g,
                                                                   OutView out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const uint32_t x = blockIdx.x * bw + threadIdx.x % bw;
+    const uint32_t y = blockIdx.y * (kGridThreads / bw) + threadIdx.x / bw;
+    if (x >= (uint32_t)src.width || y >= (uint32_t)src.height) return;
     float p[D];
-    load_position<D>(src, i, p);
+    load_position_xyt<D>(src, x, y, blockIdx.z, p);
     int I[D];
     float F[D], Fi[D];
     grid_cell<D>(g, p, I, F, Fi);
     float acc[kGridMaxVd];
 #pragma unroll
     for (int k = 0; k < kGridMaxVd; ++k) acc[k] = 0.0f;
+    long long base;
+    unsigned hi_ok;
+    const bool inside = grid_base<D>(g, I, base, hi_ok);
+#pragma unroll
     for (int corner = 0; corner < (1 << D); ++corner) {
-        float w;
+        if (!inside || (corner & ~hi_ok)) continue;
         long long off;
-        if (!grid_corner<D>(g, I, F, Fi, corner, w, off)) continue;
+        const float w = grid_corner_weight<D>(g, F, Fi, corner, base, off);
         float c[kGridMaxVd];
         if constexpr (VD == 2) {
             const float2 q = __ldg(reinterpret_cast<const float2*>(g.grid + off));
@@ -227,9 +321,7 @@ __global__ void __launch_bounds__(kGridThreads) grid_slice_kernel(PointSource sr
         for (int k = 0; k < kGridMaxVd; ++k)
             if (k < g.vd) acc[k] = __fadd_rn(acc[k], __fmul_rn(w, c[k]));
     }
-    const uint32_t wdt = (uint32_t)src.width, hgt = (uint32_t)src.height;
-    const uint32_t x = i % wdt, q = i / wdt, y = q % hgt, t = q / hgt;
-    float* o = out.base + (long long)t * out.tstride + (long long)y * out.ystride + x;
+    float* o = out.base + (long long)blockIdx.z * out.tstride + (long long)y * out.ystride + x;
     float wsum = acc[0];
 #pragma unroll
     for (int k = 0; k < kGridMaxVd; ++k) if (k == g.vd - 1) wsum = acc[k];
@@ -248,18 +340,27 @@ void launch_minmax(const PointSource& s, uint32_t n, float sf, unsigned* mm, int
 template <int D>
 void launch_splat(const PointSource& s, uint32_t n, const GridArgs& g, cudaStream_t st) {
     if (!n) return;
-    const unsigned blocks = (n + kGridThreads - 1) / kGridThreads;
-    if (g.vd == 2) grid_splat_kernel<D, 2><<<blocks, kGridThreads, 0, st>>>(s, n, g);
-    else if (g.vd == 4) grid_splat_kernel<D, 4><<<blocks, kGridThreads, 0, st>>>(s, n, g);
-    else grid_splat_kernel<D, 0><<<blocks, kGridThreads, 0, st>>>(s, n, g);
+    // runs of pixels summed in registers where the corner sums fit (2^d x vd <= 16)
+    if (g.vd == 2 && D <= 3) {
+        const PixelTiles t = pixel_tiles(s, 4);
+        grid_splat_kernel<D, 2, 4><<<t.grid, kGridThreads, 0, st>>>(s, t.bw, g);
+    } else if (g.vd == 4 && D <= 2) {
+        const PixelTiles t = pixel_tiles(s, 4);
+        grid_splat_kernel<D, 4, 4><<<t.grid, kGridThreads, 0, st>>>(s, t.bw, g);
+    } else {
+        const PixelTiles t = pixel_tiles(s, 1);
+        if (g.vd == 2) grid_splat_kernel<D, 2, 1><<<t.grid, kGridThreads, 0, st>>>(s, t.bw, g);
+        else if (g.vd == 4) grid_splat_kernel<D, 4, 1><<<t.grid, kGridThreads, 0, st>>>(s, t.bw, g);
+        else grid_splat_kernel<D, 0, 1><<<t.grid, kGridThreads, 0, st>>>(s, t.bw, g);
+    }
 }
 template <int D>
 void launch_slice(const PointSource& s, uint32_t n, const GridArgs& g, const OutView& o, cudaStream_t st) {
     if (!n) return;
-    const unsigned blocks = (n + kGridThreads - 1) / kGridThreads;
-    if (g.vd == 2) grid_slice_kernel<D, 2><<<blocks, kGridThreads, 0, st>>>(s, n, g, o);
-    else if (g.vd == 4) grid_slice_kernel<D, 4><<<blocks, kGridThreads, 0, st>>>(s, n, g, o);
-    else grid_slice_kernel<D, 0><<<blocks, kGridThreads, 0, st>>>(s, n, g, o);
+    const PixelTiles t = pixel_tiles(s, 1);
+    if (g.vd == 2) grid_slice_kernel<D, 2><<<t.grid, kGridThreads, 0, st>>>(s, t.bw, g, o);
+    else if (g.vd == 4) grid_slice_kernel<D, 4><<<t.grid, kGridThreads, 0, st>>>(s, t.bw, g, o);
+    else grid_slice_kernel<D, 0><<<t.grid, kGridThreads, 0, st>>>(s, t.bw, g, o);
 }
 
 #define PGPU_GRID_DISPATCH(d, call)          \
@@ -280,6 +381,12 @@ int run_grid(Engine& E, const LatticeJob& J, cudaStream_t st) {
                     kGridMaxD, d);
     if (vd < 1 || vd > kGridMaxVd) return fail(PGPU_ERR_UNSUPPORTED, "%d value channels", vd);
     if (J.payload != kPayloadF32) return fail(PGPU_ERR_UNSUPPORTED, "the grid method computes in FP32 only");
+    for (const PointSource* ps : {&J.splat, &J.slice}) {   // the launches' grid dimensions
+        if (ps == &J.slice && J.replay) continue;
+        if (ps->frames > 65535 || (ps->height > 1 && ps->height > 65535 * (kGridThreads / 32)))
+            return fail(PGPU_ERR_UNSUPPORTED, "the grid method takes at most 65535 frames and %d rows",
+                        65535 * (kGridThreads / 32));
+    }
     // DenseGrid's constructor (src/DenseGrid.h:111-127): sqrtf(1.0/3 + (taps-1)*0.25)
     const float sf = sqrtf((float)(1.0 / 3 + (kGridTaps - 1) * 0.25));
     const PointSource& sl = J.replay ? J.splat : J.slice;

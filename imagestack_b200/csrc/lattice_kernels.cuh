@@ -315,6 +315,30 @@ __device__ __forceinline__ void load_position(const PointSource& s, uint32_t i, 
         ++c; }
 }
 
+// positions of point (x, y, t) of a source, as load_position
+template <int D>
+__device__ __forceinline__ void load_position_xyt(const PointSource& s, uint32_t x, uint32_t y, uint32_t t,
+                                                  float (&p)[D]) {
+    const long long off_p = (long long)t * s.pos.tstride + (long long)y * s.pos.ystride + x;
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+        if (k < s.pos_channels)
+            p[k] = __fmul_rn(__ldg(s.pos.base + off_p + (long long)k * s.pos.cstride), s.pos_scale[k]);
+    int c = s.pos_channels;
+    if (s.coord_mask & 1) { float f = __fmul_rn((float)x, s.coord_scale[0]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    if (s.coord_mask & 2) { float f = __fmul_rn((float)y, s.coord_scale[1]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+    if (s.coord_mask & 4) { float f = __fmul_rn((float)t, s.coord_scale[2]);
+#pragma unroll
+        for (int k = 0; k < D; ++k) if (k == c) p[k] = f;
+        ++c; }
+}
+
 // ---------------------------------------------------------------------------------
 // accumulator rows
 // ---------------------------------------------------------------------------------
