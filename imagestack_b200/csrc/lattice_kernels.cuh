@@ -531,14 +531,23 @@ __host__ __device__ constexpr size_t tile_smem_bytes(int d, int vdp) {
            16 + 0 * (size_t)vdp;
 }
 
+// Home slot of a one-word key in a block's table: a cheap multiplicative mix of the three
+// 32-bit words that carry coordinates 0..5 and the low half of the fourth (coordinate 6);
+// the table is small and probing resolves its collisions, so the global hash (a 64-bit
+// mix) is computed only once per distinct vertex, in phase B.
+__device__ __forceinline__ uint32_t tile_home(const uint4& k) {
+    const uint32_t h = k.x * 0x9E3779B1u + k.y * 0x85EBCA77u + k.z * 0xC2B2AE3Du + (k.w & 0xFFFFu) * 0x27D4EB2Fu;
+    return (h ^ (h >> 15)) * 0x2C1B3C6Du >> (32 - 10);
+}
+
 // find-or-insert of a one-word key in the block's table; a new key's slot is appended to
 // the block's list of occupied slots.  -1 when no slot within the probe limit is free (the
 // caller then uses the global table).
 __device__ __forceinline__ int tile_insert(uint4* t_key, uint16_t* t_list, uint32_t* t_count,
-                                           const uint4& k, uint32_t h) {
+                                           const uint4& k) {
     const uint4 empty = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
-    static_assert(kTileSlots == 1024, "home slot uses the top 10 hash bits");
-    uint32_t l = h >> (32 - 10);
+    static_assert(kTileSlots == 1024, "the home slot has 10 bits");
+    uint32_t l = tile_home(k);
 #pragma unroll 1
     for (int probe = 0; probe < kTileProbe; ++probe) {
         uint4 w = t_key[l];
@@ -657,13 +666,12 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
         for (int r = 0; r <= D; ++r) {
             if (r > 0) key_step<D>(key, scr.coord[(D - (r - 1)) * scr.stride]);
             bary[r] = sx.bary[r];
-            const uint32_t hk = key_hash<1>(key);
-            const int l = tile_insert(t_key, t_list, &t_count, key.w[0], hk);
+            const int l = tile_insert(t_key, t_list, &t_count, key.w[0]);
             if (l >= 0) {
                 if (ft) atomicMin(&t_ft[l], e0 + (uint32_t)r);
                 loc[r] = l;
             } else {
-                const uint32_t home = home_slot(hk, table.cap);
+                const uint32_t home = home_slot(key_hash<1>(key), table.cap);
                 bool created = false;
                 const int s = table_insert<1>(table, key, home, __ldcg(&table.key0[home]), status, &created);
                 if (s >= 0) {
