@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "engine.h"
@@ -82,17 +83,28 @@ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 // largest ratio per d as the guess for an unseen signature.  A guess that is too small
 // makes the image overflow its hash range and run again.
 std::mutex g_ratio_mu;
-std::map<std::string, double> g_ratio_by_sig;
+std::unordered_map<uint64_t, double> g_ratio_by_sig;
 std::map<int, double> g_ratio;
 
-// an image's key for the learned vertex ratio: its shape and position scales
-std::string item_signature(int d, const PointSource& s) {
-    char buf[320];
-    int n = snprintf(buf, sizeof(buf), "%d:%dx%dx%d:%x", d, s.width, s.height, s.frames, s.coord_mask);
-    for (int c = 0; c < s.pos_channels && c < kMaxD && n < 240; ++c)
-        n += snprintf(buf + n, sizeof(buf) - n, ":%a", (double)s.pos_scale[c]);
-    for (int c = 0; c < 3 && n < 300; ++c) n += snprintf(buf + n, sizeof(buf) - n, ":%a", (double)s.coord_scale[c]);
-    return std::string(buf);
+inline uint64_t mix64(uint64_t h, uint64_t v) {
+    h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+    return h * 0xBF58476D1CE4E5B9ull;
+}
+inline uint64_t float_bits(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return u;
+}
+
+// an image's key for the learned vertex ratio: a 64-bit mix of its shape and position
+// scales (a collision would only size a table from another image's ratio: at worst a rerun)
+uint64_t item_signature(int d, const PointSource& s) {
+    uint64_t h = mix64(0x51ED27B3ull, (uint64_t)d);
+    h = mix64(h, ((uint64_t)(uint32_t)s.width << 32) | (uint32_t)s.height);
+    h = mix64(h, ((uint64_t)(uint32_t)s.frames << 32) | (uint32_t)s.coord_mask);
+    for (int c = 0; c < s.pos_channels && c < kMaxD; ++c) h = mix64(h, float_bits(s.pos_scale[c]));
+    for (int c = 0; c < 3; ++c) h = mix64(h, float_bits(s.coord_scale[c]));
+    return h;
 }
 
 // device (and pinned host) metadata of one batch
@@ -172,7 +184,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     const uint32_t nwords = (uint32_t)((entries + 31) / 32);
 
     // slots per lattice: (learned vertices per point) x 1.3 x points / load
-    std::vector<std::string> sig(nseg);
+    std::vector<uint64_t> sig(nseg);
     std::vector<double> ratio(nseg), density(nseg);
     {
         std::lock_guard<std::mutex> lk(g_ratio_mu);
@@ -200,15 +212,18 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         cap[k] = std::max<uint64_t>((c + 31) & ~31ull, 256);
     }
 
-    // Splat kernel per lattice: the tile splat (shared-memory table per 32x32 tile) where
+    // Splat kernel per lattice: the tile splat (shared-memory table per 16x16 tile) where
     // neighbouring points share vertices, which the learned vertices-per-point ratio tells
-    // (4K d=5 bilateral: 0.18; a 32x32 tile then holds about 370 of its 6144 entries'
-    // vertices); the direct splat for sparse lattices (ratio above kTileRatioMax, where a
-    // tile's distinct vertices would overflow its 1024 shared-memory slots), multi-word
-    // keys and FP64 accumulators.  With nothing learned yet for the image or its d, the
+    // (4K d=5 bilateral: 0.18; a 16x16 tile then holds about 155 of its 1536 entries'
+    // vertices); the direct splat for sparse lattices (ratio above kTileRatioMax: measured
+    // on the mixed batch, 1.5 beats 0.8 by 2 % and 0.4 by 3 %), multi-word keys and FP64
+    // accumulators.  With nothing learned yet for the image or its d, the
     // tile splat.  PGPU_SPLAT=direct or =tile in the environment overrides the choice
     // where both exist (the parity tests compare the two).
-    constexpr double kTileRatioMax = 0.8;
+#ifndef PGPU_TILE_RATIO_MAX
+#define PGPU_TILE_RATIO_MAX 1.5
+#endif
+    constexpr double kTileRatioMax = PGPU_TILE_RATIO_MAX;
     const char* mode = std::getenv("PGPU_SPLAT");
     const int forced = !mode ? 0 : !strcmp(mode, "direct") ? 1 : !strcmp(mode, "tile") ? 2 : 0;
     const bool tile_ok = kw == 1 && B.payload != kPayloadF64 && forced != 1 && (forced == 2 || B.splat == 0);
@@ -301,6 +316,8 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         unsigned char* dmeta = (unsigned char*)E.meta.p;
         uint32_t* dM = (uint32_t*)dmeta + 1;
         auto enqueue = [&](bool timed) -> int {
+            // the lattice's time (and so the autotuner's) includes clearing its tables
+            if (timed) CUDA_TRY(cudaEventRecord(E.ev[6], st));
             CUDA_TRY(cudaMemcpyAsync(dmeta + L.slotbase, h + L.slotbase, L.total - L.slotbase,
                                      cudaMemcpyHostToDevice, st));
             CUDA_TRY(cudaMemsetAsync(dmeta, 0, L.slotbase, st));
@@ -439,16 +456,20 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         };
 
         if (graph) {
-            // the graph bakes in sizes and buffer addresses, so both key it
-            char key[256];
-            snprintf(key, sizeof(key), "%d:%d:%d:%d:%d:%d:%llu:%llu:%llu:%u:%p:%p:%p:%p:%p:%p:%p", d, vd,
-                     B.payload, (int)homog, (int)B.replay, nseg, (unsigned long long)n_total,
-                     (unsigned long long)ns_total, (unsigned long long)cap_total, nwords, E.key0.p,
-                     E.tvals.p, E.nbr.p, E.rec.p, E.meta.p, (void*)E.hmeta, E.sval.p);
-            std::string gk(key);
-            gk += B.blur_pairs ? ":p" : ":s";
-            gk += tile_blocks ? ":t" + std::to_string(tile_blocks) : ":d";
-            for (int k = 0; k < nseg; ++k) gk += ":" + std::to_string(cap[k]) + "/" + std::to_string(B.items[k].n);
+            // the graph bakes in sizes, settings and buffer addresses, so all of them key it
+            std::vector<uint64_t> gk = {
+                (uint64_t)d, (uint64_t)vd, (uint64_t)B.payload, (uint64_t)homog, (uint64_t)B.replay,
+                (uint64_t)nseg, n_total, ns_total, cap_total, nwords, (uint64_t)B.blur_pairs, blocks,
+                tile_blocks, slice_blocks, (uint64_t)(uintptr_t)E.key0.p, (uint64_t)(uintptr_t)E.keyn.p,
+                (uint64_t)(uintptr_t)E.tvals.p, (uint64_t)(uintptr_t)E.nbr.p, (uint64_t)(uintptr_t)E.rec.p,
+                (uint64_t)(uintptr_t)E.recw.p, (uint64_t)(uintptr_t)E.meta.p, (uint64_t)(uintptr_t)E.hmeta,
+                (uint64_t)(uintptr_t)E.sval.p, (uint64_t)(uintptr_t)E.vlist.p, (uint64_t)(uintptr_t)E.vv0.p,
+                (uint64_t)(uintptr_t)E.vv1.p, (uint64_t)(uintptr_t)E.vkey0.p, (uint64_t)(uintptr_t)E.vf32.p};
+            gk.reserve(gk.size() + 2 * (size_t)nseg);
+            for (int k = 0; k < nseg; ++k) {
+                gk.push_back(cap[k]);
+                gk.push_back(((uint64_t)B.items[k].n << 1) | (segs[k].tile_w ? 1u : 0u));
+            }
             auto it = E.graphs.find(gk);
             if (it == E.graphs.end()) {
                 if (E.graphs.size() >= 32) E.drop_graphs();
@@ -532,8 +553,10 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             cudaEventElapsedTime(&s.ms_neighbours, E.ev[2], E.ev[3]);
             cudaEventElapsedTime(&s.ms_blur, E.ev[3], E.ev[4]);
             cudaEventElapsedTime(&s.ms_slice, E.ev[4], E.ev[5]);
+            cudaEventElapsedTime(&s.ms_total, E.ev[6], E.ev[5]);
+        } else {
+            cudaEventElapsedTime(&s.ms_total, E.ev[0], E.ev[5]);
         }
-        cudaEventElapsedTime(&s.ms_total, E.ev[0], E.ev[5]);
         set_stats(s);
         return PGPU_OK;
     }

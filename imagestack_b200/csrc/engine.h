@@ -78,7 +78,9 @@ struct Engine {
     // host-memory batches: uploads and downloads overlap the lattices on these streams
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
     cudaEvent_t pipe_ev[9] = {};   // per device slot (3): uploaded, filtered, downloaded
-    std::map<std::string, cudaGraphExec_t> graphs;  // captured batch pipelines, by batch shape
+    // captured batch pipelines, keyed by everything a graph bakes in (sizes, buffer
+    // addresses, settings, each image's points and slot range)
+    std::map<std::vector<uint64_t>, cudaGraphExec_t> graphs;
     // autotuner state per batch shape: candidate trials so far, their times, the choice
     struct Tuning {
         int trials = 0;
