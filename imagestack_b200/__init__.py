@@ -179,6 +179,48 @@ def _view(a, name: str) -> tuple[Image, int]:
     return v, MEM_HOST
 
 
+_IMAGE_DTYPE = np.dtype([("base", np.uintp), ("width", np.int32), ("height", np.int32),
+                         ("frames", np.int32), ("channels", np.int32), ("ystride", np.int64),
+                         ("tstride", np.int64), ("cstride", np.int64)])
+assert _IMAGE_DTYPE.itemsize == C.sizeof(Image)
+
+
+def _views_torch(images):
+    """Views of many torch tensors at once: one column per pgpu_image field, filled by
+    list comprehensions into a buffer laid out like the C array (a per-image ctypes
+    structure costs several microseconds).  Returns (views, memory), or None when any
+    image would fail _view's checks, so that the per-image path raises its message."""
+    import torch
+    try:
+        dims = [a.dim() for a in images]
+        if any(a.dtype != torch.float32 for a in images):
+            return None
+        cuda = [a.is_cuda for a in images]
+    except AttributeError:
+        return None
+    if not (all(cuda) or not any(cuda)) or any(k not in (3, 4) for k in dims):
+        return None
+    shapes = [a.shape for a in images]
+    strides = [a.stride() for a in images]
+    if any(s[-1] != 1 for s in strides):
+        return None
+    n = len(images)
+    arr = np.empty(n, _IMAGE_DTYPE)
+    arr["base"] = [a.data_ptr() for a in images]
+    arr["channels"] = [s[0] for s in shapes]
+    arr["width"] = [s[-1] for s in shapes]
+    arr["height"] = [s[-2] for s in shapes]
+    arr["frames"] = [s[1] if k == 4 else 1 for s, k in zip(shapes, dims)]
+    arr["ystride"] = [s[-2] for s in strides]
+    arr["cstride"] = [s[0] for s in strides]
+    # A (c, h, w) tensor is the single frame of (c, 1, h, w), whose frame stride torch's
+    # unsqueeze(1) sets to height x row stride.
+    arr["tstride"] = [s[1] if k == 4 else s[1] * sh[1]
+                      for s, sh, k in zip(strides, shapes, dims)]
+    views = (Image * n).from_buffer(arr)
+    return views, (MEM_DEVICE if cuda[0] else MEM_HOST)
+
+
 def _options(memory: int, payload: str, device: int = 0, stream=None, load_factor: float = 0.5):
     o = Options()
     lib().pgpu_default_options(C.byref(o))
@@ -293,14 +335,18 @@ def bilateral_batch(images, filter_widths, color_sigmas, payload: str = "fp32",
     n = len(images)
     if len(filter_widths) != n or len(color_sigmas) != n:
         raise PgpuError(ERR_ARGUMENT, "one filter width and colour sigma per image")
-    views = (Image * max(n, 1))()
-    mem = MEM_HOST
-    for i, im in enumerate(images):
-        views[i], m = _view(im, "image %d" % i)
-        if i == 0:
-            mem = m
-        elif m != mem:
-            raise PgpuError(ERR_ARGUMENT, "images must all be on the host or all on the device")
+    fast = _views_torch(images) if n and _is_torch(images[0]) else None
+    if fast is not None:
+        views, mem = fast
+    else:
+        views = (Image * max(n, 1))()
+        mem = MEM_HOST
+        for i, im in enumerate(images):
+            views[i], m = _view(im, "image %d" % i)
+            if i == 0:
+                mem = m
+            elif m != mem:
+                raise PgpuError(ERR_ARGUMENT, "images must all be on the host or all on the device")
     fw = (C.c_float * max(n, 1))(*[float(x) for x in filter_widths])
     cs = (C.c_float * max(n, 1))(*[float(x) for x in color_sigmas])
     stream = _torch_stream(images[0]) if (n and mem == MEM_DEVICE) else None

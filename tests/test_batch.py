@@ -35,6 +35,35 @@ def test_batch_argument_checks_need_no_gpu():
         ib.bilateral_batch([a], [4.0, 5.0], [0.1])
 
 
+def test_batched_views_equal_per_image_views():
+    """The batched view builder writes the same pgpu_image fields as _view, for (c, h, w)
+    and (c, f, h, w) tensors, cropped and channel-sliced ones included, and declines
+    (returns None) whatever _view would reject."""
+    torch = pytest.importorskip("torch")
+    g = torch.Generator().manual_seed(0)
+    ims = []
+    for i in range(40):
+        h, w = 16 + (i * 7) % 23, 16 + (i * 11) % 29
+        t = torch.rand(3, h, w, generator=g)
+        if i % 5 == 1:
+            t = t[:, 1:, 2:]
+        if i % 7 == 2:
+            t = torch.rand(3, 2, h, w, generator=g)
+        if i % 11 == 3:
+            t = torch.rand(5, h, w + 3, generator=g)[1:4, :, :w]
+        ims.append(t)
+    views, mem = ib._views_torch(ims)
+    assert mem == ib.MEM_HOST
+    for i, t in enumerate(ims):
+        v, m = ib._view(t, "image")
+        assert m == mem
+        for f, _ in ib.Image._fields_:
+            assert getattr(views[i], f) == getattr(v, f), (i, f)
+    assert ib._views_torch([torch.zeros(3, 4, 4, dtype=torch.float64)]) is None
+    assert ib._views_torch([torch.zeros(3, 4, 4).transpose(1, 2)]) is None
+    assert ib._views_torch([torch.zeros(4, 4)]) is None
+
+
 @pytest.mark.gpu
 def test_batch_matches_single_image_path(gpu):
     imgs, ss, sr = uneven_batch(24, seed=3)
