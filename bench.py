@@ -44,8 +44,25 @@ def workload(payload):
 
 
 L2_BYTES = 126 * 1024 * 1024
-KERNELS_PER_LATTICE = 4   # tile splat, list assign, neighbours, replay slice (+ the blur's)
-TUNE_TRIALS = 5           # candidate settings the batch autotuner tries per batch shape
+# launches of one lattice besides the blur's: tile splat, neighbours, replay slice, and the
+# list-ordered compaction where rows stay in slot space
+
+
+def kernels_per_lattice(vertex_rows):
+    return 3 if vertex_rows else 4
+TUNE_MAX_CALLS = 24       # at most this many calls for the autotuner to finish a shape
+
+
+def tune(fn, prepare=None):
+    """Call fn until the batch autotuner reports its choice for the shape (stats "tuned"
+    2: its trials, each setting timed twice, are over); returns the calls made."""
+    for k in range(TUNE_MAX_CALLS):
+        if prepare:
+            prepare()
+        fn()
+        if fn.stats()["tuned"] != 1:
+            return k + 1
+    return TUNE_MAX_CALLS
 D = 5
 
 
@@ -62,26 +79,37 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def stage_bytes(N, M, d=D, C=3, p=4, vdp=4, blur_passes=3):
+def stage_bytes(N, M, d=D, C=3, p=4, vdp=4, blur_passes=3, vertex_rows=False, nbr_half=False):
     """Algorithmic bytes of each lattice stage for N points and M vertices: what each stage's
     kernels must move as they are built, every input read once and every output written
     once (a row is vdp values of p bytes; the splat's sums and the slice's rows are FP32).
-      splat       image N*C*4 read; replay record N*(d+1)*(4 slot + 4 weight) written;
-                  table M*(16 key + 4*vdp row) written once
-      compaction  vertex list M*4, key M*16 and row M*4*vdp read; key M*16, row M*p*vdp,
-                  both index maps M*8 and the index in the key word M*16 written
-      neighbours  key M*16 read, one table slot M*16 per lookup (2(d+1) lookups), the
+      splat       image N*C*4 read; replay record N*(d+1)*(4 index + 4 weight) written;
+                  table M*(16 key + 4*vdp row) written once; with vertex-ordered rows the
+                  creator also writes the key in vertex order M*16, the vertex's slot M*4
+                  and its index in the key word M*4 (and, for the one-lookup neighbour
+                  search, the vertex's absent-neighbour pairs M*8*(d+1))
+      compaction  (slot-space rows only) vertex list M*4, key M*16 and row M*4*vdp read;
+                  key M*16, row M*p*vdp, both index maps M*8 and the index in the key word
+                  M*16 written
+      neighbours  key M*16 read, one table slot M*16 per lookup (2(d+1) lookups, or d+1
+                  with one lookup per axis plus a 4-byte pair entry written per lookup), the
                   pairs M*8*(d+1) written
-      blur        per pass: rows M*p*vdp read and written, neighbour pairs M*8 per axis
-                  (2 axes per fused pass); the last pass writes FP32 rows M*4*vdp through
-                  the vertex->slot map M*4
+      blur        per pass: rows M*p*vdp read and written, neighbour pairs M*8 per axis;
+                  the last pass writes FP32 rows M*4*vdp (slot-space rows: through the
+                  vertex->slot map M*4)
       slice       replay record N*(d+1)*8 and the FP32 rows M*4*vdp read, N*C*4 written"""
     axes = d + 1
     splat = N * C * 4 + N * axes * 8 + M * (16 + 4 * vdp)
-    compact = M * (4 + 16 + 4 * vdp) + M * (16 + p * vdp + 8 + 16)
-    neighbours = M * 16 + 2 * axes * M * 16 + axes * M * 8
+    if vertex_rows:
+        splat += M * (16 + 4 + 4) + (M * 8 * axes if nbr_half else 0)
+        compact = 0
+    else:
+        compact = M * (4 + 16 + 4 * vdp) + M * (16 + p * vdp + 8 + 16)
+    lookups = axes if nbr_half else 2 * axes
+    neighbours = M * 16 + lookups * M * 16 + axes * M * 8 + (lookups * M * 4 if nbr_half else 0)
     per_pass_axes = axes / blur_passes
-    blur = blur_passes * (2 * M * p * vdp + per_pass_axes * M * 8) + M * (4 * vdp - p * vdp + 4)
+    blur = blur_passes * (2 * M * p * vdp + per_pass_axes * M * 8) + M * (4 * vdp - p * vdp) + \
+        (0 if vertex_rows else M * 4)
     slice_ = N * axes * 8 + M * 4 * vdp + N * C * 4
     return {"splat": int(splat), "compact": int(compact), "neighbours": int(neighbours),
             "blur": int(blur), "slice": int(slice_)}
@@ -416,9 +444,8 @@ def mixed_batch(ib, synth, torch, dev, steps):
         for wk, s, r in zip(work, ss, sr):
             ib.Bilateral.apply(wk, s, s, 0.0, r)
 
-    for _ in range(TUNE_TRIALS):   # the autotuner's trials of this batch shape
-        restore()
-        batched()
+    batched.stats = ib.last_stats
+    tune(batched, restore)   # the autotuner's trials of this batch shape
     for _ in range(2):
         restore()
         batched()
@@ -596,12 +623,11 @@ def run_ours(args):
         ib.bilateral_batch(work, ss, sr, payload=alt_payload, autotune=not args.no_autotune)
     alt.stats = ib.last_stats
 
-    for _ in range(0 if args.no_autotune else TUNE_TRIALS):   # the autotuner's trials
-        prepare()
-        headline()
+    tune_calls = {}
+    if not args.no_autotune:   # the autotuner's trials
+        tune_calls[args.payload] = tune(headline, prepare)
         if not args.quick:
-            prepare()
-            alt()
+            tune_calls[alt_payload] = tune(alt, prepare)
     for _ in range(args.warmup):
         prepare()
         headline()
@@ -625,22 +651,80 @@ def run_ours(args):
     value = world * px_step * args.steps / (total_ms / 1e3) / 1e6
     plain_mpix = W * H * args.steps / (plain_ms / 1e3) / 1e6
 
-    # end to end through the C ABI: pinned host frames in, filtered frames back out
-    host = [torch.from_numpy(f.copy()).pin_memory() for f in frames]
-    host_np = [h.numpy() for h in host]
-    e2e_steps = min(args.steps, 10)
-    e2e_times = []
-    for i in range(args.warmup + e2e_steps):
+    # End to end through the C ABI, pinned host frames in and filtered frames out, every
+    # step's uploads and downloads inside the timed region.  A step is one queued batch of
+    # the four frames (pgpu_bilateral_batch_submit, out of place, so the inputs stay as
+    # they are); two steps are in flight, so one step's uploads overlap the previous
+    # step's lattices and downloads.  Timed by the host clock from the first submission to
+    # the last wait.
+    host_in = [torch.from_numpy(f.copy()).pin_memory() for f in frames]
+    host_out = [[torch.empty_like(h).pin_memory() for h in host_in] for _ in range(2)]
+    in_np = [h.numpy() for h in host_in]
+    out_np = [[h.numpy() for h in row] for row in host_out]
+    autotune = not args.no_autotune
+
+    def submit(i):
+        return ib.bilateral_batch_submit(in_np, ss, sr, outputs=out_np[i % 2], payload=args.payload,
+                                         autotune=autotune)
+    e2e_steps = max(args.steps, 10)
+    e2e_tune = 0
+    for i in range(TUNE_MAX_CALLS):   # the autotuner's trials of the one-frame chunk shape
+        submit(i).wait()
+        e2e_tune += 1
+        if not autotune or ib.last_stats()["tuned"] != 1:
+            break
+    for i in range(args.warmup):
+        submit(i).wait()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    from collections import deque
+    t0 = time.perf_counter()
+    inflight = deque()
+    for i in range(e2e_steps):
+        if len(inflight) == 2:
+            inflight.popleft().wait()
+        inflight.append(submit(i))
+    while inflight:
+        inflight.popleft().wait()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dev)
+    e2e = world * px_step * e2e_steps / e2e_s / 1e6
+    e2e_out = out_np[(e2e_steps - 1) % 2][0].copy()
+
+    # the same step as one synchronous call (in place: the frames are restored outside the
+    # timed region), which cannot overlap one step's copies with the next step's
+    host_np = out_np[0]
+    sync_times = []
+    for i in range(args.warmup + 10):
         for hn, f in zip(host_np, frames):
             hn[...] = f
-        t0 = time.perf_counter()
-        ib.bilateral_batch(host_np, ss, sr, payload=args.payload, autotune=not args.no_autotune)
-        el = time.perf_counter() - t0
+        t1 = time.perf_counter()
+        ib.bilateral_batch(host_np, ss, sr, payload=args.payload, autotune=autotune)
         if i >= args.warmup:
-            e2e_times.append(el)
-    e2e_s = sum(e2e_times)
-    e2e_s = max_over_ranks(e2e_s, dev)
-    e2e = world * px_step * e2e_steps / e2e_s / 1e6
+            sync_times.append(time.perf_counter() - t1)
+    e2e_sync = px_step * len(sync_times) / sum(sync_times) / 1e6
+
+    # the copies alone: the four frames up, down, and both at once on two streams
+    def copy_ms(up, down, reps=5):
+        s_up, s_dn = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        best = 1e30
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            if up:
+                with torch.cuda.stream(s_up):
+                    for wk, h in zip(work, host_in):
+                        wk.copy_(h, non_blocking=True)
+            if down:
+                with torch.cuda.stream(s_dn):
+                    for p_, h in zip(pristine, host_out[1]):
+                        h.copy_(p_, non_blocking=True)
+            torch.cuda.synchronize()
+            best = min(best, (time.perf_counter() - t2) * 1e3)
+        return best
+    copies = {"h2d_ms": round(copy_ms(True, False), 3), "d2h_ms": round(copy_ms(False, True), 3),
+              "both_ms": round(copy_ms(True, True), 3)}
+    copies["bound_mpix_s"] = round(px_step / (copies["both_ms"] / 1e3) / 1e6, 1)
 
     if rank == 0:
         hbm, peak_kind = peaks()
@@ -658,7 +742,8 @@ def run_ours(args):
         p = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[args.payload]
         N = FRAMES_PER_STEP * n
         passes = blur_launches(D, bool(stage[-1]["blur_pairs"]))
-        sb = stage_bytes(N, M, p=p, blur_passes=passes)
+        sb = stage_bytes(N, M, p=p, blur_passes=passes, vertex_rows=bool(stage[-1]["vertex_rows"]),
+                         nbr_half=bool(stage[-1]["nbr_half"]))
         splat_bytes = sb["splat"]
         achieved = splat_bytes / (splat_ms / 1e3) / 1e9
         total_bytes = sum(sb.values())
@@ -669,7 +754,7 @@ def run_ours(args):
         roofline_stages = {}
         for k, b in sb.items():
             ms = stages[stage_ms_key[k]]
-            ach = b / (ms / 1e3) / 1e9 if ms > 0 else None
+            ach = b / (ms / 1e3) / 1e9 if (ms > 0 and b > 0) else None
             roofline_stages[k] = {"bytes": b, "ms": ms, "achieved_gbs": round(ach, 1) if ach else None,
                                   "frac": round(ach / hbm, 4) if ach else None,
                                   "traffic_per_frame": traffic.get(k + "_dram_bytes")}
@@ -731,13 +816,24 @@ def run_ours(args):
                                   "peak": hbm, "unit": "GB/s",
                                   "frac": round(total_bytes / (lattice_ms / 1e3) / 1e9 / hbm, 4)},
             "e2e": {"value": round(e2e, 2), "unit": "Mpix/s",
-                    "h2d_bytes_per_step": px_step * 3 * 4, "d2h_bytes_per_step": px_step * 3 * 4},
-            "gpu_launches": args.steps * (KERNELS_PER_LATTICE + passes),
+                    "h2d_bytes_per_step": px_step * 3 * 4, "d2h_bytes_per_step": px_step * 3 * 4,
+                    "steps": e2e_steps, "ms_per_step": round(e2e_s * 1e3 / e2e_steps, 3),
+                    "path": "pgpu_bilateral_batch_submit / pgpu_batch_wait, pinned host frames, "
+                            "out of place, two steps in flight",
+                    "max_rel_err_vs_device_path": rel_err(e2e_out, a.cpu().numpy()),
+                    "copies_alone": copies,
+                    "one_call_per_step_mpix_s": round(e2e_sync, 2),
+                    "autotuner_calls": e2e_tune},
+            "gpu_launches": args.steps * (kernels_per_lattice(stage[-1]["vertex_rows"]) + passes),
             "autotuned": {"load_factor": round(stage[-1]["load_factor"], 3),
                           "blur_pairs": bool(stage[-1]["blur_pairs"]),
+                          "blur_grid": "one vertex per thread" if stage[-1]["blur_grid"]
+                                       else "16 blocks per SM, striding",
                           "splat": "tile" if stage[-1]["tiled"] else "direct",
-                          "candidates": "load factor 0.5/0.35/0.7, blur axes in pairs or one "
-                                        "per pass (FP32), tile or direct splat"},
+                          "calls": tune_calls,
+                          "knobs": "coordinate descent, each option timed twice: load factor "
+                                   "0.5/0.35/0.7, blur axes in pairs or one per pass (FP32/FP64), "
+                                   "blur grid, tile or direct splat"},
             "stages_ms": stages, "vertices": M, "capacity": stage[-1]["capacity"],
             "clocks": clk.summary(),
         }

@@ -60,7 +60,9 @@ class Stats(C.Structure):
                 ("d", C.c_int), ("vd", C.c_int), ("payload", C.c_int), ("retries", C.c_int),
                 ("ms_splat", C.c_float), ("ms_compact", C.c_float), ("ms_neighbours", C.c_float),
                 ("ms_blur", C.c_float), ("ms_slice", C.c_float), ("ms_total", C.c_float),
-                ("load_factor", C.c_float), ("blur_pairs", C.c_int), ("tiled", C.c_int)]
+                ("load_factor", C.c_float), ("blur_pairs", C.c_int), ("tiled", C.c_int),
+                ("blur_grid", C.c_int), ("tuned", C.c_int), ("nbr_half", C.c_int),
+                ("vertex_rows", C.c_int)]
 
 
 from .tmpfile import load_tmp, save_tmp  # noqa: E402,F401  (ImageStack .tmp files)
@@ -68,7 +70,7 @@ from .tmpfile import load_tmp, save_tmp  # noqa: E402,F401  (ImageStack .tmp fil
 EXPORTS = ["pgpu_default_options", "pgpu_last_error", "pgpu_version", "pgpu_device_count",
            "pgpu_gauss_transform", "pgpu_joint_bilateral", "pgpu_bilateral", "pgpu_last_stats",
            "pgpu_lattice_dump", "pgpu_bilateral_batch", "pgpu_exact_gauss_transform_f64",
-           "pgpu_probe_red_rate"]
+           "pgpu_probe_red_rate", "pgpu_bilateral_batch_submit", "pgpu_batch_wait"]
 
 _lib = None
 
@@ -91,6 +93,9 @@ def lib():
     L.pgpu_bilateral.argtypes = [P(Image), C.c_float, C.c_float, C.c_float, C.c_float, P(Options)]
     L.pgpu_last_stats.argtypes = [P(Stats)]
     L.pgpu_bilateral_batch.argtypes = [P(Image), C.c_int, P(C.c_float), P(C.c_float), P(Options)]
+    L.pgpu_bilateral_batch_submit.argtypes = [P(Image), P(Image), C.c_int, P(C.c_float), P(C.c_float),
+                                              P(Options), P(C.c_longlong)]
+    L.pgpu_batch_wait.argtypes = [C.c_longlong]
     L.pgpu_lattice_dump.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                     P(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p]
@@ -355,6 +360,61 @@ def bilateral_batch(images, filter_widths, color_sigmas, payload: str = "fp32",
     opt.flags = (FLAG_GRAPH if graph else 0) | (FLAG_AUTOTUNE if autotune else 0)
     _check(lib().pgpu_bilateral_batch(views, n, fw, cs, C.byref(opt)))
     return images
+
+
+class BatchTicket:
+    """A host batch queued by bilateral_batch_submit.  wait() returns the outputs once
+    they are written; the input and output arrays are held (and must not be modified)
+    until then.  A ticket dropped without wait() is waited for first."""
+
+    def __init__(self, ticket: int, images, outputs):
+        self.ticket = ticket
+        self.images = images
+        self.outputs = outputs
+        self.done = False
+
+    def wait(self):
+        if not self.done:
+            self.done = True
+            _check(lib().pgpu_batch_wait(self.ticket))
+        return self.outputs
+
+    def __del__(self):
+        if not getattr(self, "done", True):
+            try:
+                self.wait()
+            except Exception:
+                pass
+
+
+def bilateral_batch_submit(images, filter_widths, color_sigmas, outputs=None, payload: str = "fp32",
+                           graph: bool = False, load_factor: float = 0.5, autotune: bool = False):
+    """Queue the bilateral filter of many host (numpy) images and return a BatchTicket at
+    once (pgpu_bilateral_batch_submit): each result goes to outputs[i] (same shape; None:
+    in place).  Consecutive submissions overlap their copies and filtering on the device;
+    each result equals Bilateral.apply on the image."""
+    n = len(images)
+    if n == 0 or len(filter_widths) != n or len(color_sigmas) != n:
+        raise PgpuError(ERR_ARGUMENT, "one filter width and colour sigma per image, at least one image")
+    if outputs is not None and len(outputs) != n:
+        raise PgpuError(ERR_ARGUMENT, "one output per image")
+    views = (Image * n)()
+    outs = (Image * n)() if outputs is not None else None
+    for i, im in enumerate(images):
+        views[i], m = _view(im, "image %d" % i)
+        if m != MEM_HOST:
+            raise PgpuError(ERR_ARGUMENT, "queued batches take host (numpy) images")
+        if outs is not None:
+            outs[i], m = _view(outputs[i], "output %d" % i)
+            if m != MEM_HOST:
+                raise PgpuError(ERR_ARGUMENT, "queued batches take host (numpy) outputs")
+    fw = (C.c_float * n)(*[float(x) for x in filter_widths])
+    cs = (C.c_float * n)(*[float(x) for x in color_sigmas])
+    opt = _options(MEM_HOST, payload, load_factor=load_factor)
+    opt.flags = (FLAG_GRAPH if graph else 0) | (FLAG_AUTOTUNE if autotune else 0)
+    t = C.c_longlong(0)
+    _check(lib().pgpu_bilateral_batch_submit(views, outs, n, fw, cs, C.byref(opt), C.byref(t)))
+    return BatchTicket(t.value, images, outputs if outputs is not None else images)
 
 
 REQ_BILATERAL, REQ_JOINT_BILATERAL, REQ_GAUSS_TRANSFORM = 0, 1, 2

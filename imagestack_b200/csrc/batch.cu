@@ -49,6 +49,9 @@ void Engine::drop_graphs() {
 
 void Engine::shutdown() {
     if (device >= 0) cudaSetDevice(device);
+    drain_async(*this);
+    for (auto& pb : pinned_free) cudaFreeHost(pb.first);
+    pinned_free.clear();
     if (stream) cudaStreamSynchronize(stream);
     drop_graphs();
     for (auto& e : ev)
@@ -127,12 +130,14 @@ MetaLayout layout(int nseg, bool slice_segs) {
 
 }  // namespace
 
-// One pass over the batch.  Images whose hash-table range overflowed are listed in
-// *failed, with the larger range to use in *cap_next; their output is untouched (the
-// slice skips them), while every other image of the pass is finished.
-static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
-                          const std::vector<uint64_t>* cap_in, std::vector<int>* failed,
-                          std::vector<uint64_t>* cap_next, int pass) {
+size_t batch_meta_bytes(int nseg) { return layout(nseg, false).total; }
+
+// Queue one pass over the batch on st, its metadata staged in the pinned buffer h (E.hmeta
+// when null); *ps receives what finish_pass needs once the stream has run it.  timed: CUDA
+// events around every stage (read by finish_pass).
+static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
+                        const std::vector<uint64_t>* cap_in, unsigned char* h_in, bool timed,
+                        int pass, PassState* ps) {
     const int d = B.d, vd = B.vd;
     const int nseg = (int)B.items.size();
     if (nseg == 0) return PGPU_OK;
@@ -260,9 +265,23 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         return fail(PGPU_ERR_UNSUPPORTED, "too many points for one batch (%llu)",
                     (unsigned long long)n_total);
 
+    // Vertex-ordered rows: where every image takes the tile splat with one-word keys that
+    // hold their vertex index (d <= 6) and the slice replays the splat points, the splat
+    // numbers the vertices as it creates them and accumulates straight into
+    // vertex-ordered FP32 rows, so no compaction runs; the first blur pass reads those
+    // sums (16-bit payloads: FP32 rows, homogeneous ones normalised as they are read) and
+    // the slice reads rows by vertex index.
+    // PGPU_ROWS=slot in the environment keeps slot-space rows (the parity tests compare both).
+    const char* rows_mode = std::getenv("PGPU_ROWS");
+    const bool vrows = !exact_order && B.replay && kw == 1 && index_in_key(d) && tiled_count == nseg &&
+                       B.payload != kPayloadF64 && !B.slot_rows &&
+                       !(rows_mode && !strcmp(rows_mode, "slot"));
+    // 16-bit payloads accumulate in FP32 rows (vf32), which the first blur pass reads
+    const bool f32_rows = vrows && (B.payload == kPayloadF16 || B.payload == kPayloadBF16);
     const MetaLayout L = layout(nseg, !B.replay);
     int rc;
-    if ((rc = E.ensure_hmeta(L.total)) || (rc = E.meta.ensure(L.total))) return rc;
+    if ((!h_in && (rc = E.ensure_hmeta(L.total))) || (rc = E.meta.ensure(L.total))) return rc;
+    if (h_in && !B.replay) return fail(PGPU_ERR_UNSUPPORTED, "queued passes replay the splat points");
 
     {
         std::vector<uint64_t> sbase(nseg + 1);
@@ -285,7 +304,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             (rc = E.vkey0.ensure(cap_total * 16)) || (rc = E.vkeyn.ensure((kw - 1) * cap_total * 16)) ||
             (rc = E.vv0.ensure(cap_total * vdp * payb)) || (rc = E.vv1.ensure(cap_total * vdp * payb)) ||
             (rc = E.nbr.ensure((size_t)(d + 1) * cap_total * 8)) ||
-            (homog && (rc = E.vf32.ensure(cap_total * vdp * 4))) ||
+            ((homog || f32_rows) && (rc = E.vf32.ensure(cap_total * vdp * 4))) ||
             (rc = E.vtx2slot.ensure(cap_total * 4)) || (rc = E.sval.ensure(cap_total * vdp * accb)) ||
             (use_tags && (rc = E.tags.ensure(cap_total))) ||
             (B.replay && (rc = E.rec.ensure((size_t)entries * 4))) ||
@@ -293,7 +312,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             return rc;
 
         // per-lattice descriptors, staged in pinned memory and uploaded by the first copy
-        unsigned char* h = E.hmeta;
+        unsigned char* h = h_in ? h_in : E.hmeta;
         uint32_t* hslot = (uint32_t*)(h + L.slotbase);
         uint32_t* hentry = (uint32_t*)(h + L.entry);
         Segment* hseg = (Segment*)(h + L.segs);
@@ -322,7 +341,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
                                      cudaMemcpyHostToDevice, st));
             CUDA_TRY(cudaMemsetAsync(dmeta, 0, L.slotbase, st));
             CUDA_TRY(cudaMemsetAsync(E.key0.p, 0xFF, cap_total * 16, st));
-            CUDA_TRY(cudaMemsetAsync(E.tvals.p, 0, cap_total * vdp * accb, st));
+            if (!vrows) CUDA_TRY(cudaMemsetAsync(E.tvals.p, 0, cap_total * vdp * accb, st));
             if (exact_order) {
                 CUDA_TRY(cudaMemsetAsync(E.ft.p, 0xFF, cap_total * 4, st));
                 CUDA_TRY(cudaMemsetAsync(E.bitmap.p, 0, (size_t)nwords * 4, st));
@@ -340,7 +359,17 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             sa.cap_total = (uint32_t)cap_total;
             sa.vals = E.tvals.p;
             sa.ft = exact_order ? (uint32_t*)E.ft.p : nullptr;
-            sa.vlist = exact_order ? nullptr : (uint32_t*)E.vlist.p;
+            sa.vlist = (exact_order || vrows) ? nullptr : (uint32_t*)E.vlist.p;
+            if (vrows) {
+                sa.vrows = (homog || f32_rows) ? E.vf32.p : E.vv0.p;
+                sa.vkey0 = (uint4*)E.vkey0.p;
+                sa.vtx2slot = (uint32_t*)E.vtx2slot.p;
+                if (B.nbr_half) {
+                    sa.nbr_init = (int2*)E.nbr.p;
+                    sa.nbr_stride = (uint32_t)cap_total;
+                    sa.nbr_axes = d + 1;
+                }
+            }
             sa.vcount = dM;
             sa.seg_counts = (uint32_t*)(dmeta + L.counts);
             sa.rec_slot = B.replay ? (uint32_t*)E.rec.p : nullptr;
@@ -364,6 +393,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             }
             CompactArgs ca;
             memset(&ca, 0, sizeof(ca));
+            if (!vrows) {
             ca.table = TableView{(uint4*)E.key0.p, (uint4*)E.keyn.p, (uint32_t)cap_total, (uint32_t)cap_total};
             ca.ft = (const uint32_t*)E.ft.p;
             ca.bitmap = (uint32_t*)E.bitmap.p;
@@ -384,6 +414,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             if (!launch_assign(ca, kw, vdp, B.payload, homog, E.sms, st))
                 return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
             CUDA_TRY(cudaGetLastError());
+            }
             if (B.dump_splat)
                 CUDA_TRY(cudaMemcpyAsync(B.dump_splat, E.vv0.p,
                                          std::min<size_t>(cap_total * vdp * payb, B.dump_bytes),
@@ -405,6 +436,7 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             na.nbr = (int2*)E.nbr.p;
             na.tags = use_tags ? (const uint8_t*)E.tags.p : nullptr;
             na.seg_status = (const unsigned*)(dmeta + L.segstat);
+            na.half = (vrows && B.nbr_half) ? 1 : 0;
             ops->neighbours(na, (uint32_t)cap_total, E.sms, st);
             CUDA_TRY(cudaGetLastError());
             if (timed) CUDA_TRY(cudaEventRecord(E.ev[3], st));
@@ -414,19 +446,21 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             bp.vdp = vdp;
             bp.payload = B.payload;
             bp.homog = homog;
-            bp.src_f32 = homog;
+            bp.src_f32 = homog || f32_rows;
+            bp.raw = vrows && homog;
             bp.nbr = (const int2*)E.nbr.p;
             bp.nbr_stride = cap_total;
             bp.nverts = dM;
             bp.vmax = (uint32_t)cap_total;
-            bp.src = homog ? E.vf32.p : E.vv0.p;
+            bp.src = (homog || f32_rows) ? E.vf32.p : E.vv0.p;
             bp.bufs[0] = E.vv1.p;
             bp.bufs[1] = E.vv0.p;
             bp.sval = E.sval.p;
-            bp.vtx2slot = (const uint32_t*)E.vtx2slot.p;
+            bp.vtx2slot = vrows ? nullptr : (const uint32_t*)E.vtx2slot.p;   // null: vertex order
             bp.wc = vd - 1;
             bp.sms = E.sms;
             bp.pairs = B.blur_pairs;
+            bp.grid = B.blur_grid;
             if (blur_all_axes(bp, st)) return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
             CUDA_TRY(cudaGetLastError());
             if (timed) CUDA_TRY(cudaEventRecord(E.ev[4], st));
@@ -459,12 +493,14 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             // the graph bakes in sizes, settings and buffer addresses, so all of them key it
             std::vector<uint64_t> gk = {
                 (uint64_t)d, (uint64_t)vd, (uint64_t)B.payload, (uint64_t)homog, (uint64_t)B.replay,
-                (uint64_t)nseg, n_total, ns_total, cap_total, nwords, (uint64_t)B.blur_pairs, blocks,
+                (uint64_t)nseg, n_total, ns_total, cap_total, nwords, (uint64_t)B.blur_pairs,
+                (uint64_t)B.blur_grid, blocks,
                 tile_blocks, slice_blocks, (uint64_t)(uintptr_t)E.key0.p, (uint64_t)(uintptr_t)E.keyn.p,
                 (uint64_t)(uintptr_t)E.tvals.p, (uint64_t)(uintptr_t)E.nbr.p, (uint64_t)(uintptr_t)E.rec.p,
-                (uint64_t)(uintptr_t)E.recw.p, (uint64_t)(uintptr_t)E.meta.p, (uint64_t)(uintptr_t)E.hmeta,
+                (uint64_t)(uintptr_t)E.recw.p, (uint64_t)(uintptr_t)E.meta.p, (uint64_t)(uintptr_t)h,
                 (uint64_t)(uintptr_t)E.sval.p, (uint64_t)(uintptr_t)E.vlist.p, (uint64_t)(uintptr_t)E.vv0.p,
-                (uint64_t)(uintptr_t)E.vv1.p, (uint64_t)(uintptr_t)E.vkey0.p, (uint64_t)(uintptr_t)E.vf32.p};
+                (uint64_t)(uintptr_t)E.vv1.p, (uint64_t)(uintptr_t)E.vkey0.p, (uint64_t)(uintptr_t)E.vf32.p,
+                (uint64_t)vrows, (uint64_t)(uintptr_t)E.vtx2slot.p, (uint64_t)B.nbr_half};
             gk.reserve(gk.size() + 2 * (size_t)nseg);
             for (int k = 0; k < nseg; ++k) {
                 gk.push_back(cap[k]);
@@ -488,98 +524,189 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
                 if (ie != cudaSuccess) return fail(PGPU_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
                 it = E.graphs.emplace(gk, ex).first;
             }
-            CUDA_TRY(cudaEventRecord(E.ev[0], st));
+            if (timed) CUDA_TRY(cudaEventRecord(E.ev[0], st));
             CUDA_TRY(cudaGraphLaunch(it->second, st));
-            CUDA_TRY(cudaEventRecord(E.ev[5], st));
+            if (timed) CUDA_TRY(cudaEventRecord(E.ev[5], st));
         } else {
-            if ((rc = enqueue(true))) return rc;
+            if ((rc = enqueue(timed))) return rc;
         }
-        CUDA_TRY(cudaStreamSynchronize(st));
-
-        const uint32_t M = ((const uint32_t*)h)[1];
-        const unsigned* segstat = (const unsigned*)(h + L.segstat);
-        const uint32_t* counts = (const uint32_t*)(h + L.counts);
-        bool retry = false;
-        for (int k = 0; k < nseg; ++k) {
-            if (segstat[k] & kStatusKeyRange)
-                return fail(PGPU_ERR_ARGUMENT,
-                            "image %d: positions leave the lattice's int16 key range (the reference's "
-                            "keys wrap there and its rank indices leave [0, d]); scale them down", k);
-            if (segstat[k] & (kStatusProbeLimit | kStatusSpinLimit)) {
-                uint64_t c = std::max<uint64_t>((uint64_t)(cap[k] * 2.5), (uint64_t)(counts[k] / load * 2));
-                failed->push_back(k);
-                cap_next->push_back((c + 31) & ~31ull);
-                retry = true;
-            }
-        }
-
-        double rmax = 0.0;
-        uint64_t done_vertices = 0;
-        size_t fi = 0;
-        {
-            std::lock_guard<std::mutex> lk(g_ratio_mu);
-            if (g_ratio_by_sig.size() > 4096) g_ratio_by_sig.clear();
-            for (int k = 0; k < nseg; ++k) {
-                if (fi < failed->size() && (*failed)[fi] == k) {
-                    ++fi;
-                    continue;
-                }
-                done_vertices += counts[k];
-                if (!B.items[k].n) continue;
-                const double r = (double)counts[k] / (double)B.items[k].n;
-                g_ratio_by_sig[sig[k]] = r;
-                rmax = std::max(rmax, r);
-            }
-            if (!retry) g_ratio[d] = rmax;
-        }
-        E.last_cap = cap_total;
-        if (B.vertices_out && !retry) B.vertices_out->assign(counts, counts + nseg);
-
-        pgpu_stats s;
-        memset(&s, 0, sizeof(s));
-        s.points = (long long)n_total;
-        s.vertices = retry ? (long long)done_vertices : (long long)M;
-        s.capacity = (long long)cap_total;
-        s.d = d;
-        s.vd = vd;
-        s.payload = B.payload;
-        s.retries = pass;
-        s.load_factor = load;
-        s.blur_pairs = B.blur_pairs ? 1 : 0;
-        s.tiled = tiled_count;
-        if (!graph) {
-            cudaEventElapsedTime(&s.ms_splat, E.ev[0], E.ev[1]);
-            cudaEventElapsedTime(&s.ms_compact, E.ev[1], E.ev[2]);
-            cudaEventElapsedTime(&s.ms_neighbours, E.ev[2], E.ev[3]);
-            cudaEventElapsedTime(&s.ms_blur, E.ev[3], E.ev[4]);
-            cudaEventElapsedTime(&s.ms_slice, E.ev[4], E.ev[5]);
-            cudaEventElapsedTime(&s.ms_total, E.ev[6], E.ev[5]);
-        } else {
-            cudaEventElapsedTime(&s.ms_total, E.ev[0], E.ev[5]);
-        }
-        set_stats(s);
+        ps->h = h;
+        ps->segstat = L.segstat;
+        ps->counts = L.counts;
+        ps->cap = cap;
+        ps->sig = sig;
+        ps->load = load;
+        ps->tiled = tiled_count;
+        ps->pass = pass;
+        ps->n_total = n_total;
+        ps->cap_total = cap_total;
+        ps->timed = timed ? (graph ? 2 : 1) : 0;
+        ps->nbr_half = (vrows && B.nbr_half) ? 1 : 0;
+        ps->vertex_rows = vrows ? 1 : 0;
         return PGPU_OK;
     }
 }
 
-// Every image of a batch is filtered in place, so an image whose range overflowed cannot
-// simply be rerun with its whole batch: the others are finished.  Only the overflowed
-// ones go again, as a smaller batch with larger ranges.  The statistics cover all passes.
-// Autotuner candidates: hash-table load factor, blur pairing and the splat kernel (the
-// tile splat wherever the learned vertex density allows it, or the direct splat for every
-// image).  The first calls of a batch shape try them in turn; later calls of the shape use
-// the fastest by the lattice's device time.  Keys, vertex order and FP32/FP64 results do not depend on the choice; a
-// 16-bit payload tries fused pairs only, because one axis per pass rounds its rows to 16
-// bits between axes, which the pair keeps in FP32 registers.
-struct TuneCandidate {
-    float load;
-    bool pairs;
-    int splat;   // BatchJob::splat
-};
-// the last candidate (one axis per pass) only for FP32/FP64 payloads
-constexpr TuneCandidate kTune[] = {{0.5f, true, 0}, {0.35f, true, 0}, {0.7f, true, 0},
-                                   {0.5f, true, 1}, {0.5f, false, 0}};
-constexpr int kTuneCount = (int)(sizeof(kTune) / sizeof(kTune[0]));
+// The rest of a pass once st has run it: statuses, learned ratios, statistics.  Images
+// whose range overflowed are listed in *failed, with the larger range to use in *cap_next
+// (when given); their output is untouched (the slice skips them), while every other image
+// of the pass is finished.
+static int finish_pass(Engine& E, const BatchJob& B, const PassState& ps, std::vector<int>* failed,
+                       std::vector<uint64_t>* cap_next) {
+    const int d = B.d, nseg = (int)B.items.size();
+    if (nseg == 0) return PGPU_OK;
+    const unsigned char* h = ps.h;
+    const uint32_t M = ((const uint32_t*)h)[1];
+    const unsigned* segstat = (const unsigned*)(h + ps.segstat);
+    const uint32_t* counts = (const uint32_t*)(h + ps.counts);
+    bool retry = false;
+    for (int k = 0; k < nseg; ++k) {
+        if (segstat[k] & kStatusKeyRange)
+            return fail(PGPU_ERR_ARGUMENT,
+                        "image %d: positions leave the lattice's int16 key range (the reference's "
+                        "keys wrap there and its rank indices leave [0, d]); scale them down", k);
+        if (segstat[k] & (kStatusProbeLimit | kStatusSpinLimit)) {
+            uint64_t c = std::max<uint64_t>((uint64_t)(ps.cap[k] * 2.5), (uint64_t)(counts[k] / ps.load * 2));
+            failed->push_back(k);
+            if (cap_next) cap_next->push_back((c + 31) & ~31ull);
+            retry = true;
+        }
+    }
+
+    double rmax = 0.0;
+    uint64_t done_vertices = 0;
+    size_t fi = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_ratio_mu);
+        if (g_ratio_by_sig.size() > 4096) g_ratio_by_sig.clear();
+        for (int k = 0; k < nseg; ++k) {
+            if (fi < failed->size() && (*failed)[fi] == k) {
+                ++fi;
+                continue;
+            }
+            done_vertices += counts[k];
+            if (!B.items[k].n) continue;
+            const double r = (double)counts[k] / (double)B.items[k].n;
+            g_ratio_by_sig[ps.sig[k]] = r;
+            rmax = std::max(rmax, r);
+        }
+        if (!retry) g_ratio[d] = rmax;
+    }
+    E.last_cap = ps.cap_total;
+    if (B.vertices_out && !retry) B.vertices_out->assign(counts, counts + nseg);
+
+    pgpu_stats s;
+    memset(&s, 0, sizeof(s));
+    s.points = (long long)ps.n_total;
+    s.vertices = retry ? (long long)done_vertices : (long long)M;
+    s.capacity = (long long)ps.cap_total;
+    s.d = d;
+    s.vd = B.vd;
+    s.payload = B.payload;
+    s.retries = ps.pass;
+    s.load_factor = ps.load;
+    s.blur_pairs = B.blur_pairs ? 1 : 0;
+    s.blur_grid = B.blur_grid;
+    s.nbr_half = ps.nbr_half;
+    s.vertex_rows = ps.vertex_rows;
+    s.tiled = ps.tiled;
+    if (ps.timed == 1) {
+        cudaEventElapsedTime(&s.ms_splat, E.ev[0], E.ev[1]);
+        cudaEventElapsedTime(&s.ms_compact, E.ev[1], E.ev[2]);
+        cudaEventElapsedTime(&s.ms_neighbours, E.ev[2], E.ev[3]);
+        cudaEventElapsedTime(&s.ms_blur, E.ev[3], E.ev[4]);
+        cudaEventElapsedTime(&s.ms_slice, E.ev[4], E.ev[5]);
+        cudaEventElapsedTime(&s.ms_total, E.ev[6], E.ev[5]);
+    } else if (ps.timed == 2) {
+        cudaEventElapsedTime(&s.ms_total, E.ev[0], E.ev[5]);
+    }
+    set_stats(s);
+    return PGPU_OK;
+}
+
+static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
+                          const std::vector<uint64_t>* cap_in, std::vector<int>* failed,
+                          std::vector<uint64_t>* cap_next, int pass) {
+    if (B.items.empty()) return PGPU_OK;
+    PassState ps;
+    int rc;
+    if ((rc = enqueue_pass(E, B, st, cap_in, nullptr, true, pass, &ps))) return rc;
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return finish_pass(E, B, ps, failed, cap_next);
+}
+
+// Autotuner: coordinate descent over four knobs, starting from load 0.5, blur axes in
+// pairs, the capped blur grid and the tile splat.  Each knob's options are tried with the
+// best setting found so far for the other knobs, each twice (the faster time counts: the
+// first call of a shape also learns its vertex ratio), by the lattice's device time:
+//   0. hash-table load factor 0.5 / 0.35 / 0.7;
+//   1. blur passes: axes fused in pairs, or one axis per pass (FP32/FP64 payloads only:
+//      one axis per pass would round 16-bit rows between axes, which a pair keeps in FP32
+//      registers, so 16-bit results would depend on the choice);
+//   2. blur grid: 16 blocks per SM striding over the vertices, one vertex per thread, or
+//      (one-axis passes) 16 blocks per SM with two vertices per iteration;
+//   3. splat: the tile splat wherever the learned vertex density allows it, or the direct
+//      splat for every image;
+//   4. neighbour search (vertex-ordered rows only): two lookups per axis, or one (n1) with
+//      the other pair entry written by the neighbour found (n2(n1(v)) = v).
+// Keys, vertex order and FP32/FP64 results do not depend on the choice.
+constexpr float kTuneLoads[] = {0.5f, 0.35f, 0.7f};
+constexpr int kTuneKnobs = 5;
+constexpr int kTuneReps = 2;
+
+static int knob_options(int k) { return k == 0 || k == 2 ? 3 : 2; }
+
+static Engine::Tuning::Setting with_option(Engine::Tuning::Setting s, int k, int o) {
+    switch (k) {
+    case 0: s.load = kTuneLoads[o]; break;
+    case 1: s.pairs = o == 0; break;
+    case 2: s.blur_grid = o; break;
+    case 3: s.splat = o; break;
+    case 4: s.nbr_half = o; break;
+    }
+    return s;
+}
+
+static bool same_setting(const Engine::Tuning::Setting& a, const Engine::Tuning::Setting& b) {
+    return a.load == b.load && a.pairs == b.pairs && a.blur_grid == b.blur_grid && a.splat == b.splat &&
+           a.nbr_half == b.nbr_half;
+}
+
+// the next setting to try (skipping options that are the best setting itself, already
+// timed, and options the payload does not allow); false once every knob is done
+static bool tune_next(Engine::Tuning& t, bool singles_ok, Engine::Tuning::Setting* out) {
+    while (t.knob < kTuneKnobs) {
+        if (t.option >= knob_options(t.knob)) {
+            ++t.knob;
+            t.option = 0;
+            continue;
+        }
+        const Engine::Tuning::Setting c = with_option(t.best, t.knob, t.option);
+        const bool timed_already = t.best_ms < 1e29f && same_setting(c, t.best);
+        // two vertices per blur iteration exist for one-axis passes only
+        if (timed_already || (!singles_ok && !c.pairs) || (c.pairs && c.blur_grid == 2)) {
+            ++t.option;
+            continue;
+        }
+        *out = c;
+        return true;
+    }
+    t.done = true;
+    return false;
+}
+
+static void tune_record(Engine::Tuning& t, const Engine::Tuning::Setting& c, float ms) {
+    ++t.trials;
+    t.cur_ms = std::min(t.cur_ms, ms);
+    if (++t.rep < kTuneReps) return;
+    if (t.cur_ms < t.best_ms) {
+        t.best_ms = t.cur_ms;
+        t.best = c;
+    }
+    t.cur_ms = 1e30f;
+    t.rep = 0;
+    ++t.option;
+}
 
 static std::string tune_key(const BatchJob& B) {
     uint64_t n = 0;
@@ -592,19 +719,52 @@ static std::string tune_key(const BatchJob& B) {
     return buf;
 }
 
+static bool tunable(const BatchJob& B) { return B.autotune && !B.rec_vtx && !B.dump_splat; }
+static bool singles_allowed(const BatchJob& B) {
+    return B.payload != kPayloadF16 && B.payload != kPayloadBF16;
+}
+static void apply_setting(BatchJob& B, const Engine::Tuning::Setting& s) {
+    B.load = s.load;
+    B.blur_pairs = s.pairs;
+    B.blur_grid = s.blur_grid;
+    B.splat = s.splat;
+    B.nbr_half = s.nbr_half;
+}
+
+bool tuned_settings(Engine& E, const BatchJob& B, BatchJob* out) {
+    *out = B;
+    if (!tunable(B)) return true;
+    auto it = E.tuning.find(tune_key(B));
+    if (it == E.tuning.end() || !it->second.done) return false;
+    apply_setting(*out, it->second.best);
+    return true;
+}
+
+int enqueue_batch(Engine& E, const BatchJob& B, cudaStream_t st, unsigned char* h, PassState* ps) {
+    return enqueue_pass(E, B, st, nullptr, h, false, 0, ps);
+}
+
+int finish_batch(Engine& E, const BatchJob& B, const PassState& ps, std::vector<int>* failed) {
+    return finish_pass(E, B, ps, failed, nullptr);
+}
+
+// Every image of a batch is filtered in place, so an image whose range overflowed cannot
+// simply be rerun with its whole batch: the others are finished.  Only the overflowed
+// ones go again, as a smaller batch with larger ranges.  The statistics cover all passes.
 int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
     if (B.items.empty()) return PGPU_OK;
     BatchJob cur = B;
-    int cand = -1;
     Engine::Tuning* tune = nullptr;
-    if (B.autotune && !B.rec_vtx && !B.dump_splat) {
+    Engine::Tuning::Setting trial;
+    if (tunable(B)) {
         if (E.tuning.size() > 1024) E.tuning.clear();
-        tune = &E.tuning[tune_key(B)];
-        tune->count = (B.payload == kPayloadF16 || B.payload == kPayloadBF16) ? kTuneCount - 1 : kTuneCount;
-        cand = tune->trials < tune->count ? tune->trials : tune->best;
-        cur.load = kTune[cand].load;
-        cur.blur_pairs = kTune[cand].pairs;
-        cur.splat = kTune[cand].splat;
+        Engine::Tuning& t = E.tuning[tune_key(B)];
+        if (!t.done && tune_next(t, singles_allowed(B), &trial)) {
+            tune = &t;
+            apply_setting(cur, trial);
+        } else {
+            apply_setting(cur, t.best);
+        }
     }
     std::vector<uint64_t> caps;
     pgpu_stats sum;
@@ -627,17 +787,13 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
         if (failed.empty()) {
             sum.load_factor = s.load_factor;
             sum.blur_pairs = s.blur_pairs;
+            sum.blur_grid = s.blur_grid;
+            sum.nbr_half = s.nbr_half;
+            sum.vertex_rows = s.vertex_rows;
             sum.tiled = s.tiled;
+            sum.tuned = tune ? 1 : tunable(B) ? 2 : 0;
+            if (tune) tune_record(*tune, trial, sum.ms_total);
             set_stats(sum);
-            if (tune && tune->trials < tune->count) {
-                tune->ms[tune->trials++] = sum.ms_total;
-                if (tune->trials == tune->count) {
-                    int best = 0;
-                    for (int c = 1; c < tune->count; ++c)
-                        if (tune->ms[c] < tune->ms[best]) best = c;
-                    tune->best = best;
-                }
-            }
             return PGPU_OK;
         }
         BatchJob again = cur;

@@ -448,7 +448,8 @@ struct ApiScope {
     std::unique_lock<std::mutex> lock;
     cudaStream_t st = nullptr;
     int rc = PGPU_OK;
-    ApiScope(const pgpu_options* opt) {
+    // queue: a submission, which leaves the batches queued before it running
+    ApiScope(const pgpu_options* opt, bool queue = false) {
         clear_error();
         const int dev = opt ? opt->device : 0;
         rc = get_engine(dev, &E);
@@ -457,6 +458,11 @@ struct ApiScope {
         if (cudaSetDevice(dev) != cudaSuccess) {
             rc = fail(PGPU_ERR_CUDA, "cudaSetDevice(%d) failed", dev);
             return;
+        }
+        if (!queue && !E->async_q.empty()) {
+            set_call_stream(E->stream);
+            drain_async(*E);
+            clear_error();
         }
         const bool device = opt && opt->memory == PGPU_MEM_DEVICE;
         st = (device && opt->stream) ? (cudaStream_t)opt->stream : E->stream;
@@ -531,12 +537,141 @@ void bilateral_job(const pgpu_image* dv, int i0, int i1, const float* filter_wid
 // is uploaded on one copy stream and chunk k-1 downloaded on the other, so with pinned host
 // images the transfers hide behind the filtering.  (With two slots, the upload of chunk
 // k+1 would wait for the download of chunk k-1 from the same slot.)  A batch smaller than two
-// chunks is one chunk.  The reported statistics sum over the chunks.
+// chunks is one chunk.  The reported statistics sum over the chunks.  The slots keep turning
+// from one call to the next, so a queued batch (pgpu_bilateral_batch_submit) uploads its
+// first chunks while the previous batch's last chunks are filtered and downloaded.
 constexpr size_t kChunkPixels = size_t(1) << 22;
 
-int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int count,
-                         const float* filter_width, const float* color_sigma,
-                         const pgpu_options& opt) {
+}  // namespace
+
+namespace pgpu {
+// One queued chunk of a submitted host batch: its lattice job (device slot views), the
+// queued pass and the pinned buffer its metadata is staged in.
+struct AsyncChunk {
+    BatchJob job;
+    PassState ps;
+    unsigned char* h = nullptr;
+    size_t h_bytes = 0;
+    int i0 = 0, i1 = 0;
+};
+
+struct AsyncBatch {
+    long long id = 0;
+    std::vector<pgpu_image> in, out;
+    std::vector<float> fw, cs;
+    pgpu_options opt;
+    std::vector<AsyncChunk> chunks;
+    cudaEvent_t done = nullptr;   // on the download stream after the last download
+};
+}  // namespace pgpu
+
+namespace {
+
+unsigned char* pinned_get(Engine& E, size_t need, size_t* got) {
+    for (size_t i = 0; i < E.pinned_free.size(); ++i) {
+        if (E.pinned_free[i].second >= need) {
+            unsigned char* p = E.pinned_free[i].first;
+            *got = E.pinned_free[i].second;
+            E.pinned_free.erase(E.pinned_free.begin() + i);
+            return p;
+        }
+    }
+    unsigned char* p = nullptr;
+    const size_t nb = std::max<size_t>(need, 65536);
+    if (cudaHostAlloc((void**)&p, nb, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    *got = nb;
+    return p;
+}
+
+void pinned_put(Engine& E, unsigned char* p, size_t bytes) {
+    if (p) E.pinned_free.emplace_back(p, bytes);
+}
+
+int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, const pgpu_image* outs,
+                         int count, const float* filter_width, const float* color_sigma,
+                         const pgpu_options& opt, AsyncBatch* ab);
+
+// Finish the oldest queued batch (its download stream has reached its event): statuses and
+// learned ratios of every chunk; images whose hash range overflowed were left unfiltered
+// and are filtered again here, synchronously, once every stream is idle.
+void complete_oldest(Engine& E) {
+    AsyncBatch* ab = E.async_q.front();
+    E.async_q.pop_front();
+    int rc = PGPU_OK;
+    std::string msg;
+    const cudaError_t ce = cudaEventSynchronize(ab->done);
+    if (ce != cudaSuccess) {
+        rc = fail(PGPU_ERR_CUDA, "queued batch: %s", cudaGetErrorString(ce));
+        msg = last_error();
+    }
+    std::vector<int> again;
+    pgpu_stats sum;
+    memset(&sum, 0, sizeof(sum));
+    for (AsyncChunk& c : ab->chunks) {
+        if (rc) break;
+        std::vector<int> failed;
+        const int r = finish_batch(E, c.job, c.ps, &failed);
+        if (r) {
+            rc = r;
+            msg = last_error();
+            break;
+        }
+        pgpu_stats s;
+        if (get_stats(&s)) {
+            sum.points += s.points, sum.vertices += s.vertices;
+            sum.capacity = std::max(sum.capacity, s.capacity);
+            sum.d = s.d, sum.vd = s.vd, sum.payload = s.payload;
+            sum.load_factor = s.load_factor, sum.blur_pairs = s.blur_pairs;
+            sum.blur_grid = s.blur_grid;
+            sum.nbr_half = s.nbr_half;
+            sum.vertex_rows = s.vertex_rows;
+            sum.tuned = c.job.autotune ? 2 : 0;
+            sum.tiled += s.tiled;
+        }
+        for (int k : failed) again.push_back(c.i0 + k);
+    }
+    if (!rc && !again.empty()) {
+        // the slots may hold later batches' images: wait for everything queued
+        cudaStreamSynchronize(E.copy_in);
+        cudaStreamSynchronize(E.stream);
+        cudaStreamSynchronize(E.copy_out);
+        std::vector<pgpu_image> in, out;
+        std::vector<float> fw, cs;
+        for (int i : again) {
+            in.push_back(ab->in[i]);
+            out.push_back(ab->out[i]);
+            fw.push_back(ab->fw[i]);
+            cs.push_back(ab->cs[i]);
+        }
+        rc = bilateral_batch_host(E, E.stream, in.data(), out.data(), (int)in.size(), fw.data(), cs.data(),
+                                  ab->opt, nullptr);
+        if (rc) msg = last_error();
+        else sum.retries = 1;
+    }
+    if (!rc) set_stats(sum);
+    for (AsyncChunk& c : ab->chunks) pinned_put(E, c.h, c.h_bytes);
+    if (ab->done) cudaEventDestroy(ab->done);
+    E.async_done[ab->id] = std::make_pair(rc, msg);
+    if (E.async_done.size() > 4096) E.async_done.erase(E.async_done.begin());
+    delete ab;
+}
+
+}  // namespace
+
+// Every call but a submission first finishes the queued batches: they share the device
+// slots, the workspace and the copy streams.
+void pgpu::drain_async(Engine& E) {
+    while (!E.async_q.empty()) complete_oldest(E);
+}
+
+namespace {
+
+int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, const pgpu_image* outs,
+                         int count, const float* filter_width, const float* color_sigma,
+                         const pgpu_options& opt, AsyncBatch* ab) {
     const int C = ims[0].channels;
     std::vector<int> cut{0};
     size_t acc = 0, slot_floats = 0, chunk_floats = 0;
@@ -551,28 +686,41 @@ int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int 
         }
     }
     const int nchunks = (int)cut.size() - 1;
+    DevBuf* slots[3] = {&E.img_a, &E.img_b, &E.img_c};
+    const size_t slot_bytes = slot_floats * sizeof(float);
+    // a slot that must grow may still be read by queued batches: finish them first
+    for (DevBuf* b : slots)
+        if (b->bytes < slot_bytes && !E.async_q.empty()) drain_async(E);
     int rc;
-    if ((rc = E.img_a.ensure(slot_floats * sizeof(float))) ||
-        (nchunks > 1 && (rc = E.img_b.ensure(slot_floats * sizeof(float)))) ||
-        (nchunks > 2 && (rc = E.img_c.ensure(slot_floats * sizeof(float)))) ||
-        (rc = E.ensure_copy_streams()))
-        return rc;
+    bool grown = false;
+    for (DevBuf* b : slots) {
+        const void* before = b->p;
+        if ((rc = b->ensure(slot_bytes))) return rc;
+        grown |= b->p != before;
+    }
+    const bool fresh_streams = !E.copy_in;
+    if ((rc = E.ensure_copy_streams())) return rc;
     cudaStream_t cin = E.copy_in, cout = E.copy_out;
-    // the slots were allocated in order on the compute stream: the copy streams start after
-    CUDA_TRY(cudaEventRecord(E.join_ev[0], st));
-    CUDA_TRY(cudaStreamWaitEvent(cin, E.join_ev[0], 0));
-    CUDA_TRY(cudaStreamWaitEvent(cout, E.join_ev[0], 0));
+    // slots (re)allocated in order on the compute stream: the copy streams start after it.
+    // Otherwise they do not wait for the compute stream, so a queued batch's uploads run
+    // while the previous batch is still being filtered.
+    if (grown || fresh_streams) {
+        CUDA_TRY(cudaEventRecord(E.join_ev[0], st));
+        CUDA_TRY(cudaStreamWaitEvent(cin, E.join_ev[0], 0));
+        CUDA_TRY(cudaStreamWaitEvent(cout, E.join_ev[0], 0));
+    }
     cudaEvent_t* uploaded = E.pipe_ev;
     cudaEvent_t* filtered = E.pipe_ev + 3;
     cudaEvent_t* downloaded = E.pipe_ev + 6;
-    bool slot_used[3] = {false, false, false};
-    DevBuf* slots[3] = {&E.img_a, &E.img_b, &E.img_c};
+    std::vector<int> slot_of(nchunks);
+    for (int k = 0; k < nchunks; ++k) slot_of[k] = (E.slot_next + k) % 3;
+    E.slot_next = (E.slot_next + nchunks) % 3;
     std::vector<pgpu_image> dv(ims, ims + count);
 
     auto upload = [&](int k) -> int {
-        const int slot = k % 3;
+        const int slot = slot_of[k];
         float* base = (float*)slots[slot]->p;
-        if (slot_used[slot]) CUDA_TRY(cudaStreamWaitEvent(cin, downloaded[slot], 0));
+        if (E.slot_recorded[slot]) CUDA_TRY(cudaStreamWaitEvent(cin, downloaded[slot], 0));
         size_t off = 0;
         for (int i = cut[k]; i < cut[k + 1]; ++i) {
             dv[i] = dense_like(ims[i], base + off, C);
@@ -583,42 +731,69 @@ int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, int 
         CUDA_TRY(cudaEventRecord(uploaded[slot], cin));
         return PGPU_OK;
     };
+    auto download = [&](int k) -> int {
+        const int slot = slot_of[k];
+        CUDA_TRY(cudaEventRecord(filtered[slot], st));
+        CUDA_TRY(cudaStreamWaitEvent(cout, filtered[slot], 0));
+        for (int i = cut[k]; i < cut[k + 1]; ++i) {
+            const int r = copy_view(dv[i], outs[i], C, cudaMemcpyDeviceToHost, cout);
+            if (r) return r;
+        }
+        CUDA_TRY(cudaEventRecord(downloaded[slot], cout));
+        E.slot_recorded[slot] = true;
+        return PGPU_OK;
+    };
     auto run = [&]() -> int {
         pgpu_stats sum;
         memset(&sum, 0, sizeof(sum));
         int r = upload(0);
         for (int k = 0; k < nchunks && !r; ++k) {
-            const int slot = k % 3;
             if (k + 1 < nchunks && (r = upload(k + 1))) break;
-            CUDA_TRY(cudaStreamWaitEvent(st, uploaded[slot], 0));
+            CUDA_TRY(cudaStreamWaitEvent(st, uploaded[slot_of[k]], 0));
             BatchJob B;
             bilateral_job(dv.data(), cut[k], cut[k + 1], filter_width, color_sigma, opt, B);
-            if ((r = run_batch(E, B, st))) break;
-            pgpu_stats s;
-            if (get_stats(&s)) {
-                sum.points += s.points;
-                sum.vertices += s.vertices;
-                sum.capacity = std::max(sum.capacity, s.capacity);
-                sum.d = s.d, sum.vd = s.vd, sum.payload = s.payload;
-                sum.load_factor = s.load_factor, sum.blur_pairs = s.blur_pairs;
-                sum.tiled += s.tiled;
-                sum.retries += s.retries;
-                sum.ms_splat += s.ms_splat, sum.ms_compact += s.ms_compact;
-                sum.ms_neighbours += s.ms_neighbours, sum.ms_blur += s.ms_blur;
-                sum.ms_slice += s.ms_slice, sum.ms_total += s.ms_total;
+            if (ab) {
+                // queued: the autotuner's choice, no host wait (checked when it completes)
+                AsyncChunk c;
+                c.i0 = cut[k];
+                c.i1 = cut[k + 1];
+                tuned_settings(E, B, &c.job);
+                c.h = pinned_get(E, batch_meta_bytes((int)c.job.items.size()), &c.h_bytes);
+                if (!c.h) return fail(PGPU_ERR_MEMORY, "pinned allocation for a queued batch failed");
+                ab->chunks.push_back(std::move(c));
+                AsyncChunk& q = ab->chunks.back();
+                if ((r = enqueue_batch(E, q.job, st, q.h, &q.ps))) break;
+            } else {
+                if ((r = run_batch(E, B, st))) break;
+                pgpu_stats s;
+                if (get_stats(&s)) {
+                    sum.points += s.points;
+                    sum.vertices += s.vertices;
+                    sum.capacity = std::max(sum.capacity, s.capacity);
+                    sum.d = s.d, sum.vd = s.vd, sum.payload = s.payload;
+                    sum.load_factor = s.load_factor, sum.blur_pairs = s.blur_pairs;
+                    sum.blur_grid = s.blur_grid;
+                    sum.nbr_half = s.nbr_half;
+                    sum.vertex_rows = s.vertex_rows;
+                    if (s.tuned == 1 || sum.tuned != 1) sum.tuned = s.tuned;   // 1 if any chunk was a trial
+                    sum.tiled += s.tiled;
+                    sum.retries += s.retries;
+                    sum.ms_splat += s.ms_splat, sum.ms_compact += s.ms_compact;
+                    sum.ms_neighbours += s.ms_neighbours, sum.ms_blur += s.ms_blur;
+                    sum.ms_slice += s.ms_slice, sum.ms_total += s.ms_total;
+                }
             }
-            CUDA_TRY(cudaEventRecord(filtered[slot], st));
-            CUDA_TRY(cudaStreamWaitEvent(cout, filtered[slot], 0));
-            for (int i = cut[k]; i < cut[k + 1] && !r; ++i)
-                r = copy_view(dv[i], ims[i], C, cudaMemcpyDeviceToHost, cout);
-            if (r) break;
-            CUDA_TRY(cudaEventRecord(downloaded[slot], cout));
-            slot_used[slot] = true;
+            if ((r = download(k))) break;
         }
-        if (!r) set_stats(sum);
+        if (!r && !ab) set_stats(sum);
         return r;
     };
     rc = run();
+    if (ab && !rc) {
+        CUDA_TRY(cudaEventCreateWithFlags(&ab->done, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventRecord(ab->done, cout));
+        return PGPU_OK;
+    }
     // the caller's host images are in use until every copy has landed, error or not
     const cudaError_t e1 = cudaStreamSynchronize(cin), e2 = cudaStreamSynchronize(cout);
     if (!rc && (e1 != cudaSuccess || e2 != cudaSuccess))
@@ -745,7 +920,112 @@ int pgpu_bilateral_batch(pgpu_image* ims, int count, const float* filter_width,
         bilateral_job(ims, 0, count, filter_width, color_sigma, opt, B);
         return run_batch(E, B, S.st);
     }
-    return bilateral_batch_host(E, S.st, ims, count, filter_width, color_sigma, opt);
+    return bilateral_batch_host(E, S.st, ims, ims, count, filter_width, color_sigma, opt, nullptr);
+}
+
+int pgpu_bilateral_batch_submit(const pgpu_image* in, pgpu_image* out, int count,
+                                const float* filter_width, const float* color_sigma,
+                                const pgpu_options* opt_in, long long* ticket) {
+    const pgpu_options opt = opts_or_default(opt_in);
+    if (!ticket || count < 1 || !in || !filter_width || !color_sigma)
+        return fail(PGPU_ERR_ARGUMENT, "invalid batch arguments");
+    if (opt.memory != PGPU_MEM_HOST) return fail(PGPU_ERR_ARGUMENT, "queued batches take host-memory images");
+    if (opt.device < 0 || opt.device > 255) return fail(PGPU_ERR_ARGUMENT, "device %d", opt.device);
+    *ticket = 0;
+    const pgpu_image* outs = out ? out : in;
+    const int C = in[0].channels;
+    if (C + 1 > 8) return fail(PGPU_ERR_UNSUPPORTED, "%d image channels (supported: 1..7)", C);
+    for (int i = 0; i < count; ++i) {
+        const pgpu_image& v = in[i];
+        const pgpu_image& o = outs[i];
+        const float fw = filter_width[i];
+        if (!view_ok(&v) || v.channels != C || v.frames != 1)
+            return fail(PGPU_ERR_ARGUMENT, "batch image %d: single-frame images with %d channels expected", i, C);
+        if (!view_ok(&o) || o.width != v.width || o.height != v.height || o.frames != 1 || o.channels != C)
+            return fail(PGPU_ERR_ARGUMENT, "batch image %d: the output view differs in size from the input", i);
+        if (v.width < 2 || v.height < 2 || !(fw > 0) || !(fw < 10 * v.width) || !(fw < 10 * v.height) ||
+            !(color_sigma[i] > 0))
+            return fail(PGPU_ERR_UNSUPPORTED,
+                        "batch image %d: needs width, height > 1 and 0 < filter width < 10 x its "
+                        "width and height (filter it with pgpu_bilateral)", i);
+    }
+    ApiScope S(&opt, true);
+    if (S.rc) return S.rc;
+    Engine& E = *S.E;
+    const long long id = (++E.async_seq << 8) | opt.device;
+    // a shape the autotuner is still timing runs now, as pgpu_bilateral_batch would
+    bool queued = true;
+    {
+        std::vector<pgpu_image> probe(in, in + count);
+        BatchJob T;
+        // the chunks of one submission are cut by pixel count; each chunk is tuned by its
+        // own shape, so check each
+        size_t acc = 0;
+        int i0 = 0;
+        for (int i = 0; i < count && queued; ++i) {
+            acc += (size_t)in[i].width * in[i].height;
+            if ((acc >= kChunkPixels && i + 1 < count) || i + 1 == count) {
+                BatchJob P;
+                bilateral_job(probe.data(), i0, i + 1, filter_width, color_sigma, opt, P);
+                queued = tuned_settings(E, P, &T);
+                acc = 0;
+                i0 = i + 1;
+            }
+        }
+    }
+    if (!queued) {
+        drain_async(E);
+        clear_error();
+        const int rc = bilateral_batch_host(E, S.st, in, outs, count, filter_width, color_sigma, opt, nullptr);
+        if (rc) return rc;
+        E.async_done[id] = std::make_pair(PGPU_OK, std::string());
+        *ticket = id;
+        return PGPU_OK;
+    }
+    AsyncBatch* ab = new AsyncBatch();
+    ab->id = id;
+    ab->in.assign(in, in + count);
+    ab->out.assign(outs, outs + count);
+    ab->fw.assign(filter_width, filter_width + count);
+    ab->cs.assign(color_sigma, color_sigma + count);
+    ab->opt = opt;
+    const int rc = bilateral_batch_host(E, S.st, in, outs, count, filter_width, color_sigma, opt, ab);
+    if (rc) {
+        // nothing of it may still run when the caller gets its buffers back
+        cudaStreamSynchronize(E.copy_in);
+        cudaStreamSynchronize(E.stream);
+        cudaStreamSynchronize(E.copy_out);
+        for (AsyncChunk& c : ab->chunks) pinned_put(E, c.h, c.h_bytes);
+        if (ab->done) cudaEventDestroy(ab->done);
+        delete ab;
+        return rc;
+    }
+    E.async_q.push_back(ab);
+    *ticket = id;
+    return PGPU_OK;
+}
+
+int pgpu_batch_wait(long long ticket) {
+    if (ticket <= 0) return fail(PGPU_ERR_ARGUMENT, "invalid ticket");
+    pgpu_options opt;
+    pgpu_default_options(&opt);
+    opt.device = (int)(ticket & 0xFF);
+    ApiScope S(&opt, true);
+    if (S.rc) return S.rc;
+    Engine& E = *S.E;
+    for (;;) {
+        auto it = E.async_done.find(ticket);
+        if (it != E.async_done.end()) {
+            const std::pair<int, std::string> r = it->second;
+            E.async_done.erase(it);
+            if (r.first) return fail(r.first, "%s", r.second.c_str());
+            return PGPU_OK;
+        }
+        bool queued = false;
+        for (AsyncBatch* a : E.async_q) queued |= a->id == ticket;
+        if (!queued) return fail(PGPU_ERR_ARGUMENT, "unknown or already waited-for ticket");
+        complete_oldest(E);
+    }
 }
 
 int pgpu_lattice_dump(int d, int vd, int n, const float* pos, const float* val, int payload,

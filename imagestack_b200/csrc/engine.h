@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <string>
@@ -46,6 +47,8 @@ struct DevBuf {
     ~DevBuf();
 };
 
+struct AsyncBatch;   // a host-memory batch queued by pgpu_bilateral_batch_submit (engine.cu)
+
 struct Engine {
     int device = -1;
     int sms = 0;
@@ -78,15 +81,31 @@ struct Engine {
     // host-memory batches: uploads and downloads overlap the lattices on these streams
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
     cudaEvent_t pipe_ev[9] = {};   // per device slot (3): uploaded, filtered, downloaded
+    int slot_next = 0;              // device slot of the next host chunk, in turn over 3
+    bool slot_recorded[3] = {};     // the slot's download event has been recorded
+    // queued host-memory batches (oldest first), the outcomes of finished ones that no
+    // one has waited for yet (status, message), and pinned metadata buffers to reuse
+    std::deque<AsyncBatch*> async_q;
+    std::map<long long, std::pair<int, std::string>> async_done;
+    long long async_seq = 0;
+    std::vector<std::pair<unsigned char*, size_t>> pinned_free;
     // captured batch pipelines, keyed by everything a graph bakes in (sizes, buffer
     // addresses, settings, each image's points and slot range)
     std::map<std::vector<uint64_t>, cudaGraphExec_t> graphs;
-    // autotuner state per batch shape: candidate trials so far, their times, the choice
+    // autotuner state per batch shape (batch.cu): the knob and option being tried, the
+    // repeats of that trial, the best setting so far and its time
     struct Tuning {
-        int trials = 0;
-        int count = 0;   // candidates this shape tries
-        float ms[8] = {};
-        int best = 0;
+        struct Setting {
+            float load = 0.5f;
+            bool pairs = true;
+            int blur_grid = 0;
+            int splat = 0;
+            int nbr_half = 0;
+        };
+        int knob = 0, option = 0, rep = 0, trials = 0;
+        bool done = false;
+        float best_ms = 1e30f, cur_ms = 1e30f;
+        Setting best;
     };
     std::map<std::string, Tuning> tuning;
     size_t last_cap = 0;
@@ -109,6 +128,8 @@ PlanarView planar(const pgpu_image& v);
 OutView outview(const pgpu_image& v, int channels, int normalize);
 
 int get_engine(int dev, Engine** out);
+// finish every queued host batch of E (engine.cu); E.mu held
+void drain_async(Engine& E);
 int device_count_sm100();
 
 // One image of a batch.
@@ -129,7 +150,11 @@ struct BatchJob {
     bool use_graph = false;   // capture / replay the launch sequence as a CUDA graph
     bool autotune = false;    // pick load factor and blur pairing per batch shape
     bool blur_pairs = true;   // blur two axes per launch
+    int blur_grid = 0;        // 0: 16 blocks per SM striding over the vertices, 1: one vertex per
+                              // thread, 2: as 0 with two vertices per iteration (one-axis passes)
     int splat = 0;            // 0: the tile splat where vertices are shared, 1: direct only
+    bool slot_rows = false;   // keep rows in slot space with a compaction (no vertex-ordered splat)
+    int nbr_half = 0;         // with vertex-ordered rows: one neighbour lookup per axis (1) or two (0)
     std::vector<BatchItem> items;
     // parity dumps (single-item jobs)
     int* rec_vtx = nullptr;
@@ -140,6 +165,31 @@ struct BatchJob {
     std::vector<uint32_t>* vertices_out = nullptr;   // per item
 };
 int run_batch(Engine& E, const BatchJob& B, cudaStream_t st);
+
+// A pass of a batch whose launches are queued on the stream but not read back yet: the
+// pinned buffer its statuses and vertex counts land in, and what finishing it needs.
+struct PassState {
+    unsigned char* h = nullptr;
+    size_t segstat = 0, counts = 0;   // offsets in h
+    std::vector<uint64_t> cap, sig;
+    float load = 0.5f;
+    int tiled = 0, pass = 0;
+    uint64_t n_total = 0, cap_total = 0;
+    int timed = 0;   // 0: no events, 1: events around every stage, 2: around a graph
+    int nbr_half = 0;   // the neighbour search looked up one direction per axis
+    int vertex_rows = 0;   // the splat filled vertex-ordered rows (no compaction)
+};
+// Bytes of pinned metadata a batch of nseg replayed lattices stages.
+size_t batch_meta_bytes(int nseg);
+// Settings the autotuner chose for B's shape; false while its trials are not finished
+// (an untuned shape runs through run_batch, which times the trials).
+bool tuned_settings(Engine& E, const BatchJob& B, BatchJob* out);
+// Queue the first pass of B on st with its metadata staged in the pinned buffer h (at
+// least batch_meta_bytes), without waiting for it.
+int enqueue_batch(Engine& E, const BatchJob& B, cudaStream_t st, unsigned char* h, PassState* ps);
+// Once st has run the pass: statuses, learned vertex ratios, statistics.  Images whose
+// range overflowed (their output left as it was) are listed in *failed.
+int finish_batch(Engine& E, const BatchJob& B, const PassState& ps, std::vector<int>* failed);
 
 struct LatticeJob {
     int d = 0, vd = 0, payload = 0;

@@ -5,50 +5,53 @@
 namespace pgpu {
 namespace {
 
-int grid_blur(uint64_t work, int sms) {
+// blocks of 256 threads over `work` vertex slots: capped at 16 per SM (the kernels stride
+// over the vertices; modes 0 and 2), or one vertex per thread (mode 1)
+int grid_blur(uint64_t work, int sms, int mode) {
     uint64_t g = (work + 255) / 256;
-    const uint64_t cap = (uint64_t)sms * 16;
+    const uint64_t cap = mode == 1 ? 0x7FFFFFFFull : (uint64_t)sms * 16;
     if (g > cap) g = cap;
     if (g < 1) g = 1;
     return (int)g;
 }
 
 template <int VDP, typename PS, typename PD, bool HOMOG>
-void blur_t(const BlurArgs& a, bool pair, uint32_t vmax, int sms, cudaStream_t st) {
-    if (pair) blur_kernel<VDP, PS, PD, HOMOG, true><<<grid_blur(vmax, sms), 256, 0, st>>>(a);
-    else blur_kernel<VDP, PS, PD, HOMOG, false><<<grid_blur(vmax, sms), 256, 0, st>>>(a);
+void blur_t(const BlurArgs& a, bool pair, int blocks, int ilp, cudaStream_t st) {
+    if (pair) blur_kernel<VDP, PS, PD, HOMOG, true, 1><<<blocks, 256, 0, st>>>(a);
+    else if (ilp == 2) blur_kernel<VDP, PS, PD, HOMOG, false, 2><<<blocks, 256, 0, st>>>(a);
+    else blur_kernel<VDP, PS, PD, HOMOG, false, 1><<<blocks, 256, 0, st>>>(a);
 }
 
 // 16-bit payload P: rows are P between passes, FP32 when read from the compaction
 // (homogeneous lattices) or written for the slice (last pass)
 template <int VDP, typename P, bool HOMOG>
-void blur_16(const BlurArgs& a, bool src_f32, bool dst_acc, bool pair, uint32_t vmax, int sms,
-             cudaStream_t st) {
-    if (src_f32 && dst_acc) blur_t<VDP, float, float, HOMOG>(a, pair, vmax, sms, st);
-    else if (src_f32) blur_t<VDP, float, P, HOMOG>(a, pair, vmax, sms, st);
-    else if (dst_acc) blur_t<VDP, P, float, HOMOG>(a, pair, vmax, sms, st);
-    else blur_t<VDP, P, P, HOMOG>(a, pair, vmax, sms, st);
+void blur_16(const BlurArgs& a, bool src_f32, bool dst_acc, bool pair, int blocks,
+             int ilp, cudaStream_t st) {
+    if (src_f32 && dst_acc) blur_t<VDP, float, float, HOMOG>(a, pair, blocks, ilp, st);
+    else if (src_f32) blur_t<VDP, float, P, HOMOG>(a, pair, blocks, ilp, st);
+    else if (dst_acc) blur_t<VDP, P, float, HOMOG>(a, pair, blocks, ilp, st);
+    else blur_t<VDP, P, P, HOMOG>(a, pair, blocks, ilp, st);
 }
 
 template <int VDP>
 bool blur_v(const BlurArgs& a, int payload, bool homog, bool src_f32, bool dst_acc, bool pair,
-            uint32_t vmax, int sms, cudaStream_t st) {
+            int blocks, int ilp, cudaStream_t st) {
     switch (payload) {
     case kPayloadF32:
         if (homog) return false;
-        blur_t<VDP, float, float, false>(a, pair, vmax, sms, st);
+        blur_t<VDP, float, float, false>(a, pair, blocks, ilp, st);
         return true;
     case kPayloadF64:
         if (homog) return false;
-        blur_t<VDP, double, double, false>(a, pair, vmax, sms, st);
+        blur_t<VDP, double, double, false>(a, pair, blocks, ilp, st);
         return true;
     case kPayloadF16:
-        if (homog) blur_16<VDP, __half, true>(a, src_f32, dst_acc, pair, vmax, sms, st);
-        else blur_16<VDP, __half, false>(a, src_f32, dst_acc, pair, vmax, sms, st);
+        if (homog) blur_16<VDP, __half, true>(a, src_f32, dst_acc, pair, blocks, ilp, st);
+        else blur_16<VDP, __half, false>(a, src_f32, dst_acc, pair, blocks, ilp, st);
         return true;
     case kPayloadBF16:
-        if (homog) blur_16<VDP, __nv_bfloat16, true>(a, src_f32, dst_acc, pair, vmax, sms, st);
-        else blur_16<VDP, __nv_bfloat16, false>(a, src_f32, dst_acc, pair, vmax, sms, st);
+        if (homog) blur_16<VDP, __nv_bfloat16, true>(a, src_f32, dst_acc, pair, blocks, ilp, st);
+        else blur_16<VDP, __nv_bfloat16, false>(a, src_f32, dst_acc, pair, blocks, ilp, st);
         return true;
     }
     return false;
@@ -56,18 +59,19 @@ bool blur_v(const BlurArgs& a, int payload, bool homog, bool src_f32, bool dst_a
 
 }  // namespace
 
-bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, bool homog, bool src_f32,
-                 bool dst_acc, bool pair, int sms, cudaStream_t st) {
+bool launch_blur(const BlurArgs& a, int blocks, int ilp, int vdp, int payload, bool homog,
+                 bool src_f32, bool dst_acc, bool pair, cudaStream_t st) {
     switch (vdp) {
-    case 2: return blur_v<2>(a, payload, homog, src_f32, dst_acc, pair, vmax, sms, st);
-    case 4: return blur_v<4>(a, payload, homog, src_f32, dst_acc, pair, vmax, sms, st);
-    case 8: return blur_v<8>(a, payload, homog, src_f32, dst_acc, pair, vmax, sms, st);
+    case 2: return blur_v<2>(a, payload, homog, src_f32, dst_acc, pair, blocks, ilp, st);
+    case 4: return blur_v<4>(a, payload, homog, src_f32, dst_acc, pair, blocks, ilp, st);
+    case 8: return blur_v<8>(a, payload, homog, src_f32, dst_acc, pair, blocks, ilp, st);
     }
     return false;
 }
 
 int blur_all_axes(const BlurPlan& p, cudaStream_t st) {
     const int axes = p.d + 1;
+    const int blocks = grid_blur(p.vmax, p.sms, p.grid);
     const void* src = p.src;
     bool src_f32 = p.src_f32;
     int flip = 0;
@@ -83,7 +87,9 @@ int blur_all_axes(const BlurPlan& p, cudaStream_t st) {
         ba.dst = last ? p.sval : p.bufs[flip];
         ba.dst_map = last ? p.vtx2slot : nullptr;
         ba.wc = p.wc;
-        if (!launch_blur(ba, p.vmax, p.vdp, p.payload, p.homog, src_f32, last, pair, p.sms, st))
+        ba.raw = (j == 0 && p.raw) ? 1 : 0;
+        ba.products = last ? 1 : 0;
+        if (!launch_blur(ba, blocks, p.grid == 2 ? 2 : 1, p.vdp, p.payload, p.homog, src_f32, last, pair, st))
             return 1;
         src = p.bufs[flip];
         flip ^= 1;

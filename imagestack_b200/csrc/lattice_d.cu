@@ -43,9 +43,15 @@ std::atomic<uint64_t> g_tile_prepared{0};
 
 template <int VDP>
 bool prepare_tile_t() {
-    if constexpr (key_words(D) == 1)
-        return cudaFuncSetAttribute(splat_tile_kernel<D, VDP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)tile_smem_bytes(D, VDP)) == cudaSuccess;
+    if constexpr (key_words(D) == 1) {
+        if (cudaFuncSetAttribute(splat_tile_kernel<D, VDP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_smem_bytes(D, VDP)) != cudaSuccess)
+            return false;
+        if constexpr (index_in_key(D))
+            return cudaFuncSetAttribute(splat_tile_kernel<D, VDP, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tile_smem_bytes(D, VDP)) == cudaSuccess;
+    }
     return true;
 }
 
@@ -63,7 +69,14 @@ template <int VDP>
 bool splat_tile_t(const SplatArgs& a, cudaStream_t st) {
     if constexpr (key_words(D) == 1) {
         if (!a.tile_blocks) return true;
-        splat_tile_kernel<D, VDP><<<a.tile_blocks, kTileThreads, tile_smem_bytes(D, VDP), st>>>(a);
+        if (a.vrows) {   // vertex-ordered rows: d <= 6 only
+            if constexpr (index_in_key(D)) {
+                splat_tile_kernel<D, VDP, true><<<a.tile_blocks, kTileThreads, tile_smem_bytes(D, VDP), st>>>(a);
+                return true;
+            }
+            return false;
+        }
+        splat_tile_kernel<D, VDP, false><<<a.tile_blocks, kTileThreads, tile_smem_bytes(D, VDP), st>>>(a);
         return true;
     } else {
         return a.tile_blocks == 0;

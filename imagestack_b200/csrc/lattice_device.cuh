@@ -144,10 +144,12 @@ __device__ __forceinline__ uint32_t home_slot(uint32_t h, uint32_t cap) { return
 // Insert-or-find during the splat, starting at slot `home` whose word 0 the caller has
 // already loaded into `first` (so the loads of several keys can be in flight at once);
 // returns the slot or -1 (status bit set).  *inserted, when given, is set when this call
-// created the slot.
-template <int KW>
+// created the slot; *seen, when given, receives the word a found slot held.  XYZ: one-word
+// keys of d <= 6 are compared on lanes 0..5 only, because a splat that numbers vertices as
+// it creates them publishes each vertex's index in lanes 6-7 while others still insert.
+template <int KW, bool XYZ = false>
 __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home, uint4 first,
-                            unsigned* status, bool* inserted = nullptr) {
+                            unsigned* status, bool* inserted = nullptr, uint4* seen = nullptr) {
     const uint4 empty = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
     uint32_t s = home;
     for (int probe = 0; probe < kMaxProbe; ++probe) {
@@ -172,7 +174,12 @@ __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home,
             }
         }
         if (KW == 1) {
-            if (words_equal(w, k.w[0])) return (int)s;
+            const bool eq = XYZ ? (w.x == k.w[0].x && w.y == k.w[0].y && w.z == k.w[0].z)
+                                : words_equal(w, k.w[0]);
+            if (eq) {
+                if (seen) *seen = w;
+                return (int)s;
+            }
         } else if (prefix_equal(w, k.w[0])) {
             int spins = 0;
             while (word_state(w) == kStatePending) {
@@ -197,12 +204,17 @@ __device__ int table_insert(const TableView& t, const Key<KW>& k, uint32_t home,
 }
 
 // For d <= 6 a one-word key leaves lanes 6 and 7 (the state lane) free of coordinates;
-// the compaction stores the vertex's index there, so a neighbour lookup returns the index
-// with the key.  Keys are then compared on lanes 0..5 only.
+// the compaction (or the splat that numbers vertices as it creates them) stores the
+// vertex's index there, so a neighbour lookup returns the index with the key.  Keys are
+// then compared on lanes 0..5 only.  The index is stored as (v << 1) | 1: odd, so it never
+// reads as the unnumbered word's lanes 6-7 (0x00008000) nor as an empty word's.
 #ifndef PGPU_INDEX_IN_KEY_MAX_D
 #define PGPU_INDEX_IN_KEY_MAX_D 6
 #endif
 __host__ __device__ constexpr bool index_in_key(int d) { return d <= PGPU_INDEX_IN_KEY_MAX_D; }
+__device__ __forceinline__ uint32_t enc_index(uint32_t v) { return (v << 1) | 1u; }
+__device__ __forceinline__ bool has_index(uint32_t w) { return (w & 1u) != 0; }
+__device__ __forceinline__ uint32_t dec_index(uint32_t w) { return w >> 1; }
 
 template <int D>
 __device__ __forceinline__ bool key_match(const uint4& w, const uint4& k) {
@@ -240,7 +252,7 @@ __device__ __forceinline__ int table_find_index(const TableView& t, const Key<1>
     for (int probe = 0; probe < kMaxProbe; ++probe) {
         const uint4 w = __ldg(&t.key0[s]);
         if (is_empty_word(w)) return -1;
-        if (key_match<D>(w, k.w[0])) return (int)w.w;
+        if (key_match<D>(w, k.w[0])) return (int)dec_index(w.w);
         s = (s + 1 == t.cap) ? 0u : s + 1;
     }
     return -1;

@@ -141,6 +141,20 @@ struct SplatArgs {
     uint32_t* vlist;
     uint32_t* vcount;
     uint32_t* seg_counts;
+    // Vertex-ordered rows (the tile splat, d <= 6): with vrows set, the splat numbers each
+    // vertex as it creates it (the position the vertex list would give it) and
+    // accumulates every lane's row into vrows[v*VDP..] (FP32; the creator zeroes the row);
+    // the record holds vertex indices instead of slots; the creator writes the vertex's
+    // key (vkey0), its slot (vtx2slot) and, last, its index into the key word, which
+    // tells other blocks the vertex is ready.  No compaction is needed afterwards.
+    void* vrows = nullptr;
+    uint4* vkey0 = nullptr;
+    uint32_t* vtx2slot = nullptr;
+    // with vrows: the creator also marks its vertex's neighbour pairs (nbr_axes axes,
+    // nbr_stride apart) absent, for a neighbour search that looks up one direction per axis
+    int2* nbr_init = nullptr;
+    uint32_t nbr_stride = 0;
+    int nbr_axes = 0;
 };
 
 // Appends of one block to the batch's vertex list: slots go to the block's shared-memory
@@ -211,6 +225,9 @@ struct NbrArgs {
     int2* nbr;             // (d+1) x vcap pairs
     const uint8_t* tags = nullptr;   // slot tags of the compaction, or null: plain lookups
     const unsigned* seg_status = nullptr;   // the splat's per-segment status, or null
+    // one lookup per axis: vertex v finds u = n1(v) and, as n2(u) = v, writes v into u's
+    // pair too; every pair must hold (-1, -1) beforehand (the splat's creators write it)
+    int half = 0;
 };
 
 // One launch blurs along one axis (nbrA) or, fused, along two consecutive axes (nbrA then
@@ -223,6 +240,8 @@ struct BlurArgs {
     void* dst;                  // rows in vertex order, or in slot space with dst_map
     const uint32_t* dst_map;    // row index of vertex v in dst (vertex -> slot); null: v
     int wc;                     // homogeneous weight channel (homogeneous rows only)
+    int raw = 0;                // homogeneous rows read as plain sums (w*m.., w): normalise them
+    int products = 0;           // homogeneous rows written as plain products (the last pass)
 };
 
 // Slice segments are the splat's for the replay slice; for a slice at other positions
@@ -527,8 +546,8 @@ __host__ __device__ constexpr int tile_min_blocks(int d) {
 // 2.1 ms per 4K frame against 0.73 ms.)
 __host__ __device__ constexpr size_t tile_smem_bytes(int d, int vdp) {
     return (size_t)kTileSlots * 16 + (size_t)kTileSlots * 4 + (size_t)kTileSlots * 2 +
-           (size_t)kBlockListCap * 4 + (size_t)(d + 1) * kTileThreads * 4 + (size_t)(d + 1) * kTileThreads +
-           16 + 0 * (size_t)vdp;
+           (size_t)kBlockListCap * 4 + (size_t)kBlockListCap * 2 + (size_t)(d + 1) * kTileThreads * 4 +
+           (size_t)(d + 1) * kTileThreads + 16 + 0 * (size_t)vdp;
 }
 
 // Home slot of a one-word key in a block's table: a cheap multiplicative mix of the three
@@ -609,15 +628,59 @@ __device__ __forceinline__ void load_point_xyt(const PointSource& s, uint32_t x,
         ++c; }
 }
 
-template <int D, int VDP>
+// Vertex v, created by this block in global slot s (batch numbering): its row zeroed,
+// its key and slot in vertex order, then, after a fence, its index in the key word,
+// which tells other blocks that the row is ready for their reductions.
+template <int VDP>
+__device__ __forceinline__ void publish_vertex(const SplatArgs& a, uint32_t s, uint32_t v, uint4 key) {
+    float* row = reinterpret_cast<float*>(a.vrows) + (size_t)v * VDP;
+#pragma unroll
+    for (int k = 0; k < VDP; k += 4)
+        if (k + 4 <= VDP) *reinterpret_cast<float4*>(row + k) = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = VDP - VDP % 4; k < VDP; ++k) row[k] = 0.f;
+    key.w = 0x00008000u;   // lane 6 = coordinate 0 (none for d <= 6), lane 7 = ready state
+    a.vkey0[v] = key;
+    a.vtx2slot[v] = s;
+    if (a.nbr_init)
+        for (int j = 0; j < a.nbr_axes; ++j) a.nbr_init[(size_t)j * a.nbr_stride + v] = make_int2(-1, -1);
+    __threadfence();
+    atomicExch(reinterpret_cast<unsigned*>(a.key0 + s) + 3, enc_index(v));
+}
+
+// the vertex index of global slot s, created by another block: wait (bounded) until its
+// creator has published it, which takes the creator's global inserts and one atomic
+// (microseconds); 0xFFFFFFFF with the spin-limit status bit if it is not published within
+// kAwaitSpin polls, or at once when another wait of the lattice has given up already
+constexpr int kAwaitSpin = 1 << 14;
+__device__ __forceinline__ uint32_t await_vertex(const SplatArgs& a, uint32_t s, unsigned* status) {
+    const unsigned* w = reinterpret_cast<const unsigned*>(a.key0 + s) + 3;
+    for (int spin = 0; spin < kAwaitSpin; ++spin) {
+        const unsigned x = __ldcg(w);
+        if (has_index(x)) {
+            __threadfence();
+            return dec_index(x);
+        }
+        if ((spin & 63) == 63 && (__ldcg(status) & kStatusSpinLimit)) return 0xFFFFFFFFu;
+        __nanosleep(64);
+    }
+    atomicOr(status, kStatusSpinLimit);
+    return 0xFFFFFFFFu;
+}
+
+// VROWS: number vertices as they are created and accumulate into vertex-ordered rows (the
+// SplatArgs::vrows protocol, d <= 6, no first touches); otherwise rows in slot space.
+template <int D, int VDP, bool VROWS>
 __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_kernel(SplatArgs a) {
     static_assert(key_words(D) == 1, "the tile splat handles one-word keys (d <= 7)");
+    static_assert(!VROWS || index_in_key(D), "vertex-ordered rows publish the index in the key word");
     extern __shared__ __align__(16) unsigned char tile_smem[];
     uint4* t_key = reinterpret_cast<uint4*>(tile_smem);
     uint32_t* t_ft = reinterpret_cast<uint32_t*>(t_key + kTileSlots);
     uint16_t* t_list = reinterpret_cast<uint16_t*>(t_ft + kTileSlots);
     uint32_t* s_new = reinterpret_cast<uint32_t*>(t_list + kTileSlots);
-    float* s_delta = reinterpret_cast<float*>(s_new + kBlockListCap);
+    uint16_t* s_new_l = reinterpret_cast<uint16_t*>(s_new + kBlockListCap);
+    float* s_delta = reinterpret_cast<float*>(s_new_l + kBlockListCap);
     unsigned char* s_coord = reinterpret_cast<unsigned char*>(s_delta + (D + 1) * kTileThreads);
     __shared__ Segment sg;
     __shared__ uint32_t t_count, s_new_count, s_new_base;
@@ -632,8 +695,9 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
 
     unsigned* status = a.seg_status + kseg;
     const TableView table{a.key0 + sg.slot_base, a.keyn + sg.slot_base, sg.cap, a.cap_total};
-    float* vals = reinterpret_cast<float*>(a.vals) + (size_t)sg.slot_base * VDP;
-    uint32_t* ft = a.ft ? a.ft + sg.slot_base : nullptr;
+    float* vals = VROWS ? reinterpret_cast<float*>(a.vrows)
+                        : reinterpret_cast<float*>(a.vals) + (size_t)sg.slot_base * VDP;
+    uint32_t* ft = (!VROWS && a.ft) ? a.ft + sg.slot_base : nullptr;
     const uint32_t b = blockIdx.x - sg.tile_base;
     const uint32_t per_frame = sg.tiles_x * sg.tiles_y;
     const uint32_t f = b / per_frame, bt = b - f * per_frame;
@@ -646,10 +710,12 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
 
     // Phase A: this pixel's simplex and the local slot of each of its d+1 vertices.
     // loc[r] >= 0: local slot; -1: not placed; <= -2: global slot -(loc + 2), taken directly
-    // because the local table was full around the key.
+    // because the local table was full around the key (VROWS: with bit r of `direct_v` set,
+    // -(loc + 2) is already the vertex index).
     float v[VDP];
     float bary[D + 1];
     int loc[D + 1];
+    uint32_t direct_v = 0;
     uint32_t gi = 0;
 #pragma unroll
     for (int r = 0; r <= D; ++r) loc[r] = -1;
@@ -673,11 +739,23 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
             } else {
                 const uint32_t home = home_slot(key_hash<1>(key), table.cap);
                 bool created = false;
-                const int s = table_insert<1>(table, key, home, __ldcg(&table.key0[home]), status, &created);
+                const int s = table_insert<1, VROWS>(table, key, home, __ldcg(&table.key0[home]), status, &created);
                 if (s >= 0) {
-                    if (ft) atomicMin(&ft[s], e0 + (uint32_t)r);
-                    if (created && a.vlist) block_list_append(blist, a, kseg, sg.slot_base + (uint32_t)s);
-                    loc[r] = -(s + 2);
+                    if constexpr (VROWS) {
+                        if (created) {   // numbered and published at once
+                            const uint32_t vv = atomicAdd(a.vcount, 1u);
+                            atomicAdd(a.seg_counts + kseg, 1u);
+                            publish_vertex<VDP>(a, sg.slot_base + (uint32_t)s, vv, key.w[0]);
+                            direct_v |= 1u << r;
+                            loc[r] = -(int)(vv + 2);
+                        } else {
+                            loc[r] = -(s + 2);
+                        }
+                    } else {
+                        if (ft) atomicMin(&ft[s], e0 + (uint32_t)r);
+                        if (created && a.vlist) block_list_append(blist, a, kseg, sg.slot_base + (uint32_t)s);
+                        loc[r] = -(s + 2);
+                    }
                 }
             }
         }
@@ -694,20 +772,81 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
         kk.w[0] = t_key[l];
         const uint32_t h = home_slot(key_hash<1>(kk), table.cap);
         bool created = false;
-        const int s = table_insert<1>(table, kk, h, __ldcg(&table.key0[h]), status, &created);
-        if (s >= 0 && ft) atomicMin(&ft[s], t_ft[l]);
-        if (created && a.vlist) block_list_append(blist, a, kseg, sg.slot_base + (uint32_t)s);
-        t_ft[l] = s >= 0 ? (uint32_t)s : 0xFFFFFFFFu;   // now the global slot (segment-relative)
+        uint4 seen = make_uint4(0u, 0u, 0u, 0u);
+        const int s = table_insert<1, VROWS>(table, kk, h, __ldcg(&table.key0[h]), status, &created, &seen);
+        if constexpr (VROWS) {
+            // t_ft[l]: the vertex index, or 0x80000000 | global slot while it is not known
+            uint32_t val = 0xFFFFFFFFu;
+            if (s >= 0) {
+                const uint32_t gs = sg.slot_base + (uint32_t)s;
+                val = 0x80000000u | gs;
+                if (created) {
+                    const uint32_t jj = atomicAdd(&s_new_count, 1u);
+                    if (jj < kBlockListCap) {
+                        s_new[jj] = gs;
+                        s_new_l[jj] = (uint16_t)l;
+                    } else {   // the block's list is full: numbered and published at once
+                        const uint32_t vv = atomicAdd(a.vcount, 1u);
+                        atomicAdd(a.seg_counts + kseg, 1u);
+                        publish_vertex<VDP>(a, gs, vv, kk.w[0]);
+                        val = vv;
+                    }
+                } else if (has_index(seen.w)) {
+                    val = dec_index(seen.w);
+                }
+            }
+            t_ft[l] = val;
+        } else {
+            if (s >= 0 && ft) atomicMin(&ft[s], t_ft[l]);
+            if (created && a.vlist) block_list_append(blist, a, kseg, sg.slot_base + (uint32_t)s);
+            t_ft[l] = s >= 0 ? (uint32_t)s : 0xFFFFFFFFu;   // now the global slot (segment-relative)
+        }
     }
     __syncthreads();
-    if (a.vlist) block_list_flush(blist, a, kseg);
+    if constexpr (VROWS) {
+        // number the block's new vertices with one atomic, publish them, then learn the
+        // indices of the vertices other blocks created
+        const uint32_t n = min(s_new_count, kBlockListCap);
+        if (n) {
+            if (threadIdx.x == 0) {
+                s_new_base = atomicAdd(a.vcount, n);
+                atomicAdd(a.seg_counts + kseg, n);
+            }
+            __syncthreads();
+            const uint32_t base = s_new_base;
+            for (uint32_t jj = threadIdx.x; jj < n; jj += kTileThreads) {
+                const int l = s_new_l[jj];
+                publish_vertex<VDP>(a, s_new[jj], base + jj, t_key[l]);
+                t_ft[l] = base + jj;
+            }
+            __syncthreads();
+        }
+#pragma unroll 1
+        for (uint32_t j = threadIdx.x; j < count; j += kTileThreads) {
+            const int l = t_list[j];
+            const uint32_t val = t_ft[l];
+            if (val != 0xFFFFFFFFu && (val & 0x80000000u)) t_ft[l] = await_vertex(a, val & 0x7FFFFFFFu, status);
+        }
+        __syncthreads();
+    } else {
+        if (a.vlist) block_list_flush(blist, a, kseg);
+    }
 
     // Phase C: every lane's rows into its vertices' global rows, and the replay record
     if (!valid) return;
 #pragma unroll
     for (int r = 0; r <= D; ++r) {
         const int l = loc[r];
-        const uint32_t s = l >= 0 ? t_ft[l] : l <= -2 ? (uint32_t)(-(l + 2)) : 0xFFFFFFFFu;
+        uint32_t s;
+        if (l >= 0) {
+            s = t_ft[l];
+        } else if (l <= -2) {
+            s = (uint32_t)(-(l + 2));
+            if constexpr (VROWS)
+                if (!(direct_v & (1u << r))) s = await_vertex(a, sg.slot_base + s, status);
+        } else {
+            s = 0xFFFFFFFFu;
+        }
         if (s != 0xFFFFFFFFu) {
             float c[VDP];
 #pragma unroll
@@ -715,7 +854,8 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
             atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
         }
         if (a.rec_slot)
-            a.rec_slot[(size_t)r * a.n_total + gi] = s != 0xFFFFFFFFu ? sg.slot_base + s : 0xFFFFFFFFu;
+            a.rec_slot[(size_t)r * a.n_total + gi] =
+                s == 0xFFFFFFFFu ? 0xFFFFFFFFu : VROWS ? s : sg.slot_base + s;
         if (a.rec_w) a.rec_w[(size_t)r * a.n_total + gi] = bary[r];
     }
 }
@@ -756,7 +896,7 @@ __device__ __forceinline__ void assign_vertex(const CompactArgs& a, uint32_t s, 
     a.vtx2slot[vtx] = s;
     const uint4 k0 = a.table.key0[s];
     a.vkey0[vtx] = k0;
-    if (KW == 1 && a.index_in_key) a.table.key0[s] = make_uint4(k0.x, k0.y, k0.z, vtx);
+    if (KW == 1 && a.index_in_key) a.table.key0[s] = make_uint4(k0.x, k0.y, k0.z, enc_index(vtx));
 #pragma unroll
     for (int k = 1; k < KW; ++k)
         a.vkeyn[(size_t)(k - 1) * a.vcap + vtx] = a.table.keyn[(size_t)(k - 1) * a.table.stride + s];
@@ -867,7 +1007,8 @@ __global__ void neighbours_kernel(NbrArgs a) {
         // a lattice whose splat overflowed is rerun by the host: its full table would make
         // every lookup of an absent key probe to the limit, so skip it
         if (a.seg_status && (__ldcg(a.seg_status + kseg) & (kStatusProbeLimit | kStatusSpinLimit))) {
-            for (int j = 0; j <= D; ++j) a.nbr[(size_t)j * a.vcap + vtx] = make_int2(-1, -1);
+            if (!a.half)
+                for (int j = 0; j <= D; ++j) a.nbr[(size_t)j * a.vcap + vtx] = make_int2(-1, -1);
             continue;
         }
         const uint32_t base = __ldg(a.seg_slot_base + kseg);
@@ -877,6 +1018,21 @@ __global__ void neighbours_kernel(NbrArgs a) {
         key.w[0] = a.vkey0[vtx];
 #pragma unroll
         for (int k = 1; k < KW; ++k) key.w[k] = a.vkeyn[(size_t)(k - 1) * a.vcap + vtx];
+        if constexpr (KW == 1) {
+            if (a.half) {
+                // n1 only: the key one step up along axis j; its vertex u has n2(u) = vtx
+#pragma unroll
+                for (int j = 0; j <= D; ++j) {
+                    Key<KW> k1;
+                    neighbour_key<D>(key, j, +1, k1);
+                    const int u1 = neighbour_index<D>(a, table, base, k1);
+                    int* pair = reinterpret_cast<int*>(a.nbr + (size_t)j * a.vcap);
+                    pair[2 * (size_t)vtx] = u1;
+                    if (u1 >= 0) pair[2 * (size_t)u1 + 1] = (int)vtx;
+                }
+                continue;
+            }
+        }
         // one-word keys: the axes unrolled, so each axis's packed step is a constant;
         // multi-word keys: rolled (d=16, 2M points: 46.7 ms unrolled, 20.5 ms rolled)
 #pragma unroll (KW == 1 ? D + 1 : 1)
@@ -985,9 +1141,28 @@ __device__ __forceinline__ void combine3(const A (&r1)[VDP], const A (&r0)[VDP],
     }
 }
 
+// A homogeneous row read as plain sums (w*m_0.., w), as the splat leaves them, in the
+// normalised form (m_0.., w) the homogeneous blur works on: m = sum / w (0 where w is 0).
+template <int VDP, typename A>
+__device__ __forceinline__ void normalise_sums(A (&r)[VDP], int wc) {
+    A w = r[0];
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) if (k == wc) w = r[k];
+#pragma unroll
+    for (int k = 0; k < VDP; ++k) r[k] = (k == wc) ? w : (k < wc && w != (A)0) ? r[k] / w : (A)0;
+}
+
+// row of vertex u for the homogeneous blur (raw: normalised from plain sums)
+template <int VDP, typename PS, typename A, bool HOMOG>
+__device__ __forceinline__ void load_blur_row(const PS* src, int u, bool raw, int wc, A (&r)[VDP]) {
+    load_row<VDP, PS, A>(src, u, r);
+    if constexpr (HOMOG)
+        if (raw) normalise_sums<VDP, A>(r, wc);
+}
+
 // the first-axis blur at vertex u (zeros when u is absent)
 template <int VDP, typename PS, typename A, bool HOMOG>
-__device__ __forceinline__ void blurred_row(const PS* src, const int2* nbr, int u, int wc,
+__device__ __forceinline__ void blurred_row(const PS* src, const int2* nbr, int u, int wc, bool raw,
                                             A (&out)[VDP]) {
     if (u < 0) {
 #pragma unroll
@@ -996,9 +1171,9 @@ __device__ __forceinline__ void blurred_row(const PS* src, const int2* nbr, int 
     }
     const int2 nb = __ldg(nbr + u);
     A r1[VDP], r0[VDP], r2[VDP];
-    load_row<VDP, PS, A>(src, nb.x, r1);
-    load_row<VDP, PS, A>(src, u, r0);
-    load_row<VDP, PS, A>(src, nb.y, r2);
+    load_blur_row<VDP, PS, A, HOMOG>(src, nb.x, raw, wc, r1);
+    load_blur_row<VDP, PS, A, HOMOG>(src, u, raw, wc, r0);
+    load_blur_row<VDP, PS, A, HOMOG>(src, nb.y, raw, wc, r2);
     combine3<VDP, A, HOMOG>(r1, r0, r2, wc, out);
 }
 
@@ -1007,38 +1182,66 @@ __device__ __forceinline__ void blurred_row(const PS* src, const int2* nbr, int 
 // lattice (FP32 rows in slot space for the slice).  A fused pair computes the first
 // axis's rows in registers with the same arithmetic a separate pass would store, so in
 // FP32 it is bit-identical to two passes.
-template <int VDP, typename PS, typename PD, bool HOMOG, bool PAIR>
+// the last pass writes the slice's rows; homogeneous rows (m_0.., w) go back to plain
+// products (w*m_0.., w), so the slice is the same kernel for every payload
+template <int VDP, typename PD, typename A, bool HOMOG>
+__device__ __forceinline__ void put_row(const BlurArgs& a, PD* dst, uint32_t vtx, A (&out)[VDP]) {
+    if constexpr (HOMOG) {
+        if (a.products) {
+            A w = out[0];
+#pragma unroll
+            for (int k = 0; k < VDP; ++k) if (k == a.wc) w = out[k];
+#pragma unroll
+            for (int k = 0; k < VDP; ++k) if (k < a.wc) out[k] = out[k] * w;
+        }
+    }
+    const size_t row = a.dst_map ? (size_t)__ldg(a.dst_map + vtx) : (size_t)vtx;
+    store_row<VDP, PD, A>(dst, row, out);
+}
+
+// ILP: vertices per thread and iteration (one-axis passes): ILP = 2 issues both vertices'
+// neighbour and row loads before either is combined, for twice the loads in flight.
+template <int VDP, typename PS, typename PD, bool HOMOG, bool PAIR, int ILP>
 __global__ void blur_kernel(BlurArgs a) {
+    static_assert(ILP == 1 || (ILP == 2 && !PAIR), "two vertices per iteration in one-axis passes");
     using A = typename AccOf<PD>::T;
     const PS* src = reinterpret_cast<const PS*>(a.src);
     PD* dst = reinterpret_cast<PD*>(a.dst);
     const uint32_t m = *a.nverts;
-    for (uint32_t vtx = blockIdx.x * blockDim.x + threadIdx.x; vtx < m;
-         vtx += gridDim.x * blockDim.x) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t vtx = blockIdx.x * blockDim.x + threadIdx.x; vtx < m; vtx += stride * ILP) {
         A out[VDP];
         if constexpr (PAIR) {
             const int2 nb = __ldg(a.nbrB + vtx);
             A r1[VDP], r0[VDP], r2[VDP];
-            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.x, a.wc, r1);
-            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, r0);
-            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.y, a.wc, r2);
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.x, a.wc, a.raw, r1);
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, a.raw, r0);
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.y, a.wc, a.raw, r2);
             combine3<VDP, A, HOMOG>(r1, r0, r2, a.wc, out);
-        } else {
-            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, out);
-        }
-        // The last pass writes the slice's rows; homogeneous rows (m_0.., w) go back to
-        // plain products (w*m_0.., w), so the slice is the same kernel for every payload.
-        if constexpr (HOMOG) {
-            if (a.dst_map) {
-                A w = out[0];
-#pragma unroll
-                for (int k = 0; k < VDP; ++k) if (k == a.wc) w = out[k];
-#pragma unroll
-                for (int k = 0; k < VDP; ++k) if (k < a.wc) out[k] = out[k] * w;
+            put_row<VDP, PD, A, HOMOG>(a, dst, vtx, out);
+        } else if constexpr (ILP == 2) {
+            const uint32_t v2 = vtx + stride;
+            const bool two = v2 < m;
+            const int2 na = __ldg(a.nbrA + vtx);
+            const int2 nb = two ? __ldg(a.nbrA + v2) : make_int2(-1, -1);
+            A p1[VDP], p0[VDP], p2[VDP], q1[VDP], q0[VDP], q2[VDP];
+            load_blur_row<VDP, PS, A, HOMOG>(src, na.x, a.raw, a.wc, p1);
+            load_blur_row<VDP, PS, A, HOMOG>(src, (int)vtx, a.raw, a.wc, p0);
+            load_blur_row<VDP, PS, A, HOMOG>(src, na.y, a.raw, a.wc, p2);
+            load_blur_row<VDP, PS, A, HOMOG>(src, nb.x, a.raw, a.wc, q1);
+            load_blur_row<VDP, PS, A, HOMOG>(src, two ? (int)v2 : -1, a.raw, a.wc, q0);
+            load_blur_row<VDP, PS, A, HOMOG>(src, nb.y, a.raw, a.wc, q2);
+            combine3<VDP, A, HOMOG>(p1, p0, p2, a.wc, out);
+            put_row<VDP, PD, A, HOMOG>(a, dst, vtx, out);
+            if (two) {
+                A out2[VDP];
+                combine3<VDP, A, HOMOG>(q1, q0, q2, a.wc, out2);
+                put_row<VDP, PD, A, HOMOG>(a, dst, v2, out2);
             }
+        } else {
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, a.raw, out);
+            put_row<VDP, PD, A, HOMOG>(a, dst, vtx, out);
         }
-        const size_t row = a.dst_map ? (size_t)__ldg(a.dst_map + vtx) : (size_t)vtx;
-        store_row<VDP, PD, A>(dst, row, out);
     }
 }
 

@@ -56,8 +56,8 @@ bool launch_assign(const CompactArgs& a, int kw, int vdp, int payload, bool homo
 // src_f32: the pass reads FP32 rows (first pass of a homogeneous 16-bit lattice);
 // dst_acc: it writes rows of the arithmetic type (the last pass, for the slice);
 // pair: it blurs along two consecutive axes
-bool launch_blur(const BlurArgs& a, uint32_t vmax, int vdp, int payload, bool homog, bool src_f32,
-                 bool dst_acc, bool pair, int sms, cudaStream_t st);
+bool launch_blur(const BlurArgs& a, int blocks, int ilp, int vdp, int payload, bool homog,
+                 bool src_f32, bool dst_acc, bool pair, cudaStream_t st);
 
 // All d+1 blur axes in fused pairs; intermediate rows ping-pong between bufs[0] and
 // bufs[1] (payload type); the last pass writes the arithmetic type into slot space
@@ -74,7 +74,10 @@ struct BlurPlan {
     void* sval;
     const uint32_t* vtx2slot;
     int wc, sms;
+    bool raw = false;      // homogeneous source rows are the splat's plain sums (no compaction)
     bool pairs = true;     // fuse consecutive axes into one launch
+    int grid = 0;          // 0: 16 blocks per SM striding over the vertices, 1: one vertex per
+                           // thread, 2: as 0 with two vertices per iteration (one-axis passes)
 };
 int blur_all_axes(const BlurPlan& p, cudaStream_t st);   // 0 on success
 

@@ -4,7 +4,8 @@
  * transform operations.  Every function takes plain pointers and sizes, returns a
  * status code (PGPU_OK == 0) and records a message for pgpu_last_error() on failure;
  * no C++ or CUDA type crosses this boundary.  Calls are synchronous: when one returns,
- * its output is in the caller's memory.  There is no CPU fallback: without a usable
+ * its output is in the caller's memory (pgpu_bilateral_batch_submit alone queues its work
+ * and returns; pgpu_batch_wait finishes it).  There is no CPU fallback: without a usable
  * sm_100 device every compute call fails with PGPU_ERR_NO_DEVICE.
  *
  * Memory: image views point at HOST memory (ImageStack images, pageable or pinned) when
@@ -77,6 +78,11 @@ typedef struct pgpu_stats {
     float load_factor;     /* hash-table load factor used */
     int blur_pairs;        /* 1: blur axes fused in pairs, 0: one axis per pass */
     int tiled;             /* images splatted by the tile splat (the others: direct) */
+    int blur_grid;         /* blur launch: 0 16 blocks per SM striding over the vertices, 1 one
+                              vertex per thread, 2 as 0 with two vertices per iteration */
+    int tuned;             /* autotuner: 0 off, 1 this call was one of its trials, 2 its choice */
+    int nbr_half;          /* 1: one neighbour lookup per axis (the other pair entry scattered) */
+    int vertex_rows;       /* 1: the splat numbered vertices and filled vertex-ordered rows (no compaction) */
 } pgpu_stats;
 
 /* Fill *opt with the defaults. */
@@ -132,6 +138,25 @@ int pgpu_bilateral(pgpu_image *im, float filter_width, float filter_height,
 #define PGPU_FLAG_AUTOTUNE 2
 int pgpu_bilateral_batch(pgpu_image *ims, int count, const float *filter_width,
                          const float *color_sigma, const pgpu_options *opt);
+
+/* Queued host-memory batches (no counterpart in the reference; each result equals
+ * Bilateral::apply on the image, src/GaussTransform.cpp:730-734).  The batch of
+ * pgpu_bilateral_batch over HOST images in[0..count), each result written to out[i] (same
+ * size; out == NULL: in place), queued on the device and returned from at once: its
+ * uploads, lattices and downloads run while the caller prepares or submits the next batch,
+ * so the copies of consecutive batches overlap one another and the filtering.  Batches run
+ * in submission order.  The in and out buffers must stay valid and untouched until
+ * pgpu_batch_wait(*ticket) returns; pinned memory lets the copies run at full speed.  A
+ * batch shape the autotuner (opt->flags & PGPU_FLAG_AUTOTUNE) is still timing runs before
+ * the call returns.  Any other call on the same device first finishes the queued batches.
+ * An image whose hash range overflows is filtered again when its batch is waited for. */
+int pgpu_bilateral_batch_submit(const pgpu_image *in, pgpu_image *out, int count,
+                                const float *filter_width, const float *color_sigma,
+                                const pgpu_options *opt, long long *ticket);
+/* Wait for a queued batch: its outputs are in place and its buffers free when this returns
+ * PGPU_OK; its failure status otherwise.  Each ticket is waited for once; waiting for a
+ * later ticket finishes the earlier ones too (their status is kept for their own wait). */
+int pgpu_batch_wait(long long ticket);
 
 /* ---- Request server (no counterpart in the reference, which runs one operation at a
  * time on the CPU).  A pool of worker threads, each with its own CUDA stream and lattice

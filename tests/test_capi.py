@@ -53,6 +53,9 @@ def test_no_device_fails_loudly():
     with pytest.raises(ib.PgpuError) as e:
         ib.Bilateral.apply(img, 4.0, 4.0, 0.0, 0.1)
     assert e.value.code == ib.ERR_NO_DEVICE
+    with pytest.raises(ib.PgpuError) as e:
+        ib.bilateral_batch_submit([img], [4.0], [0.1])
+    assert e.value.code == ib.ERR_NO_DEVICE
 
 
 def test_other_methods_are_not_served_here():

@@ -328,7 +328,7 @@ def test_both_splat_kernels_bit_exact(gpu, monkeypatch, mode):
                golden("lattice_rgb_d5"))
 
 
-@pytest.mark.parametrize("mode", ["direct", "tile"])
+@pytest.mark.parametrize("mode", ["direct", "tile", "tile-slot-rows"])
 @pytest.mark.parametrize("w,h,c,ss,sr", [
     (333, 217, 3, 6.0, 0.1),    # tiles cut by both image edges
     (1000, 31, 1, 4.0, 0.2),    # fewer rows than a tile
@@ -337,8 +337,12 @@ def test_both_splat_kernels_bit_exact(gpu, monkeypatch, mode):
 ])
 def test_both_splat_kernels_match_the_oracle_on_images(gpu, monkeypatch, mode, w, h, c, ss, sr):
     """Bilateral filtering of images whose sizes do not divide into tiles, by each splat
-    kernel, against the C oracle."""
-    monkeypatch.setenv("PGPU_SPLAT", mode)
+    kernel, against the C oracle.  The tile splat numbers the vertices as it creates them
+    and accumulates into vertex-ordered rows (no compaction); "tile-slot-rows" keeps its
+    rows in slot space with the compaction instead."""
+    monkeypatch.setenv("PGPU_SPLAT", mode.split("-")[0])
+    if mode == "tile-slot-rows":
+        monkeypatch.setenv("PGPU_ROWS", "slot")
     img = synth.image(w, h, c, rects=12, seed=w + h)
     out = img.copy()
     gpu.Bilateral.apply(out, ss, ss, 0.0, sr)
