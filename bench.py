@@ -830,10 +830,14 @@ def run_ours(args):
                           "blur_grid": "one vertex per thread" if stage[-1]["blur_grid"]
                                        else "16 blocks per SM, striding",
                           "splat": "tile" if stage[-1]["tiled"] else "direct",
+                          "rows": "vertex-ordered by the splat" if stage[-1]["vertex_rows"]
+                                  else "slot space + compaction",
+                          "neighbour_lookups_per_axis": 1 if stage[-1]["nbr_half"] else 2,
                           "calls": tune_calls,
                           "knobs": "coordinate descent, each option timed twice: load factor "
                                    "0.5/0.35/0.7, blur axes in pairs or one per pass (FP32/FP64), "
-                                   "blur grid, tile or direct splat"},
+                                   "blur grid, tile or direct splat, slot-space or vertex-ordered "
+                                   "rows, one or two neighbour lookups per axis"},
             "stages_ms": stages, "vertices": M, "capacity": stage[-1]["capacity"],
             "clocks": clk.summary(),
         }

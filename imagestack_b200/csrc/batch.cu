@@ -269,13 +269,27 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     // hold their vertex index (d <= 6) and the slice replays the splat points, the splat
     // numbers the vertices as it creates them and accumulates straight into
     // vertex-ordered FP32 rows, so no compaction runs; the first blur pass reads those
-    // sums (16-bit payloads: FP32 rows, homogeneous ones normalised as they are read) and
-    // the slice reads rows by vertex index.
-    // PGPU_ROWS=slot in the environment keeps slot-space rows (the parity tests compare both).
+    // rows (16-bit payloads: FP32 rows, homogeneous ones normalised by the neighbour
+    // search, once per vertex) and the slice reads rows by vertex index.
+    // PGPU_ROWS=slot or =vertex in the environment overrides the job's choice (the parity
+    // tests compare both).
     const char* rows_mode = std::getenv("PGPU_ROWS");
+    const bool want_vrows = rows_mode && !strcmp(rows_mode, "vertex") ? true
+                          : rows_mode && !strcmp(rows_mode, "slot")   ? false
+                                                                      : !B.slot_rows;
     const bool vrows = !exact_order && B.replay && kw == 1 && index_in_key(d) && tiled_count == nseg &&
-                       B.payload != kPayloadF64 && !B.slot_rows &&
-                       !(rows_mode && !strcmp(rows_mode, "slot"));
+                       B.payload != kPayloadF64 && want_vrows;
+    // PGPU_BLUR=pairs or =single in the environment overrides the blur pairing (tests)
+    const char* blur_mode = std::getenv("PGPU_BLUR");
+    const bool blur_pairs = blur_mode && !strcmp(blur_mode, "pairs") ? true
+                          : blur_mode && !strcmp(blur_mode, "single") ? false
+                                                                       : B.blur_pairs;
+    // one neighbour lookup per axis (vertex-ordered rows only); PGPU_NBR=half or =both
+    // in the environment overrides the job's choice
+    const char* nbr_mode = std::getenv("PGPU_NBR");
+    const bool nbr_half = vrows && (nbr_mode && !strcmp(nbr_mode, "half") ? true
+                                    : nbr_mode && !strcmp(nbr_mode, "both") ? false
+                                                                            : B.nbr_half != 0);
     // 16-bit payloads accumulate in FP32 rows (vf32), which the first blur pass reads
     const bool f32_rows = vrows && (B.payload == kPayloadF16 || B.payload == kPayloadBF16);
     const MetaLayout L = layout(nseg, !B.replay);
@@ -304,7 +318,7 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             (rc = E.vkey0.ensure(cap_total * 16)) || (rc = E.vkeyn.ensure((kw - 1) * cap_total * 16)) ||
             (rc = E.vv0.ensure(cap_total * vdp * payb)) || (rc = E.vv1.ensure(cap_total * vdp * payb)) ||
             (rc = E.nbr.ensure((size_t)(d + 1) * cap_total * 8)) ||
-            ((homog || f32_rows) && (rc = E.vf32.ensure(cap_total * vdp * 4))) ||
+            ((homog || payb == 2) && (rc = E.vf32.ensure(cap_total * vdp * 4))) ||
             (rc = E.vtx2slot.ensure(cap_total * 4)) || (rc = E.sval.ensure(cap_total * vdp * accb)) ||
             (use_tags && (rc = E.tags.ensure(cap_total))) ||
             (B.replay && (rc = E.rec.ensure((size_t)entries * 4))) ||
@@ -342,6 +356,7 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             CUDA_TRY(cudaMemsetAsync(dmeta, 0, L.slotbase, st));
             CUDA_TRY(cudaMemsetAsync(E.key0.p, 0xFF, cap_total * 16, st));
             if (!vrows) CUDA_TRY(cudaMemsetAsync(E.tvals.p, 0, cap_total * vdp * accb, st));
+            else CUDA_TRY(cudaMemsetAsync((homog || f32_rows) ? E.vf32.p : E.vv0.p, 0, cap_total * vdp * 4, st));
             if (exact_order) {
                 CUDA_TRY(cudaMemsetAsync(E.ft.p, 0xFF, cap_total * 4, st));
                 CUDA_TRY(cudaMemsetAsync(E.bitmap.p, 0, (size_t)nwords * 4, st));
@@ -364,7 +379,7 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
                 sa.vrows = (homog || f32_rows) ? E.vf32.p : E.vv0.p;
                 sa.vkey0 = (uint4*)E.vkey0.p;
                 sa.vtx2slot = (uint32_t*)E.vtx2slot.p;
-                if (B.nbr_half) {
+                if (nbr_half) {
                     sa.nbr_init = (int2*)E.nbr.p;
                     sa.nbr_stride = (uint32_t)cap_total;
                     sa.nbr_axes = d + 1;
@@ -436,7 +451,12 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             na.nbr = (int2*)E.nbr.p;
             na.tags = use_tags ? (const uint8_t*)E.tags.p : nullptr;
             na.seg_status = (const unsigned*)(dmeta + L.segstat);
-            na.half = (vrows && B.nbr_half) ? 1 : 0;
+            na.half = (vrows && nbr_half) ? 1 : 0;
+            if (vrows && homog) {   // the splat's sums, normalised once per vertex here
+                na.norm_rows = (float*)E.vf32.p;
+                na.vdp = vdp;
+                na.wc = vd - 1;
+            }
             ops->neighbours(na, (uint32_t)cap_total, E.sms, st);
             CUDA_TRY(cudaGetLastError());
             if (timed) CUDA_TRY(cudaEventRecord(E.ev[3], st));
@@ -447,7 +467,6 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             bp.payload = B.payload;
             bp.homog = homog;
             bp.src_f32 = homog || f32_rows;
-            bp.raw = vrows && homog;
             bp.nbr = (const int2*)E.nbr.p;
             bp.nbr_stride = cap_total;
             bp.nverts = dM;
@@ -459,7 +478,8 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             bp.vtx2slot = vrows ? nullptr : (const uint32_t*)E.vtx2slot.p;   // null: vertex order
             bp.wc = vd - 1;
             bp.sms = E.sms;
-            bp.pairs = B.blur_pairs;
+            bp.pairs = blur_pairs;
+            if (payb == 2) bp.f32buf = E.vf32.p;
             bp.grid = B.blur_grid;
             if (blur_all_axes(bp, st)) return fail(PGPU_ERR_UNSUPPORTED, "blur variant");
             CUDA_TRY(cudaGetLastError());
@@ -493,14 +513,14 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             // the graph bakes in sizes, settings and buffer addresses, so all of them key it
             std::vector<uint64_t> gk = {
                 (uint64_t)d, (uint64_t)vd, (uint64_t)B.payload, (uint64_t)homog, (uint64_t)B.replay,
-                (uint64_t)nseg, n_total, ns_total, cap_total, nwords, (uint64_t)B.blur_pairs,
+                (uint64_t)nseg, n_total, ns_total, cap_total, nwords, (uint64_t)blur_pairs,
                 (uint64_t)B.blur_grid, blocks,
                 tile_blocks, slice_blocks, (uint64_t)(uintptr_t)E.key0.p, (uint64_t)(uintptr_t)E.keyn.p,
                 (uint64_t)(uintptr_t)E.tvals.p, (uint64_t)(uintptr_t)E.nbr.p, (uint64_t)(uintptr_t)E.rec.p,
                 (uint64_t)(uintptr_t)E.recw.p, (uint64_t)(uintptr_t)E.meta.p, (uint64_t)(uintptr_t)h,
                 (uint64_t)(uintptr_t)E.sval.p, (uint64_t)(uintptr_t)E.vlist.p, (uint64_t)(uintptr_t)E.vv0.p,
                 (uint64_t)(uintptr_t)E.vv1.p, (uint64_t)(uintptr_t)E.vkey0.p, (uint64_t)(uintptr_t)E.vf32.p,
-                (uint64_t)vrows, (uint64_t)(uintptr_t)E.vtx2slot.p, (uint64_t)B.nbr_half};
+                (uint64_t)vrows, (uint64_t)(uintptr_t)E.vtx2slot.p, (uint64_t)nbr_half};
             gk.reserve(gk.size() + 2 * (size_t)nseg);
             for (int k = 0; k < nseg; ++k) {
                 gk.push_back(cap[k]);
@@ -541,8 +561,9 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         ps->n_total = n_total;
         ps->cap_total = cap_total;
         ps->timed = timed ? (graph ? 2 : 1) : 0;
-        ps->nbr_half = (vrows && B.nbr_half) ? 1 : 0;
+        ps->nbr_half = (vrows && nbr_half) ? 1 : 0;
         ps->vertex_rows = vrows ? 1 : 0;
+        ps->blur_pairs = blur_pairs ? 1 : 0;
         return PGPU_OK;
     }
 }
@@ -605,7 +626,7 @@ static int finish_pass(Engine& E, const BatchJob& B, const PassState& ps, std::v
     s.payload = B.payload;
     s.retries = ps.pass;
     s.load_factor = ps.load;
-    s.blur_pairs = B.blur_pairs ? 1 : 0;
+    s.blur_pairs = ps.blur_pairs;
     s.blur_grid = B.blur_grid;
     s.nbr_half = ps.nbr_half;
     s.vertex_rows = ps.vertex_rows;
@@ -640,18 +661,21 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
 // best setting found so far for the other knobs, each twice (the faster time counts: the
 // first call of a shape also learns its vertex ratio), by the lattice's device time:
 //   0. hash-table load factor 0.5 / 0.35 / 0.7;
-//   1. blur passes: axes fused in pairs, or one axis per pass (FP32/FP64 payloads only:
-//      one axis per pass would round 16-bit rows between axes, which a pair keeps in FP32
-//      registers, so 16-bit results would depend on the choice);
+//   1. blur passes: axes fused in pairs, or one axis per pass (16-bit payloads: rows kept
+//      in FP32 after every first axis of a would-be pair and rounded to 16 bits after the
+//      second, as a pair rounds them, so the results are the same bit for bit);
 //   2. blur grid: 16 blocks per SM striding over the vertices, one vertex per thread, or
 //      (one-axis passes) 16 blocks per SM with two vertices per iteration;
 //   3. splat: the tile splat wherever the learned vertex density allows it, or the direct
 //      splat for every image;
-//   4. neighbour search (vertex-ordered rows only): two lookups per axis, or one (n1) with
+//   4. rows: in slot space with a compaction into vertex order, or numbered by the tile
+//      splat as it creates the vertices, in vertex order from the start (where every image
+//      of the batch takes the tile splat);
+//   5. neighbour search (vertex-ordered rows only): two lookups per axis, or one (n1) with
 //      the other pair entry written by the neighbour found (n2(n1(v)) = v).
 // Keys, vertex order and FP32/FP64 results do not depend on the choice.
 constexpr float kTuneLoads[] = {0.5f, 0.35f, 0.7f};
-constexpr int kTuneKnobs = 5;
+constexpr int kTuneKnobs = 6;
 constexpr int kTuneReps = 2;
 
 static int knob_options(int k) { return k == 0 || k == 2 ? 3 : 2; }
@@ -662,14 +686,15 @@ static Engine::Tuning::Setting with_option(Engine::Tuning::Setting s, int k, int
     case 1: s.pairs = o == 0; break;
     case 2: s.blur_grid = o; break;
     case 3: s.splat = o; break;
-    case 4: s.nbr_half = o; break;
+    case 4: s.vertex_rows = o; break;
+    case 5: s.nbr_half = o; break;
     }
     return s;
 }
 
 static bool same_setting(const Engine::Tuning::Setting& a, const Engine::Tuning::Setting& b) {
     return a.load == b.load && a.pairs == b.pairs && a.blur_grid == b.blur_grid && a.splat == b.splat &&
-           a.nbr_half == b.nbr_half;
+           a.vertex_rows == b.vertex_rows && a.nbr_half == b.nbr_half;
 }
 
 // the next setting to try (skipping options that are the best setting itself, already
@@ -683,8 +708,10 @@ static bool tune_next(Engine::Tuning& t, bool singles_ok, Engine::Tuning::Settin
         }
         const Engine::Tuning::Setting c = with_option(t.best, t.knob, t.option);
         const bool timed_already = t.best_ms < 1e29f && same_setting(c, t.best);
-        // two vertices per blur iteration exist for one-axis passes only
-        if (timed_already || (!singles_ok && !c.pairs) || (c.pairs && c.blur_grid == 2)) {
+        // two vertices per blur iteration exist for one-axis passes only; the one-lookup
+        // neighbour search for vertex-ordered rows only
+        if (timed_already || (!singles_ok && !c.pairs) || (c.pairs && c.blur_grid == 2) ||
+            (c.nbr_half && !c.vertex_rows)) {
             ++t.option;
             continue;
         }
@@ -720,14 +747,17 @@ static std::string tune_key(const BatchJob& B) {
 }
 
 static bool tunable(const BatchJob& B) { return B.autotune && !B.rec_vtx && !B.dump_splat; }
+// 16-bit payloads blur one axis per pass with the pairs' rounding (bit-identical) from
+// d = 2 up (three or more axes)
 static bool singles_allowed(const BatchJob& B) {
-    return B.payload != kPayloadF16 && B.payload != kPayloadBF16;
+    return (B.payload != kPayloadF16 && B.payload != kPayloadBF16) || B.d >= 2;
 }
 static void apply_setting(BatchJob& B, const Engine::Tuning::Setting& s) {
     B.load = s.load;
     B.blur_pairs = s.pairs;
     B.blur_grid = s.blur_grid;
     B.splat = s.splat;
+    B.slot_rows = !s.vertex_rows;
     B.nbr_half = s.nbr_half;
 }
 

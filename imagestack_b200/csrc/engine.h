@@ -100,6 +100,7 @@ struct Engine {
             bool pairs = true;
             int blur_grid = 0;
             int splat = 0;
+            int vertex_rows = 0;
             int nbr_half = 0;
         };
         int knob = 0, option = 0, rep = 0, trials = 0;
@@ -153,7 +154,8 @@ struct BatchJob {
     int blur_grid = 0;        // 0: 16 blocks per SM striding over the vertices, 1: one vertex per
                               // thread, 2: as 0 with two vertices per iteration (one-axis passes)
     int splat = 0;            // 0: the tile splat where vertices are shared, 1: direct only
-    bool slot_rows = false;   // keep rows in slot space with a compaction (no vertex-ordered splat)
+    bool slot_rows = true;    // rows in slot space with a compaction; false: the tile splat
+                              // numbers vertices and fills vertex-ordered rows where it can
     int nbr_half = 0;         // with vertex-ordered rows: one neighbour lookup per axis (1) or two (0)
     std::vector<BatchItem> items;
     // parity dumps (single-item jobs)
@@ -178,6 +180,7 @@ struct PassState {
     int timed = 0;   // 0: no events, 1: events around every stage, 2: around a graph
     int nbr_half = 0;   // the neighbour search looked up one direction per axis
     int vertex_rows = 0;   // the splat filled vertex-ordered rows (no compaction)
+    int blur_pairs = 1;    // blur axes fused in pairs
 };
 // Bytes of pinned metadata a batch of nseg replayed lattices stages.
 size_t batch_meta_bytes(int nseg);

@@ -72,11 +72,52 @@ bool launch_blur(const BlurArgs& a, int blocks, int ilp, int vdp, int payload, b
 int blur_all_axes(const BlurPlan& p, cudaStream_t st) {
     const int axes = p.d + 1;
     const int blocks = grid_blur(p.vmax, p.sms, p.grid);
+    const bool p16 = p.payload == kPayloadF16 || p.payload == kPayloadBF16;
+    if (p16 && !p.pairs && p.f32buf && axes >= 3) {
+        // One axis per pass for 16-bit rows, rounded to 16 bits after every second axis,
+        // exactly where fused pairs round them, so the result is bit-identical to pairs:
+        // even passes write FP32 rows, odd passes 16-bit rows, the last FP32 rows for the
+        // slice.  FP32 rows alternate between f32buf and sval (never sval right before the
+        // last pass, which writes it), 16-bit rows between the two payload buffers.
+        const void* cur = p.src;
+        bool cur_f32 = p.src_f32;
+        int hflip = 0;
+        for (int j = 0; j < axes; ++j) {
+            const bool last = j + 1 == axes;
+            const bool out_f32 = last || j % 2 == 0;
+            void* dst;
+            if (last) {
+                dst = p.sval;
+            } else if (out_f32) {
+                dst = cur == p.f32buf ? p.sval : p.f32buf;
+            } else {
+                dst = p.bufs[hflip];
+                if (dst == cur) dst = p.bufs[hflip ^= 1];
+                hflip ^= 1;
+            }
+            BlurArgs ba;
+            ba.nbrA = p.nbr + (size_t)j * p.nbr_stride;
+            ba.nbrB = nullptr;
+            ba.nverts = p.nverts;
+            ba.src = cur;
+            ba.dst = dst;
+            ba.dst_map = last ? p.vtx2slot : nullptr;
+            ba.wc = p.wc;
+            ba.products = last ? 1 : 0;
+            if (!launch_blur(ba, blocks, p.grid == 2 ? 2 : 1, p.vdp, p.payload, p.homog, cur_f32, out_f32,
+                             false, st))
+                return 1;
+            cur = dst;
+            cur_f32 = out_f32;
+        }
+        return 0;
+    }
     const void* src = p.src;
     bool src_f32 = p.src_f32;
     int flip = 0;
     for (int j = 0; j < axes;) {
-        const bool pair = p.pairs && j + 1 < axes;
+        // (16-bit rows always pair here: one axis per pass would round them between axes)
+        const bool pair = (p.pairs || p16) && j + 1 < axes;
         const int step = pair ? 2 : 1;
         const bool last = j + step >= axes;
         BlurArgs ba;
@@ -87,7 +128,6 @@ int blur_all_axes(const BlurPlan& p, cudaStream_t st) {
         ba.dst = last ? p.sval : p.bufs[flip];
         ba.dst_map = last ? p.vtx2slot : nullptr;
         ba.wc = p.wc;
-        ba.raw = (j == 0 && p.raw) ? 1 : 0;
         ba.products = last ? 1 : 0;
         if (!launch_blur(ba, blocks, p.grid == 2 ? 2 : 1, p.vdp, p.payload, p.homog, src_f32, last, pair, st))
             return 1;

@@ -143,10 +143,10 @@ struct SplatArgs {
     uint32_t* seg_counts;
     // Vertex-ordered rows (the tile splat, d <= 6): with vrows set, the splat numbers each
     // vertex as it creates it (the position the vertex list would give it) and
-    // accumulates every lane's row into vrows[v*VDP..] (FP32; the creator zeroes the row);
+    // accumulates every lane's row into vrows[v*VDP..] (FP32, zeroed before the launch);
     // the record holds vertex indices instead of slots; the creator writes the vertex's
-    // key (vkey0), its slot (vtx2slot) and, last, its index into the key word, which
-    // tells other blocks the vertex is ready.  No compaction is needed afterwards.
+    // key (vkey0), its slot (vtx2slot) and its index into the key word, where other blocks
+    // read it.  No compaction is needed afterwards.
     void* vrows = nullptr;
     uint4* vkey0 = nullptr;
     uint32_t* vtx2slot = nullptr;
@@ -228,6 +228,11 @@ struct NbrArgs {
     // one lookup per axis: vertex v finds u = n1(v) and, as n2(u) = v, writes v into u's
     // pair too; every pair must hold (-1, -1) beforehand (the splat's creators write it)
     int half = 0;
+    // homogeneous FP32 rows the splat left as plain sums (w*m_0.., w), vertex-ordered:
+    // each vertex's row is normalised here in place to (m_0.., w), as the compaction
+    // would have stored it; null: nothing to do
+    float* norm_rows = nullptr;
+    int vdp = 0, wc = 0;
 };
 
 // One launch blurs along one axis (nbrA) or, fused, along two consecutive axes (nbrA then
@@ -240,7 +245,6 @@ struct BlurArgs {
     void* dst;                  // rows in vertex order, or in slot space with dst_map
     const uint32_t* dst_map;    // row index of vertex v in dst (vertex -> slot); null: v
     int wc;                     // homogeneous weight channel (homogeneous rows only)
-    int raw = 0;                // homogeneous rows read as plain sums (w*m.., w): normalise them
     int products = 0;           // homogeneous rows written as plain products (the last pass)
 };
 
@@ -628,24 +632,18 @@ __device__ __forceinline__ void load_point_xyt(const PointSource& s, uint32_t x,
         ++c; }
 }
 
-// Vertex v, created by this block in global slot s (batch numbering): its row zeroed,
-// its key and slot in vertex order, then, after a fence, its index in the key word,
-// which tells other blocks that the row is ready for their reductions.
+// Vertex v, created by this block in global slot s (batch numbering): its key and slot in
+// vertex order (read by later kernels), then its index in the key word, which tells other
+// blocks the vertex's number.  The rows were zeroed before the launch, so no fence is
+// needed between the two: nothing a reader does with v depends on the creator's stores.
 template <int VDP>
 __device__ __forceinline__ void publish_vertex(const SplatArgs& a, uint32_t s, uint32_t v, uint4 key) {
-    float* row = reinterpret_cast<float*>(a.vrows) + (size_t)v * VDP;
-#pragma unroll
-    for (int k = 0; k < VDP; k += 4)
-        if (k + 4 <= VDP) *reinterpret_cast<float4*>(row + k) = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-    for (int k = VDP - VDP % 4; k < VDP; ++k) row[k] = 0.f;
     key.w = 0x00008000u;   // lane 6 = coordinate 0 (none for d <= 6), lane 7 = ready state
     a.vkey0[v] = key;
     a.vtx2slot[v] = s;
     if (a.nbr_init)
         for (int j = 0; j < a.nbr_axes; ++j) a.nbr_init[(size_t)j * a.nbr_stride + v] = make_int2(-1, -1);
-    __threadfence();
-    atomicExch(reinterpret_cast<unsigned*>(a.key0 + s) + 3, enc_index(v));
+    __stcg(reinterpret_cast<unsigned*>(a.key0 + s) + 3, enc_index(v));
 }
 
 // the vertex index of global slot s, created by another block: wait (bounded) until its
@@ -657,10 +655,7 @@ __device__ __forceinline__ uint32_t await_vertex(const SplatArgs& a, uint32_t s,
     const unsigned* w = reinterpret_cast<const unsigned*>(a.key0 + s) + 3;
     for (int spin = 0; spin < kAwaitSpin; ++spin) {
         const unsigned x = __ldcg(w);
-        if (has_index(x)) {
-            __threadfence();
-            return dec_index(x);
-        }
+        if (has_index(x)) return dec_index(x);
         if ((spin & 63) == 63 && (__ldcg(status) & kStatusSpinLimit)) return 0xFFFFFFFFu;
         __nanosleep(64);
     }
@@ -1011,6 +1006,12 @@ __global__ void neighbours_kernel(NbrArgs a) {
                 for (int j = 0; j <= D; ++j) a.nbr[(size_t)j * a.vcap + vtx] = make_int2(-1, -1);
             continue;
         }
+        if (a.norm_rows) {   // m = sum / w, 0 where w is 0 (the compaction's arithmetic)
+            float* r = a.norm_rows + (size_t)vtx * a.vdp;
+            const float w = r[a.wc];
+            for (int k = 0; k < a.wc; ++k) r[k] = w != 0.0f ? r[k] / w : 0.0f;
+            for (int k = a.wc + 1; k < a.vdp; ++k) r[k] = 0.0f;
+        }
         const uint32_t base = __ldg(a.seg_slot_base + kseg);
         const TableView table{a.key0 + base, a.keyn + base, __ldg(a.seg_slot_base + kseg + 1) - base,
                               a.cap_total};
@@ -1141,28 +1142,9 @@ __device__ __forceinline__ void combine3(const A (&r1)[VDP], const A (&r0)[VDP],
     }
 }
 
-// A homogeneous row read as plain sums (w*m_0.., w), as the splat leaves them, in the
-// normalised form (m_0.., w) the homogeneous blur works on: m = sum / w (0 where w is 0).
-template <int VDP, typename A>
-__device__ __forceinline__ void normalise_sums(A (&r)[VDP], int wc) {
-    A w = r[0];
-#pragma unroll
-    for (int k = 0; k < VDP; ++k) if (k == wc) w = r[k];
-#pragma unroll
-    for (int k = 0; k < VDP; ++k) r[k] = (k == wc) ? w : (k < wc && w != (A)0) ? r[k] / w : (A)0;
-}
-
-// row of vertex u for the homogeneous blur (raw: normalised from plain sums)
-template <int VDP, typename PS, typename A, bool HOMOG>
-__device__ __forceinline__ void load_blur_row(const PS* src, int u, bool raw, int wc, A (&r)[VDP]) {
-    load_row<VDP, PS, A>(src, u, r);
-    if constexpr (HOMOG)
-        if (raw) normalise_sums<VDP, A>(r, wc);
-}
-
 // the first-axis blur at vertex u (zeros when u is absent)
 template <int VDP, typename PS, typename A, bool HOMOG>
-__device__ __forceinline__ void blurred_row(const PS* src, const int2* nbr, int u, int wc, bool raw,
+__device__ __forceinline__ void blurred_row(const PS* src, const int2* nbr, int u, int wc,
                                             A (&out)[VDP]) {
     if (u < 0) {
 #pragma unroll
@@ -1171,9 +1153,9 @@ __device__ __forceinline__ void blurred_row(const PS* src, const int2* nbr, int 
     }
     const int2 nb = __ldg(nbr + u);
     A r1[VDP], r0[VDP], r2[VDP];
-    load_blur_row<VDP, PS, A, HOMOG>(src, nb.x, raw, wc, r1);
-    load_blur_row<VDP, PS, A, HOMOG>(src, u, raw, wc, r0);
-    load_blur_row<VDP, PS, A, HOMOG>(src, nb.y, raw, wc, r2);
+    load_row<VDP, PS, A>(src, nb.x, r1);
+    load_row<VDP, PS, A>(src, u, r0);
+    load_row<VDP, PS, A>(src, nb.y, r2);
     combine3<VDP, A, HOMOG>(r1, r0, r2, wc, out);
 }
 
@@ -1214,9 +1196,9 @@ __global__ void blur_kernel(BlurArgs a) {
         if constexpr (PAIR) {
             const int2 nb = __ldg(a.nbrB + vtx);
             A r1[VDP], r0[VDP], r2[VDP];
-            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.x, a.wc, a.raw, r1);
-            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, a.raw, r0);
-            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.y, a.wc, a.raw, r2);
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.x, a.wc, r1);
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, r0);
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, nb.y, a.wc, r2);
             combine3<VDP, A, HOMOG>(r1, r0, r2, a.wc, out);
             put_row<VDP, PD, A, HOMOG>(a, dst, vtx, out);
         } else if constexpr (ILP == 2) {
@@ -1225,12 +1207,12 @@ __global__ void blur_kernel(BlurArgs a) {
             const int2 na = __ldg(a.nbrA + vtx);
             const int2 nb = two ? __ldg(a.nbrA + v2) : make_int2(-1, -1);
             A p1[VDP], p0[VDP], p2[VDP], q1[VDP], q0[VDP], q2[VDP];
-            load_blur_row<VDP, PS, A, HOMOG>(src, na.x, a.raw, a.wc, p1);
-            load_blur_row<VDP, PS, A, HOMOG>(src, (int)vtx, a.raw, a.wc, p0);
-            load_blur_row<VDP, PS, A, HOMOG>(src, na.y, a.raw, a.wc, p2);
-            load_blur_row<VDP, PS, A, HOMOG>(src, nb.x, a.raw, a.wc, q1);
-            load_blur_row<VDP, PS, A, HOMOG>(src, two ? (int)v2 : -1, a.raw, a.wc, q0);
-            load_blur_row<VDP, PS, A, HOMOG>(src, nb.y, a.raw, a.wc, q2);
+            load_row<VDP, PS, A>(src, na.x, p1);
+            load_row<VDP, PS, A>(src, (int)vtx, p0);
+            load_row<VDP, PS, A>(src, na.y, p2);
+            load_row<VDP, PS, A>(src, nb.x, q1);
+            load_row<VDP, PS, A>(src, two ? (int)v2 : -1, q0);
+            load_row<VDP, PS, A>(src, nb.y, q2);
             combine3<VDP, A, HOMOG>(p1, p0, p2, a.wc, out);
             put_row<VDP, PD, A, HOMOG>(a, dst, vtx, out);
             if (two) {
@@ -1239,7 +1221,7 @@ __global__ void blur_kernel(BlurArgs a) {
                 put_row<VDP, PD, A, HOMOG>(a, dst, v2, out2);
             }
         } else {
-            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, a.raw, out);
+            blurred_row<VDP, PS, A, HOMOG>(src, a.nbrA, (int)vtx, a.wc, out);
             put_row<VDP, PD, A, HOMOG>(a, dst, vtx, out);
         }
     }

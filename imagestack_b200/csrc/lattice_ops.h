@@ -71,10 +71,10 @@ struct BlurPlan {
     uint32_t vmax;
     const void* src;       // the compaction's rows in vertex order
     void* bufs[2];
+    void* f32buf = nullptr;   // FP32 rows (16-bit payloads, one axis per pass)
     void* sval;
     const uint32_t* vtx2slot;
     int wc, sms;
-    bool raw = false;      // homogeneous source rows are the splat's plain sums (no compaction)
     bool pairs = true;     // fuse consecutive axes into one launch
     int grid = 0;          // 0: 16 blocks per SM striding over the vertices, 1: one vertex per
                            // thread, 2: as 0 with two vertices per iteration (one-axis passes)

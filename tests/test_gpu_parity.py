@@ -183,8 +183,10 @@ def test_errors_are_reported(gpu):
     assert e.value.code == gpu.ERR_ARGUMENT
 
 
-def test_full_size_4k_bit_exact_vs_oracle(gpu):
-    """3840x2160 RGB, sigma_s 16, sigma_r 0.1: the whole vertex set and output."""
+def test_full_size_4k_bit_exact_vs_oracle(gpu, monkeypatch):
+    """3840x2160 RGB, sigma_s 16, sigma_r 0.1: the whole vertex set and output, the output
+    by both row layouts (slot-space rows with a compaction; vertex-ordered rows filled by
+    the splat, with either neighbour search)."""
     img = synth.image(3840, 2160, 3, rects=64, seed=2)
     pos, val = oracle.bilateral_points(img, img, 16.0, 0.1)
     ref = oracle.oracle_lattice(pos, val)
@@ -194,10 +196,15 @@ def test_full_size_4k_bit_exact_vs_oracle(gpu):
     assert sha(d["replay_vtx"]) == sha(ref.replay_vtx)
     assert sha(d["replay_w"]) == sha(ref.replay_w)
     assert rel_err(d["out"], ref.out) <= RTOL_FP32
-    out = img.copy()
-    gpu.Bilateral.apply(out, 16.0, 16.0, 0.0, 0.1)
     norm = (ref.out[:, :3] / ref.out[:, 3:4]).reshape(2160, 3840, 3).transpose(2, 0, 1)
-    assert rel_err(out, norm) <= RTOL_FP32
+    for rows, nbr in (("slot", "both"), ("vertex", "both"), ("vertex", "half")):
+        monkeypatch.setenv("PGPU_ROWS", rows)
+        monkeypatch.setenv("PGPU_NBR", nbr)
+        out = img.copy()
+        gpu.Bilateral.apply(out, 16.0, 16.0, 0.0, 0.1)
+        assert gpu.last_stats()["vertex_rows"] == (rows == "vertex")
+        assert gpu.last_stats()["nbr_half"] == (rows == "vertex" and nbr == "half")
+        assert rel_err(out, norm) <= RTOL_FP32, (rows, nbr)
 
 
 def test_fp64_payload_matches_fp64_oracle(gpu):
@@ -209,13 +216,18 @@ def test_fp64_payload_matches_fp64_oracle(gpu):
     assert rel_err(d["out"], ref.out) <= 1e-6
 
 
+@pytest.mark.parametrize("rows", ["slot", "vertex"])
 @pytest.mark.parametrize("payload,tol", [("fp16", 1e-3), ("bf16", 1e-2)])
-def test_low_precision_payload_error_vs_fp64(gpu, payload, tol):
+def test_low_precision_payload_error_vs_fp64(gpu, monkeypatch, payload, tol, rows):
+    """16-bit payloads against the FP64 lattice, with rows compacted from slot space or
+    filled in vertex order by the splat (FP32 sums the first blur pass normalises)."""
     img = synth.image(512, 512, 3, rects=16, seed=11)
     ref = img.copy()
     gpu.Bilateral.apply(ref, 8.0, 8.0, 0.0, 0.1, payload="fp64")
+    monkeypatch.setenv("PGPU_ROWS", rows)
     out = img.copy()
     gpu.Bilateral.apply(out, 8.0, 8.0, 0.0, 0.1, payload=payload)
+    assert gpu.last_stats()["vertex_rows"] == (rows == "vertex")
     err = rel_err(out, ref, floor_frac=1e-2)
     print(payload, "max relative error vs FP64 lattice:", err)
     assert err <= tol
@@ -328,7 +340,7 @@ def test_both_splat_kernels_bit_exact(gpu, monkeypatch, mode):
                golden("lattice_rgb_d5"))
 
 
-@pytest.mark.parametrize("mode", ["direct", "tile", "tile-slot-rows"])
+@pytest.mark.parametrize("mode", ["direct", "tile", "tile-vertex-rows"])
 @pytest.mark.parametrize("w,h,c,ss,sr", [
     (333, 217, 3, 6.0, 0.1),    # tiles cut by both image edges
     (1000, 31, 1, 4.0, 0.2),    # fewer rows than a tile
@@ -337,12 +349,11 @@ def test_both_splat_kernels_bit_exact(gpu, monkeypatch, mode):
 ])
 def test_both_splat_kernels_match_the_oracle_on_images(gpu, monkeypatch, mode, w, h, c, ss, sr):
     """Bilateral filtering of images whose sizes do not divide into tiles, by each splat
-    kernel, against the C oracle.  The tile splat numbers the vertices as it creates them
-    and accumulates into vertex-ordered rows (no compaction); "tile-slot-rows" keeps its
-    rows in slot space with the compaction instead."""
+    kernel, against the C oracle.  "tile-vertex-rows": the tile splat numbers the vertices
+    as it creates them and accumulates into vertex-ordered rows (no compaction); the other
+    modes keep rows in slot space with the compaction."""
     monkeypatch.setenv("PGPU_SPLAT", mode.split("-")[0])
-    if mode == "tile-slot-rows":
-        monkeypatch.setenv("PGPU_ROWS", "slot")
+    monkeypatch.setenv("PGPU_ROWS", "vertex" if mode == "tile-vertex-rows" else "slot")
     img = synth.image(w, h, c, rects=12, seed=w + h)
     out = img.copy()
     gpu.Bilateral.apply(out, ss, ss, 0.0, sr)
