@@ -656,10 +656,11 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     return finish_pass(E, B, ps, failed, cap_next);
 }
 
-// Autotuner: coordinate descent over four knobs, starting from load 0.5, blur axes in
-// pairs, the capped blur grid and the tile splat.  Each knob's options are tried with the
-// best setting found so far for the other knobs, each twice (the faster time counts: the
-// first call of a shape also learns its vertex ratio), by the lattice's device time:
+// Autotuner: coordinate descent over six knobs, starting from load 0.5, blur axes in
+// pairs, the capped blur grid, the tile splat and slot-space rows.  Each knob's options are
+// tried with the best setting found so far for the other knobs, each twice (the faster
+// time counts: the first call of a shape also learns its vertex ratio), by the device time
+// of what the knob changes (knob_time):
 //   0. hash-table load factor 0.5 / 0.35 / 0.7;
 //   1. blur passes: axes fused in pairs, or one axis per pass (16-bit payloads: rows kept
 //      in FP32 after every first axis of a would-be pair and rounded to 16 bits after the
@@ -722,15 +723,33 @@ static bool tune_next(Engine::Tuning& t, bool singles_ok, Engine::Tuning::Settin
     return false;
 }
 
-static void tune_record(Engine::Tuning& t, const Engine::Tuning::Setting& c, float ms) {
+// The time a knob is judged by: the blur's for the blur knobs, the splat's and the
+// neighbour search's for the neighbour search (its pairs are marked absent by the splat),
+// the whole lattice's for the others — a knob that changes one stage is judged without the
+// other stages' noise.  Stage times exist for calls without a graph; with a graph every
+// knob is judged by the whole lattice.
+static float knob_time(int knob, float total, const float (&stage)[3]) {
+    const bool staged = stage[0] > 0.0f && stage[0] < 1e29f;
+    if (!staged) return total;
+    if (knob == 1 || knob == 2) return stage[2];
+    if (knob == 5) return stage[0] + stage[1];
+    return total;
+}
+
+static void tune_record(Engine::Tuning& t, const Engine::Tuning::Setting& c, const pgpu_stats& s) {
     ++t.trials;
-    t.cur_ms = std::min(t.cur_ms, ms);
+    const float st[3] = {s.ms_splat, s.ms_neighbours, s.ms_blur};
+    t.cur_ms = std::min(t.cur_ms, s.ms_total);
+    for (int i = 0; i < 3; ++i) t.cur_stage[i] = std::min(t.cur_stage[i], st[i]);
     if (++t.rep < kTuneReps) return;
-    if (t.cur_ms < t.best_ms) {
+    const bool first = t.best_ms >= 1e29f;
+    if (first || knob_time(t.knob, t.cur_ms, t.cur_stage) < knob_time(t.knob, t.best_ms, t.best_stage)) {
         t.best_ms = t.cur_ms;
+        for (int i = 0; i < 3; ++i) t.best_stage[i] = t.cur_stage[i];
         t.best = c;
     }
     t.cur_ms = 1e30f;
+    for (float& x : t.cur_stage) x = 1e30f;
     t.rep = 0;
     ++t.option;
 }
@@ -822,7 +841,7 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
             sum.vertex_rows = s.vertex_rows;
             sum.tiled = s.tiled;
             sum.tuned = tune ? 1 : tunable(B) ? 2 : 0;
-            if (tune) tune_record(*tune, trial, sum.ms_total);
+            if (tune) tune_record(*tune, trial, sum);
             set_stats(sum);
             return PGPU_OK;
         }

@@ -105,7 +105,9 @@ struct Engine {
         };
         int knob = 0, option = 0, rep = 0, trials = 0;
         bool done = false;
-        float best_ms = 1e30f, cur_ms = 1e30f;
+        float best_ms = 1e30f;            // the best setting's whole-lattice time
+        float best_stage[3] = {};         // and its splat, neighbours, blur times (0: untimed)
+        float cur_ms = 1e30f, cur_stage[3] = {1e30f, 1e30f, 1e30f};
         Setting best;
     };
     std::map<std::string, Tuning> tuning;

@@ -663,6 +663,22 @@ __device__ __forceinline__ uint32_t await_vertex(const SplatArgs& a, uint32_t s,
     return 0xFFFFFFFFu;
 }
 
+// One (point, remainder) entry of the tile splat's phase C: its weighted row into row s
+// (VROWS: vertex s; otherwise segment slot s; 0xFFFFFFFF: not placed) and its record.
+template <int D, int VDP, bool VROWS>
+__device__ __forceinline__ void splat_entry(const SplatArgs& a, float* vals, uint32_t slot_base, uint32_t gi,
+                                            int r, uint32_t s, float w, const float (&v)[VDP]) {
+    if (s != 0xFFFFFFFFu) {
+        float c[VDP];
+#pragma unroll
+        for (int q = 0; q < VDP; ++q) c[q] = __fmul_rn(w, v[q]);
+        atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
+    }
+    if (a.rec_slot)
+        a.rec_slot[(size_t)r * a.n_total + gi] = s == 0xFFFFFFFFu ? 0xFFFFFFFFu : VROWS ? s : slot_base + s;
+    if (a.rec_w) a.rec_w[(size_t)r * a.n_total + gi] = w;
+}
+
 // VROWS: number vertices as they are created and accumulate into vertex-ordered rows (the
 // SplatArgs::vrows protocol, d <= 6, no first touches); otherwise rows in slot space.
 template <int D, int VDP, bool VROWS>
@@ -816,42 +832,45 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
             }
             __syncthreads();
         }
-#pragma unroll 1
-        for (uint32_t j = threadIdx.x; j < count; j += kTileThreads) {
-            const int l = t_list[j];
-            const uint32_t val = t_ft[l];
-            if (val != 0xFFFFFFFFu && (val & 0x80000000u)) t_ft[l] = await_vertex(a, val & 0x7FFFFFFFu, status);
-        }
-        __syncthreads();
     } else {
         if (a.vlist) block_list_flush(blist, a, kseg);
     }
 
-    // Phase C: every lane's rows into its vertices' global rows, and the replay record
+    // Phase C: every lane's rows into its vertices' global rows, and the replay record.
+    // VROWS: entries whose vertex another block created and has not numbered yet (t_ft
+    // still holds 0x80000000 | slot) wait until the entries already known are sent, by
+    // which time their creators have almost always published them.
     if (!valid) return;
+    uint32_t pending = 0;
 #pragma unroll
     for (int r = 0; r <= D; ++r) {
         const int l = loc[r];
         uint32_t s;
         if (l >= 0) {
             s = t_ft[l];
+            if (VROWS && s != 0xFFFFFFFFu && (s & 0x80000000u)) {
+                pending |= 1u << r;
+                continue;
+            }
         } else if (l <= -2) {
             s = (uint32_t)(-(l + 2));
-            if constexpr (VROWS)
-                if (!(direct_v & (1u << r))) s = await_vertex(a, sg.slot_base + s, status);
+            if (VROWS && !(direct_v & (1u << r))) {
+                pending |= 1u << r;
+                continue;
+            }
         } else {
             s = 0xFFFFFFFFu;
         }
-        if (s != 0xFFFFFFFFu) {
-            float c[VDP];
+        splat_entry<D, VDP, VROWS>(a, vals, sg.slot_base, gi, r, s, bary[r], v);
+    }
+    if constexpr (VROWS) {
 #pragma unroll
-            for (int q = 0; q < VDP; ++q) c[q] = __fmul_rn(bary[r], v[q]);
-            atomic_add_row<VDP>(vals + (size_t)s * VDP, c);
+        for (int r = 0; r <= D; ++r) {
+            if (!(pending & (1u << r))) continue;
+            const int l = loc[r];
+            const uint32_t gs = l >= 0 ? (t_ft[l] & 0x7FFFFFFFu) : sg.slot_base + (uint32_t)(-(l + 2));
+            splat_entry<D, VDP, VROWS>(a, vals, sg.slot_base, gi, r, await_vertex(a, gs, status), bary[r], v);
         }
-        if (a.rec_slot)
-            a.rec_slot[(size_t)r * a.n_total + gi] =
-                s == 0xFFFFFFFFu ? 0xFFFFFFFFu : VROWS ? s : sg.slot_base + s;
-        if (a.rec_w) a.rec_w[(size_t)r * a.n_total + gi] = bary[r];
     }
 }
 
