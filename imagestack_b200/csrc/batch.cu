@@ -656,39 +656,41 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     return finish_pass(E, B, ps, failed, cap_next);
 }
 
-// Autotuner: coordinate descent over six knobs, starting from load 0.5, blur axes in
-// pairs, the capped blur grid, the tile splat and slot-space rows.  Each knob's options are
-// tried with the best setting found so far for the other knobs, each twice (the faster
-// time counts: the first call of a shape also learns its vertex ratio), by the device time
-// of what the knob changes (knob_time):
+// Autotuner: coordinate descent over six knobs, starting from load 0.5, the tile splat,
+// slot-space rows, two neighbour lookups, blur axes in pairs and the capped blur grid.
+// Each knob's options are tried with the best setting found so far for the other knobs,
+// each twice (the faster time counts: the first call of a shape also learns its vertex
+// ratio), by the device time of what the knob changes (knob_time):
 //   0. hash-table load factor 0.5 / 0.35 / 0.7;
-//   1. blur passes: axes fused in pairs, or one axis per pass (16-bit payloads: rows kept
-//      in FP32 after every first axis of a would-be pair and rounded to 16 bits after the
-//      second, as a pair rounds them, so the results are the same bit for bit);
-//   2. blur grid: 16 blocks per SM striding over the vertices, one vertex per thread, or
-//      (one-axis passes) 16 blocks per SM with two vertices per iteration;
-//   3. splat: the tile splat wherever the learned vertex density allows it, or the direct
+//   1. splat: the tile splat wherever the learned vertex density allows it, or the direct
 //      splat for every image;
-//   4. rows: in slot space with a compaction into vertex order, or numbered by the tile
+//   2. rows: in slot space with a compaction into vertex order, or numbered by the tile
 //      splat as it creates the vertices, in vertex order from the start (where every image
 //      of the batch takes the tile splat);
-//   5. neighbour search (vertex-ordered rows only): two lookups per axis, or one (n1) with
-//      the other pair entry written by the neighbour found (n2(n1(v)) = v).
+//   3. neighbour search (vertex-ordered rows only): two lookups per axis, or one (n1) with
+//      the other pair entry written by the neighbour found (n2(n1(v)) = v);
+//   4. blur passes: axes fused in pairs, or one axis per pass (16-bit payloads: rows kept
+//      in FP32 after every first axis of a would-be pair and rounded to 16 bits after the
+//      second, as a pair rounds them, so the results are the same bit for bit);
+//   5. blur grid: 16 blocks per SM striding over the vertices, one vertex per thread, or
+//      (one-axis passes) 16 blocks per SM with two vertices per iteration.
 // Keys, vertex order and FP32/FP64 results do not depend on the choice.
 constexpr float kTuneLoads[] = {0.5f, 0.35f, 0.7f};
 constexpr int kTuneKnobs = 6;
 constexpr int kTuneReps = 2;
 
-static int knob_options(int k) { return k == 0 || k == 2 ? 3 : 2; }
+// knobs in the order they are walked: 0 load, 1 splat kernel, 2 rows, 3 neighbour search,
+// 4 blur pairing, 5 blur grid (the blur's best form depends on the row layout)
+static int knob_options(int k) { return k == 0 || k == 5 ? 3 : 2; }
 
 static Engine::Tuning::Setting with_option(Engine::Tuning::Setting s, int k, int o) {
     switch (k) {
     case 0: s.load = kTuneLoads[o]; break;
-    case 1: s.pairs = o == 0; break;
-    case 2: s.blur_grid = o; break;
-    case 3: s.splat = o; break;
-    case 4: s.vertex_rows = o; break;
-    case 5: s.nbr_half = o; break;
+    case 1: s.splat = o; break;
+    case 2: s.vertex_rows = o; break;
+    case 3: s.nbr_half = o; break;
+    case 4: s.pairs = o == 0; break;
+    case 5: s.blur_grid = o; break;
     }
     return s;
 }
@@ -731,8 +733,8 @@ static bool tune_next(Engine::Tuning& t, bool singles_ok, Engine::Tuning::Settin
 static float knob_time(int knob, float total, const float (&stage)[3]) {
     const bool staged = stage[0] > 0.0f && stage[0] < 1e29f;
     if (!staged) return total;
-    if (knob == 1 || knob == 2) return stage[2];
-    if (knob == 5) return stage[0] + stage[1];
+    if (knob == 4 || knob == 5) return stage[2];
+    if (knob == 3) return stage[0] + stage[1];
     return total;
 }
 

@@ -4,6 +4,12 @@
 
 #include "lattice_ops.h"
 
+// tile splat tiles: PGPU_TILE_W pixels wide, kTilePixels / PGPU_TILE_W high (a power of two
+// up to kTilePixels; 16 measured best on the 4K d=5 bilateral)
+#ifndef PGPU_TILE_W
+#define PGPU_TILE_W 16u
+#endif
+
 namespace pgpu {
 
 __global__ void mark_kernel(const uint32_t* __restrict__ ft, uint32_t cap, uint32_t* bitmap) {
@@ -137,7 +143,7 @@ void segment_geometry(Segment& s, const PointSource& slice_src, bool tiled, uint
     if (tiled) {
         // 16x16 tiles (a warp is two rows of 16 pixels); a point list (one row) in runs
         // of kTilePixels
-        s.tile_w = (H == 1 && F == 1) ? (uint32_t)kTilePixels : std::min<uint32_t>(16u, pow2_at_least(W));
+        s.tile_w = (H == 1 && F == 1) ? (uint32_t)kTilePixels : std::min<uint32_t>(PGPU_TILE_W, pow2_at_least(W));
         s.tile_h = (uint32_t)kTilePixels / s.tile_w;
         s.tiles_x = (W + s.tile_w - 1) / s.tile_w;
         s.tiles_y = (H + s.tile_h - 1) / s.tile_h;

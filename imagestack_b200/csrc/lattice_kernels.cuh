@@ -832,45 +832,35 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
             }
             __syncthreads();
         }
+        // the numbers of the tile's vertices that other blocks created, once per vertex
+        // (faster than every lane waiting for its own entries at the end of phase C)
+#pragma unroll 1
+        for (uint32_t j = threadIdx.x; j < count; j += kTileThreads) {
+            const int l = t_list[j];
+            const uint32_t val = t_ft[l];
+            if (val != 0xFFFFFFFFu && (val & 0x80000000u)) t_ft[l] = await_vertex(a, val & 0x7FFFFFFFu, status);
+        }
+        __syncthreads();
     } else {
         if (a.vlist) block_list_flush(blist, a, kseg);
     }
 
-    // Phase C: every lane's rows into its vertices' global rows, and the replay record.
-    // VROWS: entries whose vertex another block created and has not numbered yet (t_ft
-    // still holds 0x80000000 | slot) wait until the entries already known are sent, by
-    // which time their creators have almost always published them.
+    // Phase C: every lane's rows into its vertices' global rows, and the replay record
     if (!valid) return;
-    uint32_t pending = 0;
 #pragma unroll
     for (int r = 0; r <= D; ++r) {
         const int l = loc[r];
         uint32_t s;
         if (l >= 0) {
             s = t_ft[l];
-            if (VROWS && s != 0xFFFFFFFFu && (s & 0x80000000u)) {
-                pending |= 1u << r;
-                continue;
-            }
         } else if (l <= -2) {
             s = (uint32_t)(-(l + 2));
-            if (VROWS && !(direct_v & (1u << r))) {
-                pending |= 1u << r;
-                continue;
-            }
+            if constexpr (VROWS)
+                if (!(direct_v & (1u << r))) s = await_vertex(a, sg.slot_base + s, status);
         } else {
             s = 0xFFFFFFFFu;
         }
         splat_entry<D, VDP, VROWS>(a, vals, sg.slot_base, gi, r, s, bary[r], v);
-    }
-    if constexpr (VROWS) {
-#pragma unroll
-        for (int r = 0; r <= D; ++r) {
-            if (!(pending & (1u << r))) continue;
-            const int l = loc[r];
-            const uint32_t gs = l >= 0 ? (t_ft[l] & 0x7FFFFFFFu) : sg.slot_base + (uint32_t)(-(l + 2));
-            splat_entry<D, VDP, VROWS>(a, vals, sg.slot_base, gi, r, await_vertex(a, gs, status), bary[r], v);
-        }
     }
 }
 

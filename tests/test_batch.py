@@ -151,17 +151,17 @@ def test_autotuned_batch_tries_candidates_then_keeps_one(gpu, graph):
             assert rel_err(d.cpu().numpy(), e) <= RTOL_FP32
     trials = [x for x in seen if x[4] == 1]
     n = len(trials)
-    # 6 load trials, 2 one-axis blur, 2 or 4 blur grid (a third option when one-axis passes
-    # won), 2 direct splat, 2 vertex-ordered rows, and 2 one-lookup neighbour searches when
-    # vertex-ordered rows won
+    # 6 load trials, 2 direct splat, 2 vertex-ordered rows, 2 one-lookup neighbour searches
+    # when vertex-ordered rows won, 2 one-axis blur, 2 or 4 blur grid (a third option when
+    # one-axis passes won)
     assert 14 <= n <= 18 and all(x[4] == 1 for x in seen[:n])
     assert [x[0] for x in trials[:6]] == [0.5, 0.5, 0.35, 0.35, 0.7, 0.7]
     assert all(x[1:4] == (1, 0, True) for x in trials[:6])
     best_load = trials[6][0]
     assert best_load in (0.5, 0.35, 0.7) and all(x[0] == best_load for x in trials[6:])
-    assert all(x[1] == 0 for x in trials[6:8])                  # one blur axis per pass
-    assert trials[8][2] == 1 and trials[9][2] == 1              # one vertex per blur thread
-    assert sum(1 for x in trials[8:] if x[3] is False) == 2     # the direct splat, twice
+    assert all(x[3] is False for x in trials[6:8])              # the direct splat, twice
+    assert sum(1 for x in trials if x[1] == 0) >= 2             # one blur axis per pass
+    assert sum(1 for x in trials if x[2] == 1) == 2             # one vertex per blur thread
     assert seen[n] == seen[n + 1] and seen[n][4] == 2
     assert seen[n][:4] in [x[:4] for x in trials]
 
@@ -181,7 +181,7 @@ def test_autotuned_fp16_batch_stays_within_its_error_bound(gpu):
         seen.append((round(st["load_factor"], 2), st["blur_pairs"], st["tuned"]))
         assert max(rel_err(o, r, floor_frac=1e-2) for o, r in zip(out, ref)) <= 1e-3
     assert [l for l, _, _ in seen[:6]] == [0.5, 0.5, 0.35, 0.35, 0.7, 0.7]
-    assert [p for _, p, _ in seen[6:8]] == [0, 0]
+    assert sum(1 for _, p, t in seen if p == 0 and t == 1) >= 2   # one axis per pass tried
     n = sum(1 for _, _, t in seen if t == 1)
     assert 14 <= n <= 18 and [t for _, _, t in seen] == [1] * n + [2] * (20 - n)
 
