@@ -646,6 +646,26 @@ __device__ __forceinline__ void publish_vertex(const SplatArgs& a, uint32_t s, u
     __stcg(reinterpret_cast<unsigned*>(a.key0 + s) + 3, enc_index(v));
 }
 
+// A vertex this block created in global slot gs (local slot l, or 0xFFFF for one placed in
+// the global table directly): onto the block's list, numbered and published by the flush;
+// when the list is full, numbered and published at once (returns its number then, else
+// 0xFFFFFFFF).
+template <int VDP>
+__device__ __forceinline__ uint32_t list_new_vertex(const SplatArgs& a, int kseg, uint32_t* s_new,
+                                                    uint16_t* s_new_l, uint32_t* s_new_count,
+                                                    uint32_t gs, uint16_t l, const uint4& key) {
+    const uint32_t jj = atomicAdd(s_new_count, 1u);
+    if (jj < kBlockListCap) {
+        s_new[jj] = gs;
+        s_new_l[jj] = l;
+        return 0xFFFFFFFFu;
+    }
+    const uint32_t v = atomicAdd(a.vcount, 1u);
+    atomicAdd(a.seg_counts + kseg, 1u);
+    publish_vertex<VDP>(a, gs, v, key);
+    return v;
+}
+
 // the vertex index of global slot s, created by another block: wait (bounded) until its
 // creator has published it, which takes the creator's global inserts and one atomic
 // (microseconds); 0xFFFFFFFF with the spin-limit status bit if it is not published within
@@ -721,12 +741,10 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
 
     // Phase A: this pixel's simplex and the local slot of each of its d+1 vertices.
     // loc[r] >= 0: local slot; -1: not placed; <= -2: global slot -(loc + 2), taken directly
-    // because the local table was full around the key (VROWS: with bit r of `direct_v` set,
-    // -(loc + 2) is already the vertex index).
+    // because the local table was full around the key.
     float v[VDP];
     float bary[D + 1];
     int loc[D + 1];
-    uint32_t direct_v = 0;
     uint32_t gi = 0;
 #pragma unroll
     for (int r = 0; r <= D; ++r) loc[r] = -1;
@@ -753,15 +771,11 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
                 const int s = table_insert<1, VROWS>(table, key, home, __ldcg(&table.key0[home]), status, &created);
                 if (s >= 0) {
                     if constexpr (VROWS) {
-                        if (created) {   // numbered and published at once
-                            const uint32_t vv = atomicAdd(a.vcount, 1u);
-                            atomicAdd(a.seg_counts + kseg, 1u);
-                            publish_vertex<VDP>(a, sg.slot_base + (uint32_t)s, vv, key.w[0]);
-                            direct_v |= 1u << r;
-                            loc[r] = -(int)(vv + 2);
-                        } else {
-                            loc[r] = -(s + 2);
-                        }
+                        // numbered by the flush (phase C reads the number from the key word)
+                        if (created)
+                            list_new_vertex<VDP>(a, kseg, s_new, s_new_l, &s_new_count,
+                                                 sg.slot_base + (uint32_t)s, 0xFFFFu, key.w[0]);
+                        loc[r] = -(s + 2);
                     } else {
                         if (ft) atomicMin(&ft[s], e0 + (uint32_t)r);
                         if (created && a.vlist) block_list_append(blist, a, kseg, sg.slot_base + (uint32_t)s);
@@ -792,16 +806,9 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
                 const uint32_t gs = sg.slot_base + (uint32_t)s;
                 val = 0x80000000u | gs;
                 if (created) {
-                    const uint32_t jj = atomicAdd(&s_new_count, 1u);
-                    if (jj < kBlockListCap) {
-                        s_new[jj] = gs;
-                        s_new_l[jj] = (uint16_t)l;
-                    } else {   // the block's list is full: numbered and published at once
-                        const uint32_t vv = atomicAdd(a.vcount, 1u);
-                        atomicAdd(a.seg_counts + kseg, 1u);
-                        publish_vertex<VDP>(a, gs, vv, kk.w[0]);
-                        val = vv;
-                    }
+                    const uint32_t vv = list_new_vertex<VDP>(a, kseg, s_new, s_new_l, &s_new_count, gs,
+                                                             (uint16_t)l, kk.w[0]);
+                    if (vv != 0xFFFFFFFFu) val = vv;
                 } else if (has_index(seen.w)) {
                     val = dec_index(seen.w);
                 }
@@ -827,8 +834,12 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
             const uint32_t base = s_new_base;
             for (uint32_t jj = threadIdx.x; jj < n; jj += kTileThreads) {
                 const int l = s_new_l[jj];
-                publish_vertex<VDP>(a, s_new[jj], base + jj, t_key[l]);
-                t_ft[l] = base + jj;
+                if (l != 0xFFFF) {
+                    publish_vertex<VDP>(a, s_new[jj], base + jj, t_key[l]);
+                    t_ft[l] = base + jj;
+                } else {   // placed in the global table directly in phase A
+                    publish_vertex<VDP>(a, s_new[jj], base + jj, __ldcg(&a.key0[s_new[jj]]));
+                }
             }
             __syncthreads();
         }
@@ -855,8 +866,7 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
             s = t_ft[l];
         } else if (l <= -2) {
             s = (uint32_t)(-(l + 2));
-            if constexpr (VROWS)
-                if (!(direct_v & (1u << r))) s = await_vertex(a, sg.slot_base + s, status);
+            if constexpr (VROWS) s = await_vertex(a, sg.slot_base + s, status);
         } else {
             s = 0xFFFFFFFFu;
         }
