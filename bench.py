@@ -79,7 +79,7 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def stage_bytes(N, M, d=D, C=3, p=4, vdp=4, blur_passes=3, vertex_rows=False, nbr_half=False):
+def stage_bytes(N, M, d=D, C=3, p=4, vdp=4, vertex_rows=False, nbr_half=False):
     """Algorithmic bytes of each lattice stage for N points and M vertices: what each stage's
     kernels must move as they are built, every input read once and every output written
     once (a row is vdp values of p bytes; the splat's sums and the slice's rows are FP32).
@@ -94,9 +94,10 @@ def stage_bytes(N, M, d=D, C=3, p=4, vdp=4, blur_passes=3, vertex_rows=False, nb
       neighbours  key M*16 read, one table slot M*16 per lookup (2(d+1) lookups, or d+1
                   with one lookup per axis plus a 4-byte pair entry written per lookup), the
                   pairs M*8*(d+1) written
-      blur        per pass: rows M*p*vdp read and written, neighbour pairs M*8 per axis;
-                  the last pass writes FP32 rows M*4*vdp (slot-space rows: through the
-                  vertex->slot map M*4)
+      blur        per axis (the separable [1 2 1] passes of the algorithm, however many
+                  axes a launch fuses): rows M*p*vdp read and written and the axis's
+                  neighbour pairs M*8 read; the last axis writes FP32 rows M*4*vdp
+                  (slot-space rows: through the vertex->slot map M*4)
       slice       replay record N*(d+1)*8 and the FP32 rows M*4*vdp read, N*C*4 written"""
     axes = d + 1
     splat = N * C * 4 + N * axes * 8 + M * (16 + 4 * vdp)
@@ -107,9 +108,7 @@ def stage_bytes(N, M, d=D, C=3, p=4, vdp=4, blur_passes=3, vertex_rows=False, nb
         compact = M * (4 + 16 + 4 * vdp) + M * (16 + p * vdp + 8 + 16)
     lookups = axes if nbr_half else 2 * axes
     neighbours = M * 16 + lookups * M * 16 + axes * M * 8 + (lookups * M * 4 if nbr_half else 0)
-    per_pass_axes = axes / blur_passes
-    blur = blur_passes * (2 * M * p * vdp + per_pass_axes * M * 8) + M * (4 * vdp - p * vdp) + \
-        (0 if vertex_rows else M * 4)
+    blur = axes * (2 * M * p * vdp + M * 8) + M * (4 * vdp - p * vdp) + (0 if vertex_rows else M * 4)
     slice_ = N * axes * 8 + M * 4 * vdp + N * C * 4
     return {"splat": int(splat), "compact": int(compact), "neighbours": int(neighbours),
             "blur": int(blur), "slice": int(slice_)}
@@ -742,7 +741,7 @@ def run_ours(args):
         p = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[args.payload]
         N = FRAMES_PER_STEP * n
         passes = blur_launches(D, bool(stage[-1]["blur_pairs"]))
-        sb = stage_bytes(N, M, p=p, blur_passes=passes, vertex_rows=bool(stage[-1]["vertex_rows"]),
+        sb = stage_bytes(N, M, p=p, vertex_rows=bool(stage[-1]["vertex_rows"]),
                          nbr_half=bool(stage[-1]["nbr_half"]))
         splat_bytes = sb["splat"]
         achieved = splat_bytes / (splat_ms / 1e3) / 1e9
