@@ -666,6 +666,10 @@ __device__ __forceinline__ uint32_t list_new_vertex(const SplatArgs& a, int kseg
     return v;
 }
 
+// t_ft marker of a vertex the block created and numbers in its flush (never a vertex index:
+// indices stay below the 2^31 - 256 slots of a batch)
+constexpr uint32_t kOwnPending = 0x7FFFFFFFu;
+
 // the vertex index of global slot s, created by another block: wait (bounded) until its
 // creator has published it, which takes the creator's global inserts and one atomic
 // (microseconds); 0xFFFFFFFF with the spin-limit status bit if it is not published within
@@ -800,7 +804,8 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
         uint4 seen = make_uint4(0u, 0u, 0u, 0u);
         const int s = table_insert<1, VROWS>(table, kk, h, __ldcg(&table.key0[h]), status, &created, &seen);
         if constexpr (VROWS) {
-            // t_ft[l]: the vertex index, or 0x80000000 | global slot while it is not known
+            // t_ft[l]: the vertex index; kOwnPending for a vertex this block numbers in its
+            // flush; 0x80000000 | global slot while another block's vertex is not numbered
             uint32_t val = 0xFFFFFFFFu;
             if (s >= 0) {
                 const uint32_t gs = sg.slot_base + (uint32_t)s;
@@ -808,7 +813,7 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
                 if (created) {
                     const uint32_t vv = list_new_vertex<VDP>(a, kseg, s_new, s_new_l, &s_new_count, gs,
                                                              (uint16_t)l, kk.w[0]);
-                    if (vv != 0xFFFFFFFFu) val = vv;
+                    val = vv != 0xFFFFFFFFu ? vv : kOwnPending;
                 } else if (has_index(seen.w)) {
                     val = dec_index(seen.w);
                 }
@@ -822,8 +827,9 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
     }
     __syncthreads();
     if constexpr (VROWS) {
-        // number the block's new vertices with one atomic, publish them, then learn the
-        // indices of the vertices other blocks created
+        // number the block's new vertices with one atomic and publish them; in the same
+        // pass, learn (once per vertex) the numbers of the tile's vertices other blocks
+        // created, which is faster than every lane waiting for its own entries in phase C
         const uint32_t n = min(s_new_count, kBlockListCap);
         if (n) {
             if (threadIdx.x == 0) {
@@ -831,20 +837,17 @@ __global__ void __launch_bounds__(kTileThreads, tile_min_blocks(D)) splat_tile_k
                 atomicAdd(a.seg_counts + kseg, n);
             }
             __syncthreads();
-            const uint32_t base = s_new_base;
-            for (uint32_t jj = threadIdx.x; jj < n; jj += kTileThreads) {
-                const int l = s_new_l[jj];
-                if (l != 0xFFFF) {
-                    publish_vertex<VDP>(a, s_new[jj], base + jj, t_key[l]);
-                    t_ft[l] = base + jj;
-                } else {   // placed in the global table directly in phase A
-                    publish_vertex<VDP>(a, s_new[jj], base + jj, __ldcg(&a.key0[s_new[jj]]));
-                }
-            }
-            __syncthreads();
         }
-        // the numbers of the tile's vertices that other blocks created, once per vertex
-        // (faster than every lane waiting for its own entries at the end of phase C)
+        const uint32_t base = s_new_base;
+        for (uint32_t jj = threadIdx.x; jj < n; jj += kTileThreads) {
+            const int l = s_new_l[jj];
+            if (l != 0xFFFF) {
+                publish_vertex<VDP>(a, s_new[jj], base + jj, t_key[l]);
+                t_ft[l] = base + jj;
+            } else {   // placed in the global table directly in phase A
+                publish_vertex<VDP>(a, s_new[jj], base + jj, __ldcg(&a.key0[s_new[jj]]));
+            }
+        }
 #pragma unroll 1
         for (uint32_t j = threadIdx.x; j < count; j += kTileThreads) {
             const int l = t_list[j];
