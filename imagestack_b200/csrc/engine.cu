@@ -76,6 +76,32 @@ static cudaMemPool_t device_pool() {
     return pool;
 }
 
+// Make the library's pool on the current device hold `bytes` of device memory (at most
+// half of what is free): one allocation of that size, freed at once, stays in the pool
+// (its release threshold is unlimited), so buffers that grow later are served from memory
+// the pool holds instead of mapping new memory while work is running.
+int reserve_pool_memory(size_t bytes, cudaStream_t st) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return PGPU_OK;
+    }
+    bytes = std::min(bytes, free_b / 2);
+    cudaMemPool_t pool = device_pool();
+    if (!pool || bytes == 0) return PGPU_OK;
+    size_t held = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &held) == cudaSuccess && held >= bytes)
+        return PGPU_OK;
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, bytes, pool, st) != cudaSuccess) {
+        cudaGetLastError();   // a reservation that does not fit is skipped, not an error
+        return PGPU_OK;
+    }
+    CUDA_TRY(cudaFreeAsync(p, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return PGPU_OK;
+}
+
 // Every call is synchronous, so when a buffer grows (at the start of a call) no earlier
 // work still uses the old block, whichever stream it ran on.
 int DevBuf::ensure(size_t need) {

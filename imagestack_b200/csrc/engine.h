@@ -131,6 +131,8 @@ PlanarView planar(const pgpu_image& v);
 OutView outview(const pgpu_image& v, int channels, int normalize);
 
 int get_engine(int dev, Engine** out);
+// hold `bytes` of device memory in the library's pool of the current device (engine.cu)
+int reserve_pool_memory(size_t bytes, cudaStream_t st);
 // finish every queued host batch of E (engine.cu); E.mu held
 void drain_async(Engine& E);
 int device_count_sm100();

@@ -315,6 +315,16 @@ int pgpu_server_create(const pgpu_server_config* cfg_in, void** out) {
         }
         S->engines.push_back(e);
     }
+    // The workspaces of requests admitted under the budget come from memory the library's
+    // pool already holds: reserving the budget now keeps their growth under load from
+    // mapping new device memory in the middle of the stream (served outliers of 100-350 ms).
+    {
+        const int rc = reserve_pool_memory((size_t)cfg.memory_budget, S->engines[0]->stream);
+        if (rc) {
+            for (Engine* x : S->engines) { x->shutdown(); delete x; }
+            return rc;
+        }
+    }
     Server* raw = S.get();
     for (int w = 0; w < cfg.workers; ++w) S->threads.emplace_back([raw, w] { raw->worker(w); });
     *out = S.release();
