@@ -832,11 +832,13 @@ def run_ours(args):
                           "rows": "vertex-ordered by the splat" if stage[-1]["vertex_rows"]
                                   else "slot space + compaction",
                           "neighbour_lookups_per_axis": 1 if stage[-1]["nbr_half"] else 2,
+                          "tiles": "%dx%d" % (stage[-1]["tile_w"], 256 // max(1, stage[-1]["tile_w"])),
                           "calls": tune_calls,
                           "knobs": "coordinate descent, each option timed twice: load factor "
                                    "0.5/0.35/0.7, blur axes in pairs or one per pass (FP32/FP64), "
                                    "blur grid, tile or direct splat, slot-space or vertex-ordered "
-                                   "rows, one or two neighbour lookups per axis"},
+                                   "rows, one or two neighbour lookups per axis, 16x16 or 32x8 "
+                                   "tiles"},
             "stages_ms": stages, "vertices": M, "capacity": stage[-1]["capacity"],
             "clocks": clk.summary(),
         }

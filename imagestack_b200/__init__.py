@@ -62,7 +62,7 @@ class Stats(C.Structure):
                 ("ms_blur", C.c_float), ("ms_slice", C.c_float), ("ms_total", C.c_float),
                 ("load_factor", C.c_float), ("blur_pairs", C.c_int), ("tiled", C.c_int),
                 ("blur_grid", C.c_int), ("tuned", C.c_int), ("nbr_half", C.c_int),
-                ("vertex_rows", C.c_int)]
+                ("vertex_rows", C.c_int), ("tile_w", C.c_int)]
 
 
 from .tmpfile import load_tmp, save_tmp  # noqa: E402,F401  (ImageStack .tmp files)

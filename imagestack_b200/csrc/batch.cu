@@ -245,7 +245,8 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         sgm.point_base = pbase[k];
         const bool tiled = tile_ok && (forced == 2 || (density[k] <= kTileRatioMax && it.n >= 256));
         uint32_t nb_splat = 0, nb_tile = 0, nb_slice = 0;
-        segment_geometry(sgm, B.replay ? it.splat : it.slice, tiled, &nb_splat, &nb_tile, &nb_slice);
+        segment_geometry(sgm, B.replay ? it.splat : it.slice, tiled, &nb_splat, &nb_tile, &nb_slice,
+                         (uint32_t)B.tile_w);
         tiled_count += tiled ? 1 : 0;
         sgm.splat_base = (uint32_t)blocks;
         sgm.tile_base = (uint32_t)tile_blocks;
@@ -520,7 +521,7 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
                 (uint64_t)(uintptr_t)E.recw.p, (uint64_t)(uintptr_t)E.meta.p, (uint64_t)(uintptr_t)h,
                 (uint64_t)(uintptr_t)E.sval.p, (uint64_t)(uintptr_t)E.vlist.p, (uint64_t)(uintptr_t)E.vv0.p,
                 (uint64_t)(uintptr_t)E.vv1.p, (uint64_t)(uintptr_t)E.vkey0.p, (uint64_t)(uintptr_t)E.vf32.p,
-                (uint64_t)vrows, (uint64_t)(uintptr_t)E.vtx2slot.p, (uint64_t)nbr_half};
+                (uint64_t)vrows, (uint64_t)(uintptr_t)E.vtx2slot.p, (uint64_t)nbr_half, (uint64_t)B.tile_w};
             gk.reserve(gk.size() + 2 * (size_t)nseg);
             for (int k = 0; k < nseg; ++k) {
                 gk.push_back(cap[k]);
@@ -564,6 +565,7 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         ps->nbr_half = (vrows && nbr_half) ? 1 : 0;
         ps->vertex_rows = vrows ? 1 : 0;
         ps->blur_pairs = blur_pairs ? 1 : 0;
+        ps->tile_w = B.tile_w ? B.tile_w : 16;
         return PGPU_OK;
     }
 }
@@ -630,6 +632,7 @@ static int finish_pass(Engine& E, const BatchJob& B, const PassState& ps, std::v
     s.blur_grid = B.blur_grid;
     s.nbr_half = ps.nbr_half;
     s.vertex_rows = ps.vertex_rows;
+    s.tile_w = ps.tile_w;
     s.tiled = ps.tiled;
     if (ps.timed == 1) {
         cudaEventElapsedTime(&s.ms_splat, E.ev[0], E.ev[1]);
@@ -673,14 +676,15 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
 //      in FP32 after every first axis of a would-be pair and rounded to 16 bits after the
 //      second, as a pair rounds them, so the results are the same bit for bit);
 //   5. blur grid: 16 blocks per SM striding over the vertices, one vertex per thread, or
-//      (one-axis passes) 16 blocks per SM with two vertices per iteration.
+//      (one-axis passes) 16 blocks per SM with two vertices per iteration;
+//   6. tile splat tiles (the blocks per image): 16x16 or 32x8 pixels (splat time).
 // Keys, vertex order and FP32/FP64 results do not depend on the choice.
 constexpr float kTuneLoads[] = {0.5f, 0.35f, 0.7f};
-constexpr int kTuneKnobs = 6;
+constexpr int kTuneKnobs = 7;
 constexpr int kTuneReps = 2;
 
 // knobs in the order they are walked: 0 load, 1 splat kernel, 2 rows, 3 neighbour search,
-// 4 blur pairing, 5 blur grid (the blur's best form depends on the row layout)
+// 4 blur pairing, 5 blur grid (the blur's best form depends on the row layout), 6 tiles
 static int knob_options(int k) { return k == 0 || k == 5 ? 3 : 2; }
 
 static Engine::Tuning::Setting with_option(Engine::Tuning::Setting s, int k, int o) {
@@ -691,13 +695,14 @@ static Engine::Tuning::Setting with_option(Engine::Tuning::Setting s, int k, int
     case 3: s.nbr_half = o; break;
     case 4: s.pairs = o == 0; break;
     case 5: s.blur_grid = o; break;
+    case 6: s.tile_w = o == 0 ? 16 : 32; break;
     }
     return s;
 }
 
 static bool same_setting(const Engine::Tuning::Setting& a, const Engine::Tuning::Setting& b) {
     return a.load == b.load && a.pairs == b.pairs && a.blur_grid == b.blur_grid && a.splat == b.splat &&
-           a.vertex_rows == b.vertex_rows && a.nbr_half == b.nbr_half;
+           a.vertex_rows == b.vertex_rows && a.nbr_half == b.nbr_half && a.tile_w == b.tile_w;
 }
 
 // the next setting to try (skipping options that are the best setting itself, already
@@ -735,6 +740,7 @@ static float knob_time(int knob, float total, const float (&stage)[3]) {
     if (!staged) return total;
     if (knob == 4 || knob == 5) return stage[2];
     if (knob == 3) return stage[0] + stage[1];
+    if (knob == 6) return stage[0];
     return total;
 }
 
@@ -780,6 +786,7 @@ static void apply_setting(BatchJob& B, const Engine::Tuning::Setting& s) {
     B.splat = s.splat;
     B.slot_rows = !s.vertex_rows;
     B.nbr_half = s.nbr_half;
+    B.tile_w = s.tile_w;
 }
 
 bool tuned_settings(Engine& E, const BatchJob& B, BatchJob* out) {
@@ -841,6 +848,7 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
             sum.blur_grid = s.blur_grid;
             sum.nbr_half = s.nbr_half;
             sum.vertex_rows = s.vertex_rows;
+            sum.tile_w = s.tile_w;
             sum.tiled = s.tiled;
             sum.tuned = tune ? 1 : tunable(B) ? 2 : 0;
             if (tune) tune_record(*tune, trial, sum);

@@ -654,6 +654,7 @@ void complete_oldest(Engine& E) {
             sum.blur_grid = s.blur_grid;
             sum.nbr_half = s.nbr_half;
             sum.vertex_rows = s.vertex_rows;
+            sum.tile_w = s.tile_w;
             sum.tuned = c.job.autotune ? 2 : 0;
             sum.tiled += s.tiled;
         }
@@ -801,6 +802,7 @@ int bilateral_batch_host(Engine& E, cudaStream_t st, const pgpu_image* ims, cons
                     sum.blur_grid = s.blur_grid;
                     sum.nbr_half = s.nbr_half;
                     sum.vertex_rows = s.vertex_rows;
+                    sum.tile_w = s.tile_w;
                     if (s.tuned == 1 || sum.tuned != 1) sum.tuned = s.tuned;   // 1 if any chunk was a trial
                     sum.tiled += s.tiled;
                     sum.retries += s.retries;

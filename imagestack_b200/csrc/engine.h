@@ -102,6 +102,7 @@ struct Engine {
             int splat = 0;
             int vertex_rows = 0;
             int nbr_half = 0;
+            int tile_w = 16;
         };
         int knob = 0, option = 0, rep = 0, trials = 0;
         bool done = false;
@@ -161,6 +162,7 @@ struct BatchJob {
     bool slot_rows = true;    // rows in slot space with a compaction; false: the tile splat
                               // numbers vertices and fills vertex-ordered rows where it can
     int nbr_half = 0;         // with vertex-ordered rows: one neighbour lookup per axis (1) or two (0)
+    int tile_w = 0;           // tile splat tile width in pixels (0: the default, 16; height 256 / width)
     std::vector<BatchItem> items;
     // parity dumps (single-item jobs)
     int* rec_vtx = nullptr;
@@ -185,6 +187,7 @@ struct PassState {
     int nbr_half = 0;   // the neighbour search looked up one direction per axis
     int vertex_rows = 0;   // the splat filled vertex-ordered rows (no compaction)
     int blur_pairs = 1;    // blur axes fused in pairs
+    int tile_w = 16;       // tile splat tile width
 };
 // Bytes of pinned metadata a batch of nseg replayed lattices stages.
 size_t batch_meta_bytes(int nseg);

@@ -4,8 +4,8 @@
 
 #include "lattice_ops.h"
 
-// tile splat tiles: PGPU_TILE_W pixels wide, kTilePixels / PGPU_TILE_W high (a power of two
-// up to kTilePixels; 16 measured best on the 4K d=5 bilateral)
+// default tile splat tiles: PGPU_TILE_W pixels wide, kTilePixels / PGPU_TILE_W high (a
+// power of two up to kTilePixels; the autotuner also tries 32x8)
 #ifndef PGPU_TILE_W
 #define PGPU_TILE_W 16u
 #endif
@@ -133,7 +133,7 @@ static uint32_t pow2_at_least(uint32_t x) {
 }
 
 void segment_geometry(Segment& s, const PointSource& slice_src, bool tiled, uint32_t* splat,
-                      uint32_t* tile, uint32_t* slice) {
+                      uint32_t* tile, uint32_t* slice, uint32_t tile_w) {
     const PointSource& q = s.src;
     s.src.pos_is_val = q.pos.base == q.val.base && q.pos.ystride == q.val.ystride &&
                        q.pos.tstride == q.val.tstride && q.pos.cstride == q.val.cstride &&
@@ -141,9 +141,10 @@ void segment_geometry(Segment& s, const PointSource& slice_src, bool tiled, uint
     const uint32_t W = (uint32_t)s.src.width, H = (uint32_t)s.src.height, F = (uint32_t)s.src.frames;
     const uint64_t n = (uint64_t)W * H * F;
     if (tiled) {
-        // 16x16 tiles (a warp is two rows of 16 pixels); a point list (one row) in runs
-        // of kTilePixels
-        s.tile_w = (H == 1 && F == 1) ? (uint32_t)kTilePixels : std::min<uint32_t>(PGPU_TILE_W, pow2_at_least(W));
+        // tile_w x (kTilePixels / tile_w) tiles (16x16 by default: a warp is two rows of
+        // 16 pixels); a point list (one row) in runs of kTilePixels
+        const uint32_t tw = tile_w ? tile_w : (uint32_t)PGPU_TILE_W;
+        s.tile_w = (H == 1 && F == 1) ? (uint32_t)kTilePixels : std::min<uint32_t>(tw, pow2_at_least(W));
         s.tile_h = (uint32_t)kTilePixels / s.tile_w;
         s.tiles_x = (W + s.tile_w - 1) / s.tile_w;
         s.tiles_y = (H + s.tile_h - 1) / s.tile_h;

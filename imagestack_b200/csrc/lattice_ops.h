@@ -40,7 +40,7 @@ const DimOps* dim_ops(int d);
 // sliced, are set): the direct-splat blocks or, when `tiled`, the tile-splat tiles, and
 // the slice tiles.  Returns the blocks of each launch through *splat, *tile and *slice.
 void segment_geometry(Segment& s, const PointSource& slice_src, bool tiled, uint32_t* splat,
-                      uint32_t* tile, uint32_t* slice);
+                      uint32_t* tile, uint32_t* slice, uint32_t tile_w = 0);
 
 void launch_mark(const uint32_t* ft, uint32_t cap, uint32_t* bitmap, int sms, cudaStream_t st);
 // per-segment vertex counts from the first-touch bitmap and its prefix popcount

@@ -83,6 +83,7 @@ typedef struct pgpu_stats {
     int tuned;             /* autotuner: 0 off, 1 this call was one of its trials, 2 its choice */
     int nbr_half;          /* 1: one neighbour lookup per axis (the other pair entry scattered) */
     int vertex_rows;       /* 1: the splat numbered vertices and filled vertex-ordered rows (no compaction) */
+    int tile_w;            /* tile splat tile width in pixels (tiles of 256 pixels) */
 } pgpu_stats;
 
 /* Fill *opt with the defaults. */
