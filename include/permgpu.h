@@ -131,10 +131,12 @@ int pgpu_bilateral(pgpu_image *im, float filter_width, float filter_height,
  * as a CUDA graph and replays it for later batches of the same shape.
  * opt->flags & PGPU_FLAG_AUTOTUNE lets the first calls of each batch shape (the number
  * of images, the point count to a power of two, d, the payload) try candidate settings
- * — hash-table load factor 0.5, 0.35 or 0.7, blur axes fused in pairs or (FP32/FP64
- * payloads only) one per pass, the tile splat where it applies or the direct splat for
- * every image — and keeps the fastest for later calls of that shape (opt->load_factor is
- * then unused); results do not depend on the choice. */
+ * one knob at a time — hash-table load factor 0.5, 0.35 or 0.7, the tile splat where it
+ * applies or the direct splat for every image, rows compacted from hash-slot space or
+ * numbered in vertex order by the splat, one or two neighbour lookups per axis, blur axes
+ * fused in pairs or one per pass, the blur's launch shape, 16x16 or 32x8 splat tiles —
+ * and keeps the fastest for later calls of that shape (opt->load_factor is then unused);
+ * results do not depend on the choice beyond the FP32 tolerance. */
 #define PGPU_FLAG_GRAPH 1
 #define PGPU_FLAG_AUTOTUNE 2
 int pgpu_bilateral_batch(pgpu_image *ims, int count, const float *filter_width,
