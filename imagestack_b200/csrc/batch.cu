@@ -110,6 +110,62 @@ uint64_t item_signature(int d, const PointSource& s) {
     return h;
 }
 
+// Each image's learned vertices-per-point ratio (by signature, else the latest batch's
+// largest for d, else 1.0: a large table), and the density the splat choice goes by (the
+// learned ratio, else the latest batch's for d, else 0: nothing known, the tile splat).
+void learned_ratios(const BatchJob& B, std::vector<uint64_t>* sig, std::vector<double>* ratio,
+                    std::vector<double>* density) {
+    const int nseg = (int)B.items.size();
+    sig->resize(nseg);
+    ratio->resize(nseg);
+    density->resize(nseg);
+    std::lock_guard<std::mutex> lk(g_ratio_mu);
+    const bool have_d = g_ratio.count(B.d) != 0;
+    const double dflt = have_d ? g_ratio[B.d] : 1.0;
+    for (int k = 0; k < nseg; ++k) {
+        (*sig)[k] = item_signature(B.d, B.items[k].splat);
+        auto it = g_ratio_by_sig.find((*sig)[k]);
+        (*ratio)[k] = it != g_ratio_by_sig.end() ? it->second : dflt;
+        (*density)[k] = it != g_ratio_by_sig.end() ? it->second : have_d ? dflt : 0.0;
+    }
+}
+
+// Splat kernel per lattice: the tile splat (shared-memory table per 16x16 tile) where
+// neighbouring points share vertices, which the learned vertices-per-point ratio tells
+// (4K d=5 bilateral: 0.18; a 16x16 tile then holds about 155 of its 1536 entries'
+// vertices); the direct splat for sparse lattices (ratio above kTileRatioMax: measured
+// on the mixed batch, 1.5 beats 0.8 by 2 % and 0.4 by 3 %), multi-word keys and FP64
+// accumulators.  With nothing learned yet for the image or its d, the tile splat.
+// PGPU_SPLAT=direct or =tile in the environment overrides the choice where both exist
+// (the parity tests compare the two).
+#ifndef PGPU_TILE_RATIO_MAX
+#define PGPU_TILE_RATIO_MAX 1.5
+#endif
+constexpr double kTileRatioMax = PGPU_TILE_RATIO_MAX;
+
+int splat_forced() {
+    const char* mode = std::getenv("PGPU_SPLAT");
+    return !mode ? 0 : !strcmp(mode, "direct") ? 1 : !strcmp(mode, "tile") ? 2 : 0;
+}
+
+bool tile_splat_for(const BatchJob& B, int forced, double density, uint32_t n) {
+    const bool tile_ok = key_words(B.d) == 1 && B.payload != kPayloadF64 && forced != 1 &&
+                         (forced == 2 || B.splat == 0);
+    return tile_ok && (forced == 2 || (density <= kTileRatioMax && n >= 256));
+}
+
+// the job asks for vertex-ordered rows (PGPU_ROWS=slot or =vertex in the environment
+// overrides the job's choice; the parity tests compare both), where they can apply
+bool vertex_rows_wanted(const BatchJob& B) {
+    const char* rows_mode = std::getenv("PGPU_ROWS");
+    const bool want = rows_mode && !strcmp(rows_mode, "vertex") ? true
+                    : rows_mode && !strcmp(rows_mode, "slot")   ? false
+                                                                : !B.slot_rows;
+    const bool dumps = B.rec_vtx || B.dump_splat;
+    return want && !dumps && B.replay && key_words(B.d) == 1 && index_in_key(B.d) &&
+           B.payload != kPayloadF64;
+}
+
 // device (and pinned host) metadata of one batch
 struct MetaLayout {
     size_t segstat, counts, slotbase, entry, segs, slsegs, total;
@@ -189,21 +245,9 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     const uint32_t nwords = (uint32_t)((entries + 31) / 32);
 
     // slots per lattice: (learned vertices per point) x 1.3 x points / load
-    std::vector<uint64_t> sig(nseg);
-    std::vector<double> ratio(nseg), density(nseg);
-    {
-        std::lock_guard<std::mutex> lk(g_ratio_mu);
-        const bool have_d = g_ratio.count(d) != 0;
-        const double dflt = have_d ? g_ratio[d] : 1.0;
-        for (int k = 0; k < nseg; ++k) {
-            sig[k] = item_signature(d, B.items[k].splat);
-            auto it = g_ratio_by_sig.find(sig[k]);
-            ratio[k] = it != g_ratio_by_sig.end() ? it->second : dflt;
-            // what the splat choice goes by: the learned ratio, else the latest batch's for
-            // this d, else nothing known (0: the tile splat)
-            density[k] = it != g_ratio_by_sig.end() ? it->second : have_d ? dflt : 0.0;
-        }
-    }
+    std::vector<uint64_t> sig;
+    std::vector<double> ratio, density;
+    learned_ratios(B, &sig, &ratio, &density);
     std::vector<uint64_t> cap(nseg);
     for (int k = 0; k < nseg; ++k) {
         if (cap_in) {
@@ -217,21 +261,8 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         cap[k] = std::max<uint64_t>((c + 31) & ~31ull, 256);
     }
 
-    // Splat kernel per lattice: the tile splat (shared-memory table per 16x16 tile) where
-    // neighbouring points share vertices, which the learned vertices-per-point ratio tells
-    // (4K d=5 bilateral: 0.18; a 16x16 tile then holds about 155 of its 1536 entries'
-    // vertices); the direct splat for sparse lattices (ratio above kTileRatioMax: measured
-    // on the mixed batch, 1.5 beats 0.8 by 2 % and 0.4 by 3 %), multi-word keys and FP64
-    // accumulators.  With nothing learned yet for the image or its d, the
-    // tile splat.  PGPU_SPLAT=direct or =tile in the environment overrides the choice
-    // where both exist (the parity tests compare the two).
-#ifndef PGPU_TILE_RATIO_MAX
-#define PGPU_TILE_RATIO_MAX 1.5
-#endif
-    constexpr double kTileRatioMax = PGPU_TILE_RATIO_MAX;
-    const char* mode = std::getenv("PGPU_SPLAT");
-    const int forced = !mode ? 0 : !strcmp(mode, "direct") ? 1 : !strcmp(mode, "tile") ? 2 : 0;
-    const bool tile_ok = kw == 1 && B.payload != kPayloadF64 && forced != 1 && (forced == 2 || B.splat == 0);
+    // splat kernel per lattice (tile_splat_for)
+    const int forced = splat_forced();
     std::vector<Segment> segs(nseg), slsegs(B.replay ? 0 : nseg);
     uint64_t blocks = 0, tile_blocks = 0, slice_blocks = 0;
     int tiled_count = 0;
@@ -243,7 +274,7 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         sgm.out = it.out;
         sgm.n = it.n;
         sgm.point_base = pbase[k];
-        const bool tiled = tile_ok && (forced == 2 || (density[k] <= kTileRatioMax && it.n >= 256));
+        const bool tiled = tile_splat_for(B, forced, density[k], it.n);
         uint32_t nb_splat = 0, nb_tile = 0, nb_slice = 0;
         segment_geometry(sgm, B.replay ? it.splat : it.slice, tiled, &nb_splat, &nb_tile, &nb_slice,
                          (uint32_t)B.tile_w);
@@ -272,14 +303,7 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     // vertex-ordered FP32 rows, so no compaction runs; the first blur pass reads those
     // rows (16-bit payloads: FP32 rows, homogeneous ones normalised by the neighbour
     // search, once per vertex) and the slice reads rows by vertex index.
-    // PGPU_ROWS=slot or =vertex in the environment overrides the job's choice (the parity
-    // tests compare both).
-    const char* rows_mode = std::getenv("PGPU_ROWS");
-    const bool want_vrows = rows_mode && !strcmp(rows_mode, "vertex") ? true
-                          : rows_mode && !strcmp(rows_mode, "slot")   ? false
-                                                                      : !B.slot_rows;
-    const bool vrows = !exact_order && B.replay && kw == 1 && index_in_key(d) && tiled_count == nseg &&
-                       B.payload != kPayloadF64 && want_vrows;
+    const bool vrows = vertex_rows_wanted(B) && tiled_count == nseg;
     // PGPU_BLUR=pairs or =single in the environment overrides the blur pairing (tests)
     const char* blur_mode = std::getenv("PGPU_BLUR");
     const bool blur_pairs = blur_mode && !strcmp(blur_mode, "pairs") ? true
@@ -806,9 +830,51 @@ int finish_batch(Engine& E, const BatchJob& B, const PassState& ps, std::vector<
     return finish_pass(E, B, ps, failed, nullptr);
 }
 
+// The passes of one batch with fixed settings: images whose range overflowed go again,
+// as a smaller batch with larger ranges.  *sum covers all passes.
+static int run_passes(Engine& E, BatchJob cur, cudaStream_t st, pgpu_stats* sum) {
+    const int d = cur.d, n0 = (int)cur.items.size();
+    std::vector<uint64_t> caps;
+    memset(sum, 0, sizeof(*sum));
+    for (int pass = 0; pass < 6; ++pass) {
+        std::vector<int> failed;
+        std::vector<uint64_t> next;
+        const int rc = run_batch_pass(E, cur, st, caps.empty() ? nullptr : &caps, &failed, &next, pass);
+        if (rc) return rc;
+        pgpu_stats s;
+        if (get_stats(&s)) {
+            if (pass == 0) sum->points = s.points, sum->d = s.d, sum->vd = s.vd, sum->payload = s.payload;
+            sum->vertices += s.vertices;
+            sum->capacity = std::max(sum->capacity, s.capacity);
+            sum->retries = pass;
+            sum->ms_splat += s.ms_splat, sum->ms_compact += s.ms_compact;
+            sum->ms_neighbours += s.ms_neighbours, sum->ms_blur += s.ms_blur;
+            sum->ms_slice += s.ms_slice, sum->ms_total += s.ms_total;
+            if (pass == 0) sum->tiled = s.tiled;
+        }
+        if (failed.empty()) {
+            sum->load_factor = s.load_factor;
+            sum->blur_pairs = s.blur_pairs;
+            sum->blur_grid = s.blur_grid;
+            sum->nbr_half = s.nbr_half;
+            sum->vertex_rows = s.vertex_rows;
+            sum->tile_w = s.tile_w;
+            return PGPU_OK;
+        }
+        BatchJob again = cur;
+        again.items.clear();
+        for (int k : failed) again.items.push_back(cur.items[k]);
+        caps = next;
+        cur = std::move(again);
+    }
+    return fail(PGPU_ERR_CAPACITY, "hash table overfull after retries (d=%d, %d images)", d, n0);
+}
+
 // Every image of a batch is filtered in place, so an image whose range overflowed cannot
 // simply be rerun with its whole batch: the others are finished.  Only the overflowed
-// ones go again, as a smaller batch with larger ranges.  The statistics cover all passes.
+// ones go again (run_passes).  Vertex-ordered rows need every image of the launches on
+// the tile splat; a batch that asks for them but has images for the direct splat runs as
+// two, the tile-splat images with vertex-ordered rows, the others with slot-space rows.
 int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
     if (B.items.empty()) return PGPU_OK;
     BatchJob cur = B;
@@ -824,45 +890,41 @@ int run_batch(Engine& E, const BatchJob& B, cudaStream_t st) {
             apply_setting(cur, t.best);
         }
     }
-    std::vector<uint64_t> caps;
-    pgpu_stats sum;
-    memset(&sum, 0, sizeof(sum));
-    for (int pass = 0; pass < 6; ++pass) {
-        std::vector<int> failed;
-        std::vector<uint64_t> next;
-        const int rc = run_batch_pass(E, cur, st, caps.empty() ? nullptr : &caps, &failed, &next, pass);
-        if (rc) return rc;
-        pgpu_stats s;
-        if (get_stats(&s)) {
-            if (pass == 0) sum.points = s.points, sum.d = s.d, sum.vd = s.vd, sum.payload = s.payload;
-            sum.vertices += s.vertices;
-            sum.capacity = std::max(sum.capacity, s.capacity);
-            sum.retries = pass;
-            sum.ms_splat += s.ms_splat, sum.ms_compact += s.ms_compact;
-            sum.ms_neighbours += s.ms_neighbours, sum.ms_blur += s.ms_blur;
-            sum.ms_slice += s.ms_slice, sum.ms_total += s.ms_total;
-        }
-        if (failed.empty()) {
-            sum.load_factor = s.load_factor;
-            sum.blur_pairs = s.blur_pairs;
-            sum.blur_grid = s.blur_grid;
-            sum.nbr_half = s.nbr_half;
-            sum.vertex_rows = s.vertex_rows;
-            sum.tile_w = s.tile_w;
-            sum.tiled = s.tiled;
-            sum.tuned = tune ? 1 : tunable(B) ? 2 : 0;
-            if (tune) tune_record(*tune, trial, sum);
-            set_stats(sum);
-            return PGPU_OK;
-        }
-        BatchJob again = cur;
-        again.items.clear();
-        for (int k : failed) again.items.push_back(cur.items[k]);
-        caps = next;
-        cur = std::move(again);
+    const int nseg = (int)cur.items.size();
+    std::vector<char> tiled(nseg, 0);
+    int nt = 0;
+    if (nseg > 1 && vertex_rows_wanted(cur)) {
+        std::vector<uint64_t> sig;
+        std::vector<double> ratio, density;
+        learned_ratios(cur, &sig, &ratio, &density);
+        const int forced = splat_forced();
+        for (int k = 0; k < nseg; ++k) nt += (tiled[k] = tile_splat_for(cur, forced, density[k], cur.items[k].n)) ? 1 : 0;
     }
-    return fail(PGPU_ERR_CAPACITY, "hash table overfull after retries (d=%d, %d images)", B.d,
-                (int)B.items.size());
+    pgpu_stats sum;
+    int rc;
+    if (nt > 0 && nt < nseg) {
+        BatchJob a = cur, b = cur;
+        a.items.clear();
+        b.items.clear();
+        b.slot_rows = true;
+        for (int k = 0; k < nseg; ++k) (tiled[k] ? a : b).items.push_back(cur.items[k]);
+        pgpu_stats sa, sb;
+        if ((rc = run_passes(E, a, st, &sa)) || (rc = run_passes(E, b, st, &sb))) return rc;
+        sum = sa;
+        sum.points += sb.points, sum.vertices += sb.vertices;
+        sum.capacity = std::max(sum.capacity, sb.capacity);
+        sum.retries = std::max(sum.retries, sb.retries);
+        sum.ms_splat += sb.ms_splat, sum.ms_compact += sb.ms_compact;
+        sum.ms_neighbours += sb.ms_neighbours, sum.ms_blur += sb.ms_blur;
+        sum.ms_slice += sb.ms_slice, sum.ms_total += sb.ms_total;
+        sum.tiled += sb.tiled;
+    } else if ((rc = run_passes(E, cur, st, &sum))) {
+        return rc;
+    }
+    sum.tuned = tune ? 1 : tunable(B) ? 2 : 0;
+    if (tune) tune_record(*tune, trial, sum);
+    set_stats(sum);
+    return PGPU_OK;
 }
 
 }  // namespace pgpu

@@ -310,6 +310,31 @@ def test_queued_batch_while_the_autotuner_times_runs_at_once(gpu):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("payload,tol", [("fp32", RTOL_FP32), ("fp16", 1e-3)])
+def test_vertex_rows_batch_with_direct_splat_images_runs_as_two(gpu, monkeypatch, payload, tol):
+    """Vertex-ordered rows need every image of the launches on the tile splat: a batch
+    that asks for them, with a sparse image the direct splat takes once its density is
+    learned, runs as two (the tile-splat images with vertex-ordered rows); every output
+    stays within its payload's tolerance of the FP64 lattice."""
+    rng = np.random.default_rng(5)
+    imgs = [synth.image(300 + 40 * k, 220 + 30 * k, 3, rects=8, seed=80 + k) for k in range(3)]
+    imgs.append(rng.random((3, 96, 104), dtype=np.float32))         # sparse: direct splat
+    ss, sr = [8.0, 10.0, 12.0, 1.0], [0.1, 0.12, 0.15, 0.02]
+    monkeypatch.setenv("PGPU_ROWS", "slot")
+    ref = [im.copy() for im in imgs]
+    gpu.bilateral_batch(ref, ss, sr, payload="fp64")
+    monkeypatch.setenv("PGPU_ROWS", "vertex")
+    for call in range(2):   # the first call learns the sparse image's density
+        work = [im.copy() for im in imgs]
+        gpu.bilateral_batch(work, ss, sr, payload=payload)
+        st = gpu.last_stats()
+        for w, r in zip(work, ref):
+            assert rel_err(w, r, floor_frac=1e-2) <= tol
+    assert st["tiled"] == 3 and st["vertex_rows"] == 1
+    assert st["points"] == sum(im.shape[1] * im.shape[2] for im in imgs)
+
+
+@pytest.mark.gpu
 def test_batch_fp16_payload_error_vs_fp64(gpu):
     imgs, ss, sr = uneven_batch(12, seed=5, lo=128, hi=512)
     ref = [im.copy() for im in imgs]
