@@ -226,17 +226,19 @@ def _expect_single(gpu, imgs, ss, sr):
 
 
 @pytest.mark.gpu
-def test_queued_batches_overlap_and_match_the_single_image_path(gpu):
+@pytest.mark.parametrize("rows", ["slot", "vertex"])
+def test_queued_batches_overlap_and_match_the_single_image_path(gpu, monkeypatch, rows):
     """Three queued host batches (out of place, pinned), in flight together and waited for
     out of order: every output equals the single-image path and no input is touched.  A
     batch of more than three chunks makes the device slots turn over within one batch and
-    across batches."""
+    across batches.  Both row layouts."""
     import torch
     sizes = [(2304, 1830), (2048, 2048), (2560, 1640), (1920, 1080), (1200, 900)]
     imgs = [synth.image(w, h, 3, rects=12, seed=90 + k) for k, (w, h) in enumerate(sizes)]
     ss = [12.0, 16.0, 8.0, 10.0, 6.0]
     sr = [0.1, 0.12, 0.08, 0.15, 0.2]
     expect = _expect_single(gpu, imgs, ss, sr)
+    monkeypatch.setenv("PGPU_ROWS", rows)
     keep_in = [torch.from_numpy(im.copy()).pin_memory() for im in imgs]
     keep_out = [[torch.empty(im.shape, dtype=torch.float32).pin_memory() for im in imgs]
                 for _ in range(3)]
@@ -375,15 +377,23 @@ def test_batch_retry_leaves_finished_images_alone(gpu, on_device):
 
 
 @pytest.mark.gpu
-def test_batch_retries_only_what_overflows(gpu):
+@pytest.mark.parametrize("rows", ["slot", "vertex"])
+def test_batch_retries_only_what_overflows(gpu, monkeypatch, rows):
     """A flat image teaches a small vertex ratio; a noisy one in the same batch then
-    overflows its range and is rerun; both results stay exact."""
+    overflows its range and is rerun; both results stay exact, with rows in slot space or
+    numbered by the splat (whose waits for other blocks' vertex numbers must end when the
+    table overflows)."""
     flat = np.full((3, 96, 96), 0.25, np.float32)
     gpu.bilateral_batch([flat.copy()], [16.0], [0.5])
     rng = np.random.default_rng(9)
-    noisy = rng.random((3, 80, 80), dtype=np.float32)
+    # a shape of its own per variant: ratios are learned by shape and sigmas
+    noisy = rng.random((3, 80, 80 + 3 * (rows == "vertex")), dtype=np.float32)
     work = [flat.copy(), noisy.copy()]
+    monkeypatch.setenv("PGPU_ROWS", rows)
     gpu.bilateral_batch(work, [16.0, 1.0], [0.5, 0.02])
+    st = gpu.last_stats()
+    assert st["retries"] >= 1 and st["vertex_rows"] == (rows == "vertex")
+    monkeypatch.setenv("PGPU_ROWS", "slot")
     e0, e1 = flat.copy(), noisy.copy()
     gpu.Bilateral.apply(e0, 16.0, 16.0, 0.0, 0.5)
     gpu.Bilateral.apply(e1, 1.0, 1.0, 0.0, 0.02)
