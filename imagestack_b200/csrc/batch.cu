@@ -309,12 +309,12 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
     const bool blur_pairs = blur_mode && !strcmp(blur_mode, "pairs") ? true
                           : blur_mode && !strcmp(blur_mode, "single") ? false
                                                                        : B.blur_pairs;
-    // one neighbour lookup per axis (vertex-ordered rows only); PGPU_NBR=half or =both
-    // in the environment overrides the job's choice
+    // one neighbour lookup per axis (the splat's creators or the compaction mark the pairs
+    // absent first); PGPU_NBR=half or =both in the environment overrides the job's choice
     const char* nbr_mode = std::getenv("PGPU_NBR");
-    const bool nbr_half = vrows && (nbr_mode && !strcmp(nbr_mode, "half") ? true
-                                    : nbr_mode && !strcmp(nbr_mode, "both") ? false
-                                                                            : B.nbr_half != 0);
+    const bool nbr_half = nbr_mode && !strcmp(nbr_mode, "half") ? true
+                        : nbr_mode && !strcmp(nbr_mode, "both") ? false
+                                                                : B.nbr_half != 0;
     // 16-bit payloads accumulate in FP32 rows (vf32), which the first blur pass reads
     const bool f32_rows = vrows && (B.payload == kPayloadF16 || B.payload == kPayloadBF16);
     const MetaLayout L = layout(nseg, !B.replay);
@@ -451,6 +451,11 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             ca.vlist = exact_order ? nullptr : (const uint32_t*)E.vlist.p;
             ca.nverts = dM;
             ca.index_in_key = index_in_key(d) ? 1 : 0;   // the neighbour lookups expect it
+            if (nbr_half) {
+                ca.nbr_init = (int2*)E.nbr.p;
+                ca.nbr_stride = (uint32_t)cap_total;
+                ca.nbr_axes = d + 1;
+            }
             if (!launch_assign(ca, kw, vdp, B.payload, homog, E.sms, st))
                 return fail(PGPU_ERR_UNSUPPORTED, "assign variant");
             CUDA_TRY(cudaGetLastError());
@@ -476,7 +481,7 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
             na.nbr = (int2*)E.nbr.p;
             na.tags = use_tags ? (const uint8_t*)E.tags.p : nullptr;
             na.seg_status = (const unsigned*)(dmeta + L.segstat);
-            na.half = (vrows && nbr_half) ? 1 : 0;
+            na.half = nbr_half ? 1 : 0;
             if (vrows && homog) {   // the splat's sums, normalised once per vertex here
                 na.norm_rows = (float*)E.vf32.p;
                 na.vdp = vdp;
@@ -586,7 +591,7 @@ static int enqueue_pass(Engine& E, const BatchJob& B, cudaStream_t st,
         ps->n_total = n_total;
         ps->cap_total = cap_total;
         ps->timed = timed ? (graph ? 2 : 1) : 0;
-        ps->nbr_half = (vrows && nbr_half) ? 1 : 0;
+        ps->nbr_half = nbr_half ? 1 : 0;
         ps->vertex_rows = vrows ? 1 : 0;
         ps->blur_pairs = blur_pairs ? 1 : 0;
         ps->tile_w = B.tile_w ? B.tile_w : 16;
@@ -694,8 +699,8 @@ static int run_batch_pass(Engine& E, const BatchJob& B, cudaStream_t st,
 //   2. rows: in slot space with a compaction into vertex order, or numbered by the tile
 //      splat as it creates the vertices, in vertex order from the start (where every image
 //      of the batch takes the tile splat);
-//   3. neighbour search (vertex-ordered rows only): two lookups per axis, or one (n1) with
-//      the other pair entry written by the neighbour found (n2(n1(v)) = v);
+//   3. neighbour search: one lookup per axis (n1), the other pair entry written by the
+//      neighbour found (n2(n1(v)) = v), or two lookups per axis;
 //   4. blur passes: axes fused in pairs, or one axis per pass (16-bit payloads: rows kept
 //      in FP32 after every first axis of a would-be pair and rounded to 16 bits after the
 //      second, as a pair rounds them, so the results are the same bit for bit);
@@ -740,10 +745,8 @@ static bool tune_next(Engine::Tuning& t, bool singles_ok, Engine::Tuning::Settin
         }
         const Engine::Tuning::Setting c = with_option(t.best, t.knob, t.option);
         const bool timed_already = t.best_ms < 1e29f && same_setting(c, t.best);
-        // two vertices per blur iteration exist for one-axis passes only; the one-lookup
-        // neighbour search for vertex-ordered rows only
-        if (timed_already || (!singles_ok && !c.pairs) || (c.pairs && c.blur_grid == 2) ||
-            (c.nbr_half && !c.vertex_rows)) {
+        // two vertices per blur iteration exist for one-axis passes only
+        if (timed_already || (!singles_ok && !c.pairs) || (c.pairs && c.blur_grid == 2)) {
             ++t.option;
             continue;
         }

@@ -101,7 +101,7 @@ struct Engine {
             int blur_grid = 0;
             int splat = 0;
             int vertex_rows = 0;
-            int nbr_half = 0;
+            int nbr_half = 1;
             int tile_w = 16;
         };
         int knob = 0, option = 0, rep = 0, trials = 0;
@@ -161,7 +161,7 @@ struct BatchJob {
     int splat = 0;            // 0: the tile splat where vertices are shared, 1: direct only
     bool slot_rows = true;    // rows in slot space with a compaction; false: the tile splat
                               // numbers vertices and fills vertex-ordered rows where it can
-    int nbr_half = 0;         // with vertex-ordered rows: one neighbour lookup per axis (1) or two (0)
+    int nbr_half = 1;         // one neighbour lookup per axis (1) or two (0)
     int tile_w = 0;           // tile splat tile width in pixels (0: the default, 16; height 256 / width)
     std::vector<BatchItem> items;
     // parity dumps (single-item jobs)

@@ -208,6 +208,11 @@ struct CompactArgs {
     const uint32_t* vlist = nullptr;    // the splat's vertex list (list order), or null:
     const uint32_t* nverts = nullptr;   // first-touch order through ft and the bitmap
     int index_in_key = 0;   // store each vertex's index in its key word (d <= 6)
+    // optional: mark every vertex's neighbour pairs absent (nbr_axes axes, nbr_stride apart)
+    // for the neighbour search that looks up one direction per axis
+    int2* nbr_init = nullptr;
+    uint32_t nbr_stride = 0;
+    int nbr_axes = 0;
 };
 
 struct NbrArgs {
@@ -226,7 +231,8 @@ struct NbrArgs {
     const uint8_t* tags = nullptr;   // slot tags of the compaction, or null: plain lookups
     const unsigned* seg_status = nullptr;   // the splat's per-segment status, or null
     // one lookup per axis: vertex v finds u = n1(v) and, as n2(u) = v, writes v into u's
-    // pair too; every pair must hold (-1, -1) beforehand (the splat's creators write it)
+    // pair too; every pair must hold (-1, -1) beforehand (written by the splat's creators
+    // with vertex-ordered rows, by the compaction otherwise)
     int half = 0;
     // homogeneous FP32 rows the splat left as plain sums (w*m_0.., w), vertex-ordered:
     // each vertex's row is normalised here in place to (m_0.., w), as the compaction
@@ -911,6 +917,8 @@ __device__ __forceinline__ void assign_vertex(const CompactArgs& a, uint32_t s, 
     P* vvals = reinterpret_cast<P*>(a.vvals);
     a.slot2vtx[s] = vtx;
     a.vtx2slot[vtx] = s;
+    if (a.nbr_init)
+        for (int j = 0; j < a.nbr_axes; ++j) a.nbr_init[(size_t)j * a.nbr_stride + vtx] = make_int2(-1, -1);
     const uint4 k0 = a.table.key0[s];
     a.vkey0[vtx] = k0;
     if (KW == 1 && a.index_in_key) a.table.key0[s] = make_uint4(k0.x, k0.y, k0.z, enc_index(vtx));
@@ -1041,20 +1049,19 @@ __global__ void neighbours_kernel(NbrArgs a) {
         key.w[0] = a.vkey0[vtx];
 #pragma unroll
         for (int k = 1; k < KW; ++k) key.w[k] = a.vkeyn[(size_t)(k - 1) * a.vcap + vtx];
-        if constexpr (KW == 1) {
-            if (a.half) {
-                // n1 only: the key one step up along axis j; its vertex u has n2(u) = vtx
-#pragma unroll
-                for (int j = 0; j <= D; ++j) {
-                    Key<KW> k1;
-                    neighbour_key<D>(key, j, +1, k1);
-                    const int u1 = neighbour_index<D>(a, table, base, k1);
-                    int* pair = reinterpret_cast<int*>(a.nbr + (size_t)j * a.vcap);
-                    pair[2 * (size_t)vtx] = u1;
-                    if (u1 >= 0) pair[2 * (size_t)u1 + 1] = (int)vtx;
-                }
-                continue;
+        if (a.half) {
+            // n1 only: the key one step up along axis j; its vertex u has n2(u) = vtx
+            // (axes unrolled for one-word keys, rolled for multi-word keys as below)
+#pragma unroll (KW == 1 ? D + 1 : 1)
+            for (int j = 0; j <= D; ++j) {
+                Key<KW> k1;
+                neighbour_key<D>(key, j, +1, k1);
+                const int u1 = neighbour_index<D>(a, table, base, k1);
+                int* pair = reinterpret_cast<int*>(a.nbr + (size_t)j * a.vcap);
+                pair[2 * (size_t)vtx] = u1;
+                if (u1 >= 0) pair[2 * (size_t)u1 + 1] = (int)vtx;
             }
+            continue;
         }
         // one-word keys: the axes unrolled, so each axis's packed step is a constant;
         // multi-word keys: rolled (d=16, 2M points: 46.7 ms unrolled, 20.5 ms rolled)

@@ -186,7 +186,7 @@ def test_errors_are_reported(gpu):
 def test_full_size_4k_bit_exact_vs_oracle(gpu, monkeypatch):
     """3840x2160 RGB, sigma_s 16, sigma_r 0.1: the whole vertex set and output, the output
     by both row layouts (slot-space rows with a compaction; vertex-ordered rows filled by
-    the splat, with either neighbour search)."""
+    the splat), each with either neighbour search."""
     img = synth.image(3840, 2160, 3, rects=64, seed=2)
     pos, val = oracle.bilateral_points(img, img, 16.0, 0.1)
     ref = oracle.oracle_lattice(pos, val)
@@ -197,13 +197,13 @@ def test_full_size_4k_bit_exact_vs_oracle(gpu, monkeypatch):
     assert sha(d["replay_w"]) == sha(ref.replay_w)
     assert rel_err(d["out"], ref.out) <= RTOL_FP32
     norm = (ref.out[:, :3] / ref.out[:, 3:4]).reshape(2160, 3840, 3).transpose(2, 0, 1)
-    for rows, nbr in (("slot", "both"), ("vertex", "both"), ("vertex", "half")):
+    for rows, nbr in (("slot", "both"), ("slot", "half"), ("vertex", "both"), ("vertex", "half")):
         monkeypatch.setenv("PGPU_ROWS", rows)
         monkeypatch.setenv("PGPU_NBR", nbr)
         out = img.copy()
         gpu.Bilateral.apply(out, 16.0, 16.0, 0.0, 0.1)
         assert gpu.last_stats()["vertex_rows"] == (rows == "vertex")
-        assert gpu.last_stats()["nbr_half"] == (rows == "vertex" and nbr == "half")
+        assert gpu.last_stats()["nbr_half"] == (nbr == "half")
         assert rel_err(out, norm) <= RTOL_FP32, (rows, nbr)
 
 
