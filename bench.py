@@ -90,7 +90,7 @@ def stage_bytes(N, M, d=D, C=3, p=4, vdp=4, vertex_rows=False, nbr_half=False):
                   search, the vertex's absent-neighbour pairs M*8*(d+1))
       compaction  (slot-space rows only) vertex list M*4, key M*16 and row M*4*vdp read;
                   key M*16, row M*p*vdp, both index maps M*8 and the index in the key word
-                  M*16 written
+                  M*16 written (and the absent pairs M*8*(d+1) for the one-lookup search)
       neighbours  key M*16 read, one table slot M*16 per lookup (2(d+1) lookups, or d+1
                   with one lookup per axis plus a 4-byte pair entry written per lookup), the
                   pairs M*8*(d+1) written
@@ -105,7 +105,7 @@ def stage_bytes(N, M, d=D, C=3, p=4, vdp=4, vertex_rows=False, nbr_half=False):
         splat += M * (16 + 4 + 4) + (M * 8 * axes if nbr_half else 0)
         compact = 0
     else:
-        compact = M * (4 + 16 + 4 * vdp) + M * (16 + p * vdp + 8 + 16)
+        compact = M * (4 + 16 + 4 * vdp) + M * (16 + p * vdp + 8 + 16) + (M * 8 * axes if nbr_half else 0)
     lookups = axes if nbr_half else 2 * axes
     neighbours = M * 16 + lookups * M * 16 + axes * M * 8 + (lookups * M * 4 if nbr_half else 0)
     blur = axes * (2 * M * p * vdp + M * 8) + M * (4 * vdp - p * vdp) + (0 if vertex_rows else M * 4)
