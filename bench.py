@@ -150,6 +150,7 @@ class ClockSampler:
             pynvml.nvmlInit()
             h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
             self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self._ready.set()
             while not self._stop.is_set():
                 self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
                 r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
@@ -159,10 +160,16 @@ class ClockSampler:
                 time.sleep(0.005)
         except Exception:
             pass
+        finally:
+            self._ready.set()
 
     def __enter__(self):
+        # NVML is initialised before the timed region opens, so that the region (about
+        # 0.1 s for 20 steps) is sampled from its start
+        self._ready = threading.Event()
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        self._ready.wait(timeout=10)
         return self
 
     def __exit__(self, *a):

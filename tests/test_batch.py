@@ -161,7 +161,7 @@ def test_autotuned_batch_tries_candidates_then_keeps_one(gpu, graph):
     assert best_load in (0.5, 0.35, 0.7) and all(x[0] == best_load for x in trials[6:])
     assert all(x[3] is False for x in trials[6:8])              # the direct splat, twice
     assert sum(1 for x in trials if x[1] == 0) >= 2             # one blur axis per pass
-    assert sum(1 for x in trials if x[2] == 1) == 2             # one vertex per blur thread
+    assert sum(1 for x in trials if x[2] == 1) >= 2             # one vertex per blur thread
     assert seen[n] == seen[n + 1] and seen[n][4] == 2
     assert seen[n][:4] in [x[:4] for x in trials]
 
