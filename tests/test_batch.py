@@ -35,6 +35,28 @@ def test_batch_argument_checks_need_no_gpu():
         ib.bilateral_batch([a], [4.0, 5.0], [0.1])
 
 
+def test_queued_batch_argument_checks_need_no_gpu():
+    """pgpu_bilateral_batch_submit refuses bad arguments before it touches a device: output
+    views of another size, device memory, no images."""
+    import ctypes as C
+    a = np.zeros((3, 20, 24), np.float32)
+    with pytest.raises(ib.PgpuError) as e:      # an output of another size
+        ib.bilateral_batch_submit([a], [4.0], [0.1], outputs=[np.zeros((3, 20, 20), np.float32)])
+    assert e.value.code == ib.ERR_ARGUMENT
+    with pytest.raises(ib.PgpuError) as e:      # one output per image
+        ib.bilateral_batch_submit([a, a.copy()], [4.0, 4.0], [0.1, 0.1], outputs=[a.copy()])
+    assert e.value.code == ib.ERR_ARGUMENT
+    with pytest.raises(ib.PgpuError) as e:      # no images
+        ib.bilateral_batch_submit([], [], [])
+    assert e.value.code == ib.ERR_ARGUMENT
+    v, _ = ib._view(a, "image")
+    opt = ib._options(ib.MEM_DEVICE, "fp32")
+    fw, cs, t = (C.c_float * 1)(4.0), (C.c_float * 1)(0.1), C.c_longlong(0)
+    rc = ib.lib().pgpu_bilateral_batch_submit(C.byref(v), None, 1, fw, cs, C.byref(opt), C.byref(t))
+    assert rc == ib.ERR_ARGUMENT                # queued batches take host memory
+    assert ib.lib().pgpu_batch_wait(0) == ib.ERR_ARGUMENT
+
+
 def test_batched_views_equal_per_image_views():
     """The batched view builder writes the same pgpu_image fields as _view, for (c, h, w)
     and (c, f, h, w) tensors, cropped and channel-sliced ones included, and declines
