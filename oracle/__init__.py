@@ -99,6 +99,9 @@ def _load_ref():
         lib.refh_bilateral.restype = C.c_double
         lib.refh_bilateral.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                        C.c_float, C.c_float, C.c_float, C.c_int]
+        lib.refh_nlmeans3d.restype = C.c_double
+        lib.refh_nlmeans3d.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_float, C.c_int, C.c_float, C.c_float, C.c_int]
         _ref = lib
     return _ref
 
@@ -255,6 +258,22 @@ def reference_joint_bilateral(img: np.ndarray, ref: np.ndarray, sigma_s: float, 
     return a, t
 
 
+def reference_nlmeans3d(vol: np.ndarray, patch: float, dims: int, spatial: float,
+                        patch_sigma: float, method: str = "permutohedral"):
+    """NLMeans3D::apply on a planar (c, f, h, w) volume (src/GaussTransform.cpp:934-941);
+    returns (out, guide, seconds), guide being the (dims, f, h, w) PCA projections the
+    joint bilateral filtered against (the reference draws its patches at random)."""
+    lib = _load_ref()
+    a = np.ascontiguousarray(vol, dtype=np.float32).copy()
+    c, f, h, w = a.shape
+    guide = np.empty((dims, f, h, w), np.float32)
+    t = lib.refh_nlmeans3d(a, guide, w, h, f, c, patch, dims, spatial, patch_sigma,
+                           METHODS[method])
+    if t < 0:
+        raise RuntimeError(lib.refh_last_error().decode())
+    return a, guide, t
+
+
 def reference_gauss_transform(slice_img: np.ndarray | None, splat_img: np.ndarray,
                               values: np.ndarray, sigmas, method: str = "permutohedral"):
     """GaussTransform::apply on planar (c, f, h, w) images; slice_img None = same handle."""
@@ -299,3 +318,30 @@ def bilateral_points(img: np.ndarray, ref: np.ndarray, sigma_s: float, sigma_r: 
         val[:, :, k] = img[k]
     val[:, :, c] = 1.0
     return pos.reshape(-1, cr + 2), val.reshape(-1, c + 1)
+
+
+def volume_points(img: np.ndarray, ref: np.ndarray, sigma_s: float, sigma_r: float,
+                  sigma_t: float):
+    """Positions/values as JointBilateral::apply builds them for a (c, f, h, w) volume
+    filtered in x and y (src/GaussTransform.cpp:540-545, 646-667): the points in t, y, x
+    loop order, positions (ref*(1/sr)..., x*(1/ss), y*(1/ss)[, t*(1/st)]) where the t
+    term is present only when f > 1 and sigma_t < 10 f, values (img..., 1)."""
+    c, f, h, w = img.shape
+    cr = ref.shape[0]
+    filter_t = f > 1 and sigma_t < 10 * f
+    dp = cr + 2 + (1 if filter_t else 0)
+    inv_r = np.float32(1.0) / np.float32(sigma_r)
+    inv_s = np.float32(1.0) / np.float32(sigma_s)
+    pos = np.empty((f, h, w, dp), np.float32)
+    for k in range(cr):
+        pos[..., k] = ref[k] * inv_r
+    pos[..., cr] = np.arange(w, dtype=np.float32)[None, None, :] * inv_s
+    pos[..., cr + 1] = np.arange(h, dtype=np.float32)[None, :, None] * inv_s
+    if filter_t:
+        inv_t = np.float32(1.0) / np.float32(sigma_t)
+        pos[..., cr + 2] = np.arange(f, dtype=np.float32)[:, None, None] * inv_t
+    val = np.empty((f, h, w, c + 1), np.float32)
+    for k in range(c):
+        val[..., k] = img[k]
+    val[..., c] = 1.0
+    return pos.reshape(-1, dp), val.reshape(-1, c + 1)

@@ -9,7 +9,9 @@
 //       (src/GaussTransform.cpp:163-226), and read back its private state: keys in
 //       insertion order, the per-point replay records, values after splat and blur;
 //   (2) call GaussTransform::apply, JointBilateral::apply and Bilateral::apply
-//       (src/GaussTransform.cpp:115, 504, 730) on planar float images.
+//       (src/GaussTransform.cpp:115, 504, 730) on planar float images;
+//   (3) run NLMeans3D::apply's steps (src/GaussTransform.cpp:934-941) and hand back the
+//       PCA guide it filters against, which the reference computes from random patches.
 // The replay record is private in the reference, so this harness opens the class with
 // a preprocessor switch that only affects this translation unit.
 
@@ -17,7 +19,10 @@
 #include <cstring>
 #include <string>
 
+#include "Arithmetic.h"
+#include "Convolve.h"
 #include "GaussTransform.h"
+#include "Statistics.h"
 #define private public
 #include "Permutohedral.h"
 #undef private
@@ -180,6 +185,29 @@ double refh_bilateral(float *im, int w, int h, int f, int c, float fw, float fh,
         Image a = toImage(im, w, h, f, c);
         auto t0 = std::chrono::steady_clock::now();
         Bilateral::apply(a, fw, fh, ft, cs, toMethod(method));
+        auto t1 = std::chrono::steady_clock::now();
+        fromImage(a, im);
+        return std::chrono::duration<double>(t1 - t0).count();
+    } catch (Exception &e) {
+        g_error = e.message;
+        return -1.0;
+    }
+}
+
+// NLMeans3D::apply, in place on im, with the three calls of its body
+// (src/GaussTransform.cpp:934-941) made here so that the guide they produce can be
+// returned: PatchPCA3D's filters (dims of them, drawn from random patches), the image
+// convolved with them (Zero boundary, Inner product: dims channels), and the joint
+// bilateral against that guide with frames INF.  guide receives dims planar channels.
+double refh_nlmeans3d(float *im, float *guide, int w, int h, int f, int c, float patch,
+                      int dims, float spatial, float patch_sigma, int method) {
+    try {
+        Image a = toImage(im, w, h, f, c);
+        auto t0 = std::chrono::steady_clock::now();
+        Image filters = PatchPCA3D::apply(a, patch, dims);
+        Image pca = Convolve::apply(a, filters, Convolve::Zero, Multiply::Inner);
+        fromImage(pca, guide);
+        JointBilateral::apply(a, pca, spatial, spatial, INF, patch_sigma, toMethod(method));
         auto t1 = std::chrono::steady_clock::now();
         fromImage(a, im);
         return std::chrono::duration<double>(t1 - t0).count();

@@ -32,6 +32,16 @@ from rand() seeded by the clock (src/main.cpp:67-75) and compare loosely
                         72x56 YUV image filtered against its luminance, sigmas (2, 0.5), by
                         the reference's PERMUTOHEDRAL and GRID methods (AUTO picks GRID for
                         three position channels)
+  nlmeans3d_d8          the shape of NLMeans3D::apply (src/GaussTransform.cpp:934-941): a
+                        40x32x6-frame RGB volume filtered against the reference's own PCA
+                        guide (PatchPCA3D 5x5x5 patches -> 6 dimensions, Convolve), spatial
+                        sigma 4, patch sigma 0.3, frames INF, so the six frames share one
+                        lattice with d = 6 + 2 = 8 (the guide is stored: the reference
+                        draws its patches at random)
+  video_frames          Bilateral::apply of a 44x36x5-frame RGB volume (a moving image
+                        plus noise), sigma_s 4, sigma_r 0.15, with sigma_t 1.5 (t is a
+                        position, d = 6), 0 (each frame alone, d = 5) and INF (the frames
+                        share one lattice without a t position, d = 5)
   gt_d16_2m             the full-size high-dimensional Gauss transform: 2,000,000 points of
                         synth.gauss_mixture(d=16, seed=2) (the benchmark's input), 4 values
                         + 1, unit sigmas, replay slice: vertex count, SHA-256 digests of the
@@ -173,12 +183,39 @@ def high_d_callers():
          out_permutohedral=perm, out_grid=grid)
 
 
+
+def volume_callers():
+    """Fixtures over several frames: the three ways JointBilateral::apply treats the frame
+    axis (a position, each frame alone, no position) and NLMeans3D's filter."""
+    inf = float("inf")
+    vol = np.stack([np.roll(synth.image(44, 36, 3, rects=6, seed=1100), 2 * t, axis=2) +
+                    0.05 * synth.uniform(1200 + t, 1, 3 * 36 * 44).reshape(3, 36, 44)
+                    for t in range(5)], 1).astype(np.float32)
+    outs = {}
+    for key, ft in (("t1_5", 1.5), ("t0", 0.0), ("tinf", inf)):
+        outs["out_" + key], _ = oracle.reference_bilateral(vol, 4.0, 0.15, sigma_t=ft)
+        if ft != 0.0:   # one lattice over every frame: its vertex count
+            pos, val = oracle.volume_points(vol, vol, 4.0, 0.15, ft)
+            outs["vertices_" + key] = np.int64(oracle.reference_lattice(pos, val).keys.shape[0])
+    save("video_frames", image=vol, sigma_s=np.float32(4), sigma_r=np.float32(0.15), **outs)
+
+    vol = np.stack([synth.image(40, 32, 3, rects=6, seed=1000 + t) for t in range(6)], 1)
+    out, guide, _ = oracle.reference_nlmeans3d(vol, 0.5, 6, 4.0, 0.3)
+    pos, val = oracle.volume_points(vol, guide, 4.0, 0.3, inf)
+    save("nlmeans3d_d8", image=vol, guide=guide, patch=np.float32(0.5), dims=np.int32(6),
+         sigma_s=np.float32(4), sigma_p=np.float32(0.3), out=out,
+         vertices=np.int64(oracle.reference_lattice(pos, val).keys.shape[0]))
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["high_d"]:   # only the fixtures of the high-dimensional callers
         high_d_callers()
+    elif sys.argv[1:] == ["volumes"]:   # only the fixtures over several frames
+        volume_callers()
     elif sys.argv[1:] == ["gt_d16_2m"]:
         gt_d16_2m()
     else:
         main()
         high_d_callers()
+        volume_callers()
         gt_d16_2m()

@@ -280,6 +280,36 @@ def test_nlmeans_filter_shape_d8_matches_reference(gpu):
     assert rel_err(im, g["out"]) <= RTOL_FP32
 
 
+def test_nlmeans3d_filter_shape_matches_reference(gpu):
+    """NLMeans3D::apply's filter (src/GaussTransform.cpp:934-941): six frames against the
+    reference's own 6-channel PCA guide, frames INF, so every frame's points go into one
+    lattice of d = 8 without a t position; its vertex count is the reference's."""
+    g = golden("nlmeans3d_d8")
+    im = g["image"].copy()
+    gpu.JointBilateral.apply(im, g["guide"], float(g["sigma_s"]), float(g["sigma_s"]),
+                             float("inf"), float(g["sigma_p"]))
+    st = gpu.last_stats()
+    assert st["d"] == 8 and st["points"] == im[0].size
+    assert st["vertices"] == int(g["vertices"])
+    assert rel_err(im, g["out"]) <= RTOL_FP32
+
+
+@pytest.mark.parametrize("key,sigma_t,d", [("t1_5", 1.5, 6), ("t0", 0.0, 5),
+                                           ("tinf", float("inf"), 5)])
+def test_video_frames_match_reference(gpu, key, sigma_t, d):
+    """Bilateral::apply over five frames (src/GaussTransform.cpp:532-545): t as a
+    position, each frame alone, and all frames in one lattice without a t position."""
+    g = golden("video_frames")
+    im = g["image"].copy()
+    ss = float(g["sigma_s"])
+    gpu.Bilateral.apply(im, ss, ss, sigma_t, float(g["sigma_r"]))
+    st = gpu.last_stats()
+    assert st["d"] == d
+    if sigma_t != 0.0:   # one lattice over every frame
+        assert st["points"] == im[0].size and st["vertices"] == int(g["vertices_" + key])
+    assert rel_err(im, g["out_" + key]) <= RTOL_FP32
+
+
 @pytest.mark.parametrize("method,key", [("permutohedral_gpu", "out_permutohedral"),
                                         ("grid_gpu", "out_grid")])
 def test_chromablur_filter_shape_matches_reference(gpu, method, key):

@@ -213,3 +213,43 @@ def test_oracle_high_dimensional_callers(name, guide_key, sr_key, out_key):
     c, h, w = im.shape
     norm = (d.out[:, :c] / d.out[:, c:c + 1]).reshape(h, w, c).transpose(2, 0, 1)
     np.testing.assert_array_equal(norm, g[out_key])
+
+
+def test_oracle_nlmeans3d_shape():
+    """NLMeans3D's filter (src/GaussTransform.cpp:934-941): six frames against a 6-channel
+    PCA guide with frames INF share one lattice of d = 8; the oracle reproduces the
+    reference's output bit for bit."""
+    g = golden("nlmeans3d_d8")
+    im = g["image"]
+    pos, val = oracle.volume_points(im, g["guide"], float(g["sigma_s"]), float(g["sigma_p"]),
+                                    float("inf"))
+    assert pos.shape == (im[0].size, 8)
+    d = oracle.oracle_lattice(pos, val)
+    assert d.keys.shape[0] == int(g["vertices"])
+    c, f, h, w = im.shape
+    norm = (d.out[:, :c] / d.out[:, c:c + 1]).reshape(f, h, w, c).transpose(3, 0, 1, 2)
+    np.testing.assert_array_equal(norm, g["out"])
+
+
+@pytest.mark.parametrize("key,sigma_t", [("t1_5", 1.5), ("t0", 0.0), ("tinf", float("inf"))])
+def test_oracle_video_frames(key, sigma_t):
+    """Bilateral::apply over five frames: t as a position (d = 6), each frame alone, and the
+    frames in one lattice without a t position (src/GaussTransform.cpp:532-545)."""
+    g = golden("video_frames")
+    im = g["image"]
+    ss, sr = float(g["sigma_s"]), float(g["sigma_r"])
+    c, f, h, w = im.shape
+    if sigma_t == 0.0:
+        frames = []
+        for t in range(f):
+            pos, val = oracle.bilateral_points(im[:, t], im[:, t], ss, sr)
+            d = oracle.oracle_lattice(pos, val)
+            frames.append((d.out[:, :c] / d.out[:, c:c + 1]).reshape(h, w, c).transpose(2, 0, 1))
+        norm = np.stack(frames, 1)
+    else:
+        pos, val = oracle.volume_points(im, im, ss, sr, sigma_t)
+        assert pos.shape[1] == (6 if sigma_t == 1.5 else 5)
+        d = oracle.oracle_lattice(pos, val)
+        assert d.keys.shape[0] == int(g["vertices_" + key])
+        norm = (d.out[:, :c] / d.out[:, c:c + 1]).reshape(f, h, w, c).transpose(3, 0, 1, 2)
+    np.testing.assert_array_equal(norm, g["out_" + key])
