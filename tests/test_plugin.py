@@ -120,3 +120,94 @@ def test_cli_grid_gpu_matches_cli_grid(tmp_path):
         run_cli(["-load", "in.tmp", "-bilateral", "0.1", "8", "8", "0", m, "-save", "g_%s.tmp" % m],
                 tmp_path)
     assert rel_err(load_tmp(tmp_path / "g_grid_gpu.tmp"), load_tmp(tmp_path / "g_grid.tmp")) <= 1e-5
+
+
+# The operations that end in JointBilateral::apply (src/GaussTransform.cpp:739-941).
+CALLERS = ("nlmeans", "nlmeans3d", "chromablur", "bilateralsharpen")
+
+
+@needs_cli
+def test_plugin_callers_help_and_cpu_paths_unchanged(tmp_path):
+    """-chromablur and -bilateralsharpen without a method token are the reference's own
+    operations (deterministic, so the outputs are compared bit for bit); every caller's
+    help names the GPU method."""
+    for name in CALLERS:
+        assert "permutohedral_gpu" in run_cli(["-help", name], tmp_path)
+    img = synth.image(48, 36, 3, rects=4, seed=3)
+    save_tmp(tmp_path / "in.tmp", img)
+    for op in (["-chromablur", "2", "0.5"], ["-bilateralsharpen", "4", "0.2", "0.5"]):
+        args = ["-load", "in.tmp"] + op + ["-save", "out.tmp"]
+        run_cli(args, tmp_path, plugin=False)
+        a = load_tmp(tmp_path / "out.tmp")
+        run_cli(args, tmp_path, plugin=True)
+        np.testing.assert_array_equal(load_tmp(tmp_path / "out.tmp"), a)
+
+
+@needs_cli
+def test_plugin_nlmeans3d_refuses_volumes_shorter_than_a_patch(tmp_path):
+    """The reference's 3D patch sampler has no valid patch centre in a one-frame image (it
+    samples out of bounds); the GPU path refuses it before any device call."""
+    save_tmp(tmp_path / "in.tmp", synth.image(48, 36, 3, rects=4, seed=3))
+    out = run_cli(["-load", "in.tmp", "-nlmeans3d", "0.5", "6", "4", "0.4", "permutohedral_gpu",
+                   "-save", "out.tmp"], tmp_path)
+    assert "do not fit" in out
+    assert not (tmp_path / "out.tmp").exists()
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_cli_chromablur_and_bilateralsharpen_gpu_match_cpu(tmp_path):
+    """-chromablur ... grid_gpu against the reference's -chromablur (AUTO: the grid for its
+    three position channels) and -bilateralsharpen ... permutohedral_gpu against the
+    reference's (AUTO: the lattice, d = 5).  The sharpened image is im * 1.5 - filtered *
+    0.5, which passes near zero, so its error is taken against its largest magnitude."""
+    img = synth.image(160, 120, 3, rects=8, seed=8)
+    save_tmp(tmp_path / "in.tmp", img)
+    run_cli(["-load", "in.tmp", "-chromablur", "2", "0.5", "-save", "cb_cpu.tmp"], tmp_path)
+    log = run_cli(["-load", "in.tmp", "-chromablur", "2", "0.5", "grid_gpu", "-save", "cb_gpu.tmp"],
+                  tmp_path)
+    assert (tmp_path / "cb_gpu.tmp").exists(), log
+    assert rel_err(load_tmp(tmp_path / "cb_gpu.tmp"), load_tmp(tmp_path / "cb_cpu.tmp")) <= 1e-5
+    run_cli(["-load", "in.tmp", "-bilateralsharpen", "8", "0.2", "0.5", "-save", "bs_cpu.tmp"],
+            tmp_path)
+    log = run_cli(["-load", "in.tmp", "-bilateralsharpen", "8", "0.2", "0.5", "permutohedral_gpu",
+                   "-save", "bs_gpu.tmp"], tmp_path)
+    assert (tmp_path / "bs_gpu.tmp").exists(), log
+    a, b = load_tmp(tmp_path / "bs_gpu.tmp"), load_tmp(tmp_path / "bs_cpu.tmp")
+    assert float(np.abs(a - b).max()) <= 1e-5 * float(np.abs(b).max())
+
+
+@needs_cli
+@pytest.mark.gpu
+@pytest.mark.parametrize("op,patch,frames", [("-nlmeans", "1", 1), ("-nlmeans3d", "0.5", 6)])
+def test_cli_nlmeans_gpu_denoises_like_cpu(tmp_path, op, patch, frames):
+    """-nlmeans / -nlmeans3d with the GPU filter.  The reference draws its PCA patches at
+    random (rand() seeded by the clock), so two runs filter against different guides: the
+    GPU run must remove as much noise as the reference's own run (uniform noise of +-0.2;
+    the reference leaves 0.039-0.042 mean absolute error of the 0.10 it was given)."""
+    if frames == 1:
+        clean = synth.image(96, 72, 3, rects=6, seed=41)
+    else:
+        clean = np.stack([synth.image(40, 32, 3, rects=4, seed=50)] * frames, 1)
+    noise = (synth.uniform(42, 1, clean.size).reshape(clean.shape) * 0.4 - 0.2).astype(np.float32)
+    save_tmp(tmp_path / "noisy.tmp", clean + noise)
+    args = [patch, "6", "8", "0.3"]
+    run_cli(["-load", "noisy.tmp", op] + args + ["permutohedral", "-save", "cpu.tmp"], tmp_path)
+    log = run_cli(["-load", "noisy.tmp", op] + args + ["permutohedral_gpu", "-save", "gpu.tmp"],
+                  tmp_path)
+    assert (tmp_path / "gpu.tmp").exists(), log
+    err_cpu = float(np.abs(load_tmp(tmp_path / "cpu.tmp") - clean).mean())
+    err_gpu = float(np.abs(load_tmp(tmp_path / "gpu.tmp") - clean).mean())
+    print(op, "mean abs error: noisy", float(np.abs(noise).mean()), "cpu", err_cpu, "gpu", err_gpu)
+    assert err_gpu <= 0.5 * float(np.abs(noise).mean())
+    assert err_gpu <= 1.1 * err_cpu
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_cli_caller_self_tests_pass_with_plugin(tmp_path):
+    """-test on the callers runs the plugin's checks: the GPU filter against the reference's
+    on one PCA guide (NLMeans, NLMeans3D), -chromablur against the reference's grid and
+    -bilateralsharpen against its lattice."""
+    out = run_cli(["-test"] + list(CALLERS), tmp_path)
+    assert out.count("Passed") >= 4 and "Failed" not in out, out[-2000:]
