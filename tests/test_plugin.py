@@ -159,15 +159,18 @@ def test_plugin_nlmeans3d_refuses_volumes_shorter_than_a_patch(tmp_path):
 def test_cli_chromablur_and_bilateralsharpen_gpu_match_cpu(tmp_path):
     """-chromablur ... grid_gpu against the reference's -chromablur (AUTO: the grid for its
     three position channels) and -bilateralsharpen ... permutohedral_gpu against the
-    reference's (AUTO: the lattice, d = 5).  The sharpened image is im * 1.5 - filtered *
-    0.5, which passes near zero, so its error is taken against its largest magnitude."""
+    reference's (AUTO: the lattice, d = 5).  Both outputs pass through zero (the colour
+    round trip and the sharpening mix im * 1.5 - filtered * 0.5 leave pixels near 0), where
+    summation order alone moves the last FP32 bits by more than 1e-5 of the value, so the
+    error is taken against each output's largest magnitude."""
     img = synth.image(160, 120, 3, rects=8, seed=8)
     save_tmp(tmp_path / "in.tmp", img)
     run_cli(["-load", "in.tmp", "-chromablur", "2", "0.5", "-save", "cb_cpu.tmp"], tmp_path)
     log = run_cli(["-load", "in.tmp", "-chromablur", "2", "0.5", "grid_gpu", "-save", "cb_gpu.tmp"],
                   tmp_path)
     assert (tmp_path / "cb_gpu.tmp").exists(), log
-    assert rel_err(load_tmp(tmp_path / "cb_gpu.tmp"), load_tmp(tmp_path / "cb_cpu.tmp")) <= 1e-5
+    a, b = load_tmp(tmp_path / "cb_gpu.tmp"), load_tmp(tmp_path / "cb_cpu.tmp")
+    assert float(np.abs(a - b).max()) <= 1e-5 * float(np.abs(b).max())
     run_cli(["-load", "in.tmp", "-bilateralsharpen", "8", "0.2", "0.5", "-save", "bs_cpu.tmp"],
             tmp_path)
     log = run_cli(["-load", "in.tmp", "-bilateralsharpen", "8", "0.2", "0.5", "permutohedral_gpu",
