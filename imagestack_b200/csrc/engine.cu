@@ -246,6 +246,10 @@ bool view_ok(const pgpu_image* v) {
            v->ystride >= v->width && v->tstride >= 0 && v->cstride >= 0;
 }
 
+bool points_fit(const pgpu_image* v) {
+    return (uint64_t)v->width * (uint64_t)v->height * (uint64_t)v->frames <= 0xFFFFFFFFull;
+}
+
 bool same_view(const pgpu_image& a, const pgpu_image& b) {
     return a.base == b.base && a.ystride == b.ystride && a.tstride == b.tstride &&
            a.cstride == b.cstride && a.width == b.width && a.height == b.height &&
@@ -863,6 +867,8 @@ int pgpu_gauss_transform(const pgpu_image* slice, const pgpu_image* splat, const
     const pgpu_options opt = opts_or_default(opt_in);
     if (!view_ok(splat) || !view_ok(values) || !view_ok(out) || (slice && !view_ok(slice)) || !sigmas)
         return fail(PGPU_ERR_ARGUMENT, "invalid image view or sigmas");
+    if (!points_fit(splat) || (slice && !points_fit(slice)))
+        return fail(PGPU_ERR_UNSUPPORTED, "more than 2^32 - 1 points in one lattice");
     ApiScope S(&opt);
     if (S.rc) return S.rc;
     Engine& E = *S.E;
@@ -894,6 +900,7 @@ int pgpu_joint_bilateral(pgpu_image* im, const pgpu_image* ref, float filter_wid
                          const pgpu_options* opt_in) {
     const pgpu_options opt = opts_or_default(opt_in);
     if (!view_ok(im) || !view_ok(ref)) return fail(PGPU_ERR_ARGUMENT, "invalid image view");
+    if (!points_fit(im)) return fail(PGPU_ERR_UNSUPPORTED, "more than 2^32 - 1 points in one lattice");
     ApiScope S(&opt);
     if (S.rc) return S.rc;
     Engine& E = *S.E;
@@ -932,6 +939,8 @@ int pgpu_bilateral_batch(pgpu_image* ims, int count, const float* filter_width,
         const float fw = filter_width[i];
         if (!view_ok(&v) || v.channels != C || v.frames != 1)
             return fail(PGPU_ERR_ARGUMENT, "batch image %d: single-frame images with %d channels expected", i, C);
+        if (!points_fit(&v))
+            return fail(PGPU_ERR_UNSUPPORTED, "batch image %d: more than 2^32 - 1 points", i);
         // every image must have both pixel axes as positions (d = C + 2), as
         // JointBilateral::apply makes them for fw < 10 x the size (src/GaussTransform.cpp:541-542)
         if (v.width < 2 || v.height < 2 || !(fw > 0) || !(fw < 10 * v.width) || !(fw < 10 * v.height) ||
@@ -969,6 +978,8 @@ int pgpu_bilateral_batch_submit(const pgpu_image* in, pgpu_image* out, int count
         const float fw = filter_width[i];
         if (!view_ok(&v) || v.channels != C || v.frames != 1)
             return fail(PGPU_ERR_ARGUMENT, "batch image %d: single-frame images with %d channels expected", i, C);
+        if (!points_fit(&v))
+            return fail(PGPU_ERR_UNSUPPORTED, "batch image %d: more than 2^32 - 1 points", i);
         if (!view_ok(&o) || o.width != v.width || o.height != v.height || o.frames != 1 || o.channels != C)
             return fail(PGPU_ERR_ARGUMENT, "batch image %d: the output view differs in size from the input", i);
         if (v.width < 2 || v.height < 2 || !(fw > 0) || !(fw < 10 * v.width) || !(fw < 10 * v.height) ||

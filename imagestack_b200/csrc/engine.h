@@ -123,6 +123,8 @@ struct Engine {
 
 // image views and their staging (engine.cu)
 bool view_ok(const pgpu_image* v);
+// its pixels over all frames fit the lattice's 32-bit point numbering
+bool points_fit(const pgpu_image* v);
 bool same_view(const pgpu_image& a, const pgpu_image& b);
 bool is_dense(const pgpu_image& v);
 pgpu_image dense_like(const pgpu_image& v, float* base, int channels);

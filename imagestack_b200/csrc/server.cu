@@ -225,6 +225,7 @@ public:
 
     int validate(const pgpu_request& r, Req* q) {
         if (!view_ok(&r.in) || !view_ok(&r.out)) return fail(PGPU_ERR_ARGUMENT, "invalid image view");
+        if (!points_fit(&r.in)) return fail(PGPU_ERR_UNSUPPORTED, "more than 2^32 - 1 points in one request");
         const pgpu_image& a = r.in;
         switch (r.kind) {
         case PGPU_REQ_BILATERAL:

@@ -34,7 +34,8 @@ typedef struct pgpu_image {
 /* status codes */
 #define PGPU_OK 0
 #define PGPU_ERR_ARGUMENT 1     /* bad sizes, mismatched images (the reference asserts) */
-#define PGPU_ERR_UNSUPPORTED 2  /* position dimensions > 16 or value channels > 8 */
+#define PGPU_ERR_UNSUPPORTED 2  /* position dimensions > 16, value channels > 8, or more than
+                                 * 2^32 - 1 points (pixels x frames) in one lattice */
 #define PGPU_ERR_CUDA 3         /* a CUDA call failed; see pgpu_last_error() */
 #define PGPU_ERR_MEMORY 4       /* device or pinned allocation failed */
 #define PGPU_ERR_CAPACITY 5     /* hash table still overfull after the retries */

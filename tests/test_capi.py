@@ -77,3 +77,29 @@ def test_views_mirror_image_addressing():
     assert (v.ystride, v.tstride, v.cstride) == (7, 35, 70)
     with pytest.raises(ib.PgpuError):
         ib._view(a.astype(np.float64), "f64")
+
+
+def test_views_beyond_the_point_numbering_are_refused_before_any_device_work():
+    """A lattice numbers its points in 32 bits: a view of 65536 x 65536 pixels (2^32
+    points) is refused with ERR_UNSUPPORTED by every entry point, before the library
+    looks for a device or reads a pixel (the base address is never dereferenced)."""
+    lib = ib.lib()
+    buf = np.zeros(16, np.float32)
+    n = 1 << 16
+    big = ib.Image(buf.ctypes.data, n, n, 1, 3, n, n * n, n * n)
+    small = ib.Image(buf.ctypes.data, 4, 4, 1, 3, 4, 16, 16)
+    opt = ib.Options()
+    lib.pgpu_default_options(C.byref(opt))
+    rc = lib.pgpu_joint_bilateral(C.byref(big), C.byref(big), 8.0, 8.0, 0.0, 0.1, C.byref(opt))
+    assert rc == ib.ERR_UNSUPPORTED and b"2^32" in lib.pgpu_last_error()
+    sig = (C.c_float * 3)(1.0, 1.0, 1.0)
+    rc = lib.pgpu_gauss_transform(None, C.byref(big), C.byref(big), sig, 3, C.byref(big), C.byref(opt))
+    assert rc == ib.ERR_UNSUPPORTED
+    rc = lib.pgpu_gauss_transform(C.byref(big), C.byref(small), C.byref(small), sig, 3, C.byref(big),
+                                  C.byref(opt))
+    assert rc == ib.ERR_UNSUPPORTED
+    fw, cs = (C.c_float * 1)(8.0), (C.c_float * 1)(0.1)
+    assert lib.pgpu_bilateral_batch(C.byref(big), 1, fw, cs, C.byref(opt)) == ib.ERR_UNSUPPORTED
+    ticket = C.c_longlong(0)
+    rc = lib.pgpu_bilateral_batch_submit(C.byref(big), None, 1, fw, cs, C.byref(opt), C.byref(ticket))
+    assert rc == ib.ERR_UNSUPPORTED and ticket.value == 0
